@@ -1,0 +1,206 @@
+/*
+ * sph2o_cuda.h -- C ABI of the B200 (sm_100a) SPH particle pipeline.
+ *
+ * This is the drop-in boundary for SPH2O's per-step particle path. SPH2O has
+ * no plugin or FFI layer: its boundary is the C++ virtual class
+ *   SPHSolver { init(); step(); resize(); computeDensities(); integrate();
+ *               insertFluidParticles(); neighborhoodSearch(); }
+ * (inc/SPH2O/SPHSolver/SPHSolver.h:22-37), created by
+ * SPHSimulation::setSimulationMethod (src/SPH2O/SPHSimulation.cpp:216-239)
+ * and stepped by SPHSimulation::step (src/SPH2O/SPHSimulation.cpp:168).
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions: every function returns an int status (SPH_OK = 0, negative =
+ * error; see sph_status). No C++ exception crosses this ABI. Arrays are plain
+ * host pointers; xyz arrays hold n*3 floats (x0 y0 z0 x1 ...). A context owns
+ * all of its device memory and one CUDA stream; the caller keeps ownership of
+ * every array it passes. One host thread drives a context at a time.
+ * Particle order at this boundary is always the caller's (reference) order;
+ * the internal cell-sorted order never leaks out.
+ */
+#ifndef SPH2O_CUDA_H
+#define SPH2O_CUDA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPH2O_ABI_VERSION 1
+
+/* Method ids, identical to SPHSimulation's constants
+   (src/SPH2O/SPHSimulation.cpp:21-33). */
+enum sph_method { SPH_WCSPH = 0, SPH_PCISPH = 1, SPH_DFSPH = 2 };
+enum sph_boundary_method { SPH_BOUNDARY_CUBE = 0, SPH_BOUNDARY_PCISPH = 1, SPH_BOUNDARY_AKINCI = 2 };
+enum sph_force_method {
+    SPH_VISCOSITY_STANDARD = 0,
+    SPH_VISCOSITY_ARTIFICIAL = 1,
+    SPH_VISCOSITY_XSPH = 2,
+    SPH_SURFACE_TENSION_AKINCI = 3,
+    SPH_ADHESION_AKINCI = 4
+};
+
+enum sph_status {
+    SPH_OK = 0,
+    SPH_ERR_ARG = -1,              /* bad argument or unsupported option      */
+    SPH_ERR_CUDA = -2,             /* CUDA runtime error (text in last_error) */
+    SPH_ERR_NAN = -3,              /* non-finite particle state detected      */
+    SPH_ERR_NEIGHBOR_OVERFLOW = -4,/* a particle exceeded the neighbour capacity */
+    SPH_ERR_TIMEOUT = -5,          /* a bounded device-side wait gave up      */
+    SPH_ERR_STATE = -6,            /* call out of order (e.g. step before init) */
+    SPH_ERR_NO_DEVICE = -7,        /* no CUDA device / extension unusable     */
+    SPH_ERR_IO = -8,               /* file or JSON error                      */
+    SPH_ERR_CAPACITY = -9          /* size above a fixed, documented maximum  */
+};
+
+/* Scene parameters: the fields of SceneInfo + Fluid (inc/SPH2O/SPHStructs.h:11-67)
+   that the particle path reads. */
+typedef struct sph_scene_desc {
+    int simulation_method;          /* sph_method */
+    int boundary_method;            /* only SPH_BOUNDARY_AKINCI is implemented */
+    int viscosity_method;           /* -1 none, 0 standard, 1 artificial, 2 XSPH */
+    int surface_tension_method;     /* -1 none, 3 Akinci */
+    int adhesion_method;            /* -1 none, 4 Akinci */
+    float particle_radius;          /* r; support radius h = 4r (SPHSimulation.cpp:201-208) */
+    float density0;                 /* rest density */
+    float gravity[3];
+    float time_step;                /* initial (DFSPH) or fixed (WCSPH/PCISPH) dt */
+    float min_time_step, max_time_step, fps;
+    float start_time, end_time;
+    float stiffness, gamma;         /* WCSPH Tait EOS */
+    float eta, eta_v, cfl_factor;   /* PCISPH/DFSPH tolerances, DFSPH CFL factor */
+    unsigned min_iterations, max_iterations, min_iterations_v, max_iterations_v;
+    float viscosity, boundary_viscosity, surface_tension, adhesion;
+    float domain_min[3], domain_max[3]; /* grid bounds hint; all zero = derive from particles */
+    unsigned flags;                 /* reserved, must be 0 */
+} sph_scene_desc;
+
+/* Per-call statistics (the values SPH2O prints only under DEBUG). */
+typedef struct sph_step_stats {
+    double time;                    /* simulated time after the last step */
+    double avg_density_error;       /* last density-solver residual (FP64 reduction) */
+    double avg_divergence_error;    /* last divergence-solver residual (FP64 reduction) */
+    float dt;                       /* time step used by the last step */
+    float max_velocity;             /* CFL speed of the last DFSPH step, else 0 */
+    unsigned iterations;            /* density / pressure iterations of the last step */
+    unsigned iterations_v;          /* divergence iterations of the last step (DFSPH) */
+    unsigned long long total_iterations;   /* summed over the steps of this call */
+    unsigned long long total_iterations_v;
+    unsigned steps;                 /* steps taken by this call */
+    unsigned neighbor_overflows;    /* particles whose neighbour list was truncated */
+} sph_step_stats;
+
+typedef struct sph_ctx sph_ctx;
+
+/* ---- context lifecycle ------------------------------------------------ */
+
+/* Replaces SPHSimulation::setSimulationMethod + the solver constructors
+   (SPHSimulation.cpp:216-239, 316-350). Selects the device with
+   cudaGetDevice at the time of the call. */
+int sph_create(const sph_scene_desc* desc, sph_ctx** out);
+
+/* Fluid particles (FluidObject::r / v, inc/SPH2O/FluidObject/FluidObject.h:17-24).
+   v may be NULL (zero velocities). Must precede sph_init. */
+int sph_set_fluid(sph_ctx* ctx, unsigned n, const float* xyz, const float* v);
+
+/* Akinci boundary particles of all boundary objects, concatenated in object
+   order (AkinciBoundaryObject::r, AkinciBoundaryObject.cpp:36-95). */
+int sph_set_boundary(sph_ctx* ctx, unsigned n, const float* xyz);
+
+/* Replaces SPHSimulation::init (SPHSimulation.cpp:117-126): kernel constants,
+   masses m = rho0 (2r)^3, boundary volumes (AkinciBoundaryObject::computeVolume,
+   AkinciBoundaryObject.cpp:10-34) and the solver's init (DFSPHSolver::init,
+   DFSPHSolver.cpp:22-31: neighbour search, densities, alpha;
+   PCISPHSolver::init: scaling factor, PCISPHSolver.cpp:403-436). */
+int sph_init(sph_ctx* ctx);
+
+/* Replaces nsteps calls of SPHSolver::step (WCSPHSolver.cpp:14-78,
+   PCISPHSolver.cpp:20-80, DFSPHSolver.cpp:33-107). Kernels are queued on the
+   context stream; the call returns after the last step completes and `out`
+   (may be NULL) is filled. Steps are taken unconditionally: the start/end
+   time window of SPHSimulation::step is the driver's business. */
+int sph_step(sph_ctx* ctx, int nsteps, sph_step_stats* out);
+
+/* Queue nsteps steps without waiting (no stats); sph_sync waits and returns
+   the status of everything queued since the last wait. */
+int sph_step_async(sph_ctx* ctx, int nsteps);
+int sph_sync(sph_ctx* ctx, sph_step_stats* out);
+
+/* Fluid state in the caller's particle order. Any pointer may be NULL.
+   rho is FluidObject::density as SPH2O leaves it after a step. */
+int sph_get_state(sph_ctx* ctx, float* xyz, float* v, float* rho);
+
+/* Replace positions/velocities (same order as sph_set_fluid) between steps;
+   replaces writes through FluidObject::getPosition/getVelocity. */
+int sph_set_state(sph_ctx* ctx, const float* xyz, const float* v);
+
+/* Akinci boundary volumes V_b in the sph_set_boundary order. */
+int sph_get_boundary_volume(sph_ctx* ctx, float* vol);
+
+/* Simulated time and current dt (TimeHelper::getTime/getTimeStep). */
+int sph_get_time(sph_ctx* ctx, double* time, float* dt);
+
+unsigned sph_num_fluid(const sph_ctx* ctx);
+unsigned sph_num_boundary(const sph_ctx* ctx);
+
+/* Text of the last error on this context (never NULL). */
+const char* sph_last_error(const sph_ctx* ctx);
+/* Text of the last error of a call that had no context (sph_create). */
+const char* sph_global_error(void);
+
+int sph_destroy(sph_ctx* ctx);
+
+/* ---- phase access for parity checks ------------------------------------- */
+
+enum sph_phase {
+    SPH_PHASE_DENSITY = 0,          /* SPHSolver::computeDensities (SPHSolver.cpp:42-89), n floats */
+    SPH_PHASE_ALPHA = 1,            /* DFSPHSolver::computeAlpha (DFSPHSolver.cpp:109-178), n floats */
+    SPH_PHASE_NONPRESSURE_ACC = 2,  /* SPHSimulation::computeNonPressureForces, n*3 floats */
+    SPH_PHASE_PRESSURE = 3,         /* WCSPHSolver::computePressures (WCSPHSolver.cpp:80-129), n floats */
+    SPH_PHASE_PRESSURE_ACC = 4      /* WCSPHSolver::computePressureForce (WCSPHSolver.cpp:132-188), n*3 */
+};
+
+/* Runs the neighbour search at the current positions, then the named phase
+   (and the phases it depends on: densities before alpha/forces/pressure),
+   and copies its per-particle result out in caller order. State used by the
+   next sph_step is not changed except densities and neighbour lists, which
+   the next step recomputes anyway. */
+int sph_compute_phase(sph_ctx* ctx, int phase, float* out);
+
+/* Neighbour sets of every fluid particle at the current positions, in CSR
+   form and caller order: N(i) = { j in the 27 cells around floor(x_i / h) :
+   |x_i - x_j| <= h } with |.| evaluated as sqrt((dx*dx + dy*dy) + dz*dz) in
+   IEEE single precision, the test of DFSPHSolver.cpp:575,589,603.
+   With NULL index arrays only the totals are returned in *nf_total/*nb_total.
+   Offsets arrays hold n+1 entries. Indices are caller-order fluid / boundary ids. */
+int sph_debug_neighbors(sph_ctx* ctx, unsigned* f_offsets, unsigned* f_index, size_t f_cap,
+                        unsigned* b_offsets, unsigned* b_index, size_t b_cap,
+                        size_t* nf_total, size_t* nb_total);
+
+/* ---- host scene loading (SceneLoader + object builders) --------------- */
+
+typedef struct sph_scene sph_scene;
+
+/* Replaces SceneLoader::readConfiguration (SceneLoader.cpp:11-209) and the
+   object construction of SPHSimulation::importScene (SPHSimulation.cpp:299-481):
+   FluidObject::build lattice (FluidObject.cpp:30-61), seeded jitter,
+   AkinciBoundaryObject::sampleCube/sampleSphere (AkinciBoundaryObject.cpp:97-153).
+   Missing "sphere"/"geometry" keys are tolerated. */
+int sph_scene_load(const char* json_path, sph_scene** out);
+int sph_scene_parse(const char* json_text, sph_scene** out);
+int sph_scene_get_desc(const sph_scene* s, sph_scene_desc* out);
+unsigned sph_scene_num_fluid(const sph_scene* s);
+unsigned sph_scene_num_boundary(const sph_scene* s);
+int sph_scene_get_fluid(const sph_scene* s, float* xyz, float* v);
+int sph_scene_get_boundary(const sph_scene* s, float* xyz);
+const char* sph_scene_error(void);
+void sph_scene_free(sph_scene* s);
+
+/* create + set_fluid + set_boundary + init from a loaded scene. */
+int sph_create_from_scene(const sph_scene* s, sph_ctx** out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,270 @@
+"""ctypes binding of the C ABI in include/sph2o_cuda.h.
+
+This is the binding a Python caller (tests, bench.py) uses; it adds no
+computation of its own. The CUDA library must have been built in-tree
+(`python -m sph2o_b200.build`); loading fails loudly if it is missing.
+
+    from sph2o_b200.api import Scene, Simulation
+    sim = Simulation.from_scene(Scene.load("scene.json"))
+    stats = sim.step(10)
+    pos, vel, rho = sim.state()
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsph2o_cuda.so")
+
+SPH_OK = 0
+STATUS = {
+    0: "SPH_OK", -1: "SPH_ERR_ARG", -2: "SPH_ERR_CUDA", -3: "SPH_ERR_NAN",
+    -4: "SPH_ERR_NEIGHBOR_OVERFLOW", -5: "SPH_ERR_TIMEOUT", -6: "SPH_ERR_STATE",
+    -7: "SPH_ERR_NO_DEVICE", -8: "SPH_ERR_IO", -9: "SPH_ERR_CAPACITY",
+}
+PHASE_DENSITY, PHASE_ALPHA, PHASE_NONPRESSURE_ACC, PHASE_PRESSURE, PHASE_PRESSURE_ACC = range(5)
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("simulation_method", C.c_int), ("boundary_method", C.c_int), ("viscosity_method", C.c_int),
+        ("surface_tension_method", C.c_int), ("adhesion_method", C.c_int),
+        ("particle_radius", C.c_float), ("density0", C.c_float), ("gravity", C.c_float * 3),
+        ("time_step", C.c_float), ("min_time_step", C.c_float), ("max_time_step", C.c_float),
+        ("fps", C.c_float), ("start_time", C.c_float), ("end_time", C.c_float),
+        ("stiffness", C.c_float), ("gamma", C.c_float),
+        ("eta", C.c_float), ("eta_v", C.c_float), ("cfl_factor", C.c_float),
+        ("min_iterations", C.c_uint), ("max_iterations", C.c_uint),
+        ("min_iterations_v", C.c_uint), ("max_iterations_v", C.c_uint),
+        ("viscosity", C.c_float), ("boundary_viscosity", C.c_float),
+        ("surface_tension", C.c_float), ("adhesion", C.c_float),
+        ("domain_min", C.c_float * 3), ("domain_max", C.c_float * 3), ("flags", C.c_uint),
+    ]
+
+
+class StepStats(C.Structure):
+    _fields_ = [
+        ("time", C.c_double), ("avg_density_error", C.c_double), ("avg_divergence_error", C.c_double),
+        ("dt", C.c_float), ("max_velocity", C.c_float), ("iterations", C.c_uint), ("iterations_v", C.c_uint),
+        ("total_iterations", C.c_ulonglong), ("total_iterations_v", C.c_ulonglong),
+        ("steps", C.c_uint), ("neighbor_overflows", C.c_uint),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class SphError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m sph2o_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P, U, I, F = C.c_void_p, C.c_uint, C.c_int, C.POINTER(C.c_float)
+    sigs = {
+        "sph_create": (I, [C.POINTER(SceneDesc), C.POINTER(P)]),
+        "sph_set_fluid": (I, [P, U, F, F]),
+        "sph_set_boundary": (I, [P, U, F]),
+        "sph_init": (I, [P]),
+        "sph_step": (I, [P, I, C.POINTER(StepStats)]),
+        "sph_step_async": (I, [P, I]),
+        "sph_sync": (I, [P, C.POINTER(StepStats)]),
+        "sph_get_state": (I, [P, F, F, F]),
+        "sph_set_state": (I, [P, F, F]),
+        "sph_get_boundary_volume": (I, [P, F]),
+        "sph_get_time": (I, [P, C.POINTER(C.c_double), F]),
+        "sph_num_fluid": (U, [P]),
+        "sph_num_boundary": (U, [P]),
+        "sph_last_error": (C.c_char_p, [P]),
+        "sph_global_error": (C.c_char_p, []),
+        "sph_destroy": (I, [P]),
+        "sph_compute_phase": (I, [P, I, F]),
+        "sph_debug_neighbors": (I, [P, C.POINTER(U), C.POINTER(U), C.c_size_t, C.POINTER(U), C.POINTER(U),
+                                    C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+        "sph_scene_load": (I, [C.c_char_p, C.POINTER(P)]),
+        "sph_scene_parse": (I, [C.c_char_p, C.POINTER(P)]),
+        "sph_scene_get_desc": (I, [P, C.POINTER(SceneDesc)]),
+        "sph_scene_num_fluid": (U, [P]),
+        "sph_scene_num_boundary": (U, [P]),
+        "sph_scene_get_fluid": (I, [P, F, F]),
+        "sph_scene_get_boundary": (I, [P, F]),
+        "sph_scene_error": (C.c_char_p, []),
+        "sph_scene_free": (None, [P]),
+        "sph_create_from_scene": (I, [P, C.POINTER(P)]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+
+
+def _uptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint)) if a is not None else None
+
+
+class Scene:
+    """Host-side scene: SPH2O JSON schema -> parameters + particles."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def load(cls, path):
+        h = C.c_void_p()
+        rc = lib().sph_scene_load(os.fsencode(path), C.byref(h))
+        if rc != SPH_OK:
+            raise SphError(rc, lib().sph_scene_error().decode())
+        return cls(h.value)
+
+    @classmethod
+    def from_dict(cls, d):
+        h = C.c_void_p()
+        rc = lib().sph_scene_parse(json.dumps(d).encode(), C.byref(h))
+        if rc != SPH_OK:
+            raise SphError(rc, lib().sph_scene_error().decode())
+        return cls(h.value)
+
+    def desc(self):
+        d = SceneDesc()
+        lib().sph_scene_get_desc(self._h, C.byref(d))
+        return d
+
+    def fluid(self):
+        n = lib().sph_scene_num_fluid(self._h)
+        x = np.zeros((n, 3), np.float32)
+        v = np.zeros((n, 3), np.float32)
+        lib().sph_scene_get_fluid(self._h, _fptr(x), _fptr(v))
+        return x, v
+
+    def boundary(self):
+        n = lib().sph_scene_num_boundary(self._h)
+        b = np.zeros((n, 3), np.float32)
+        lib().sph_scene_get_boundary(self._h, _fptr(b))
+        return b
+
+    def close(self):
+        if self._h:
+            lib().sph_scene_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Simulation:
+    """One GPU simulation context (sph_ctx)."""
+
+    def __init__(self, desc: SceneDesc, fluid, boundary, vel=None):
+        L = lib()
+        h = C.c_void_p()
+        rc = L.sph_create(C.byref(desc), C.byref(h))
+        if rc != SPH_OK:
+            raise SphError(rc, L.sph_global_error().decode())
+        self._h = h
+        self.desc = desc
+        x = np.ascontiguousarray(fluid, np.float32).reshape(-1, 3)
+        v = None if vel is None else np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
+        b = np.ascontiguousarray(boundary, np.float32).reshape(-1, 3)
+        self._check(L.sph_set_fluid(h, x.shape[0], _fptr(x), _fptr(v)))
+        self._check(L.sph_set_boundary(h, b.shape[0], _fptr(b)))
+        self._check(L.sph_init(h))
+        self.nf, self.nb = x.shape[0], b.shape[0]
+
+    @classmethod
+    def from_scene(cls, scene: Scene, vel=None):
+        x, v = scene.fluid()
+        return cls(scene.desc(), x, scene.boundary(), v if vel is None else vel)
+
+    def _check(self, rc):
+        if rc != SPH_OK:
+            raise SphError(rc, lib().sph_last_error(self._h).decode())
+
+    def step(self, n=1):
+        s = StepStats()
+        self._check(lib().sph_step(self._h, int(n), C.byref(s)))
+        return s.as_dict()
+
+    def step_async(self, n=1):
+        self._check(lib().sph_step_async(self._h, int(n)))
+
+    def sync(self):
+        s = StepStats()
+        self._check(lib().sph_sync(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def state(self):
+        x = np.zeros((self.nf, 3), np.float32)
+        v = np.zeros((self.nf, 3), np.float32)
+        r = np.zeros(self.nf, np.float32)
+        self._check(lib().sph_get_state(self._h, _fptr(x), _fptr(v), _fptr(r)))
+        return x, v, r
+
+    def set_state(self, x=None, v=None):
+        x = None if x is None else np.ascontiguousarray(x, np.float32)
+        v = None if v is None else np.ascontiguousarray(v, np.float32)
+        self._check(lib().sph_set_state(self._h, _fptr(x), _fptr(v)))
+
+    def boundary_volume(self):
+        out = np.zeros(self.nb, np.float32)
+        self._check(lib().sph_get_boundary_volume(self._h, _fptr(out)))
+        return out
+
+    def time(self):
+        t = C.c_double()
+        dt = C.c_float()
+        self._check(lib().sph_get_time(self._h, C.byref(t), C.byref(dt)))
+        return t.value, dt.value
+
+    def phase(self, phase):
+        vec = phase in (PHASE_NONPRESSURE_ACC, PHASE_PRESSURE_ACC)
+        out = np.zeros((self.nf, 3) if vec else self.nf, np.float32)
+        self._check(lib().sph_compute_phase(self._h, int(phase), _fptr(out)))
+        return out
+
+    def neighbors(self):
+        """CSR neighbour sets (caller order): (f_off, f_idx, b_off, b_idx)."""
+        L = lib()
+        tf, tb = C.c_size_t(), C.c_size_t()
+        self._check(L.sph_debug_neighbors(self._h, None, None, 0, None, None, 0, C.byref(tf), C.byref(tb)))
+        f_off = np.zeros(self.nf + 1, np.uint32)
+        b_off = np.zeros(self.nf + 1, np.uint32)
+        f_idx = np.zeros(max(tf.value, 1), np.uint32)
+        b_idx = np.zeros(max(tb.value, 1), np.uint32)
+        self._check(L.sph_debug_neighbors(self._h, _uptr(f_off), _uptr(f_idx), f_idx.size, _uptr(b_off),
+                                          _uptr(b_idx), b_idx.size, C.byref(tf), C.byref(tb)))
+        return f_off, f_idx[: tf.value], b_off, b_idx[: tb.value]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

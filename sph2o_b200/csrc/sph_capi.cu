@@ -1,0 +1,753 @@
+/*
+ * Context management and the extern "C" entry points of include/sph2o_cuda.h.
+ *
+ * A context owns one CUDA stream and every device buffer of one scene. The
+ * step sequences mirror the reference solvers' step() order:
+ *   WCSPH  (WCSPHSolver.cpp:14-78):  neighbour search -> density + Tait EOS ->
+ *          [surface-tension normals] -> pressure + non-pressure forces +
+ *          symplectic Euler (one kernel, writes the spare buffers)
+ *   PCISPH (PCISPHSolver.cpp:20-80): neighbour search -> density ->
+ *          [normals] -> non-pressure forces -> persistent pressure solver
+ *          (predict / density / pressure / pressure force loop + integrate)
+ *   DFSPH  (DFSPHSolver.cpp:33-107): [normals] -> non-pressure forces + CFL
+ *          speed -> persistent density solver (dt update, predict v, warm
+ *          start, loop, update x) -> neighbour search -> density + alpha ->
+ *          persistent divergence solver (warm start, loop, t += dt)
+ * No step makes a host round trip; sph_step waits once at the end.
+ */
+#include "../../include/sph2o_cuda.h"
+#include "sph_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace sph;
+
+namespace {
+
+thread_local std::string g_global_error;
+
+struct DeviceBuffer {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+} // namespace
+
+struct sph_ctx {
+    sph_scene_desc desc{};
+    SimParams P{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    bool initialized = false;
+    unsigned nf = 0, nb = 0;
+    std::vector<float> h_fluid, h_vel, h_bound;
+    std::vector<void*> allocations;
+
+    /* current / spare buffers (swapped by the neighbour-search sort) */
+    float4 *pos = nullptr, *vel = nullptr, *pos2 = nullptr, *vel2 = nullptr;
+    unsigned *orig = nullptr, *orig2 = nullptr;
+    float *kws = nullptr, *kws2 = nullptr, *kvws = nullptr, *kvws2 = nullptr;
+    float4 *acc = nullptr, *normal = nullptr, *predr = nullptr, *pacc = nullptr;
+    float *rho = nullptr, *alpha = nullptr, *k = nullptr, *press = nullptr;
+    unsigned *cell_of = nullptr, *slot = nullptr, *tmp_key = nullptr, *tmp_src = nullptr, *cell_sorted = nullptr;
+    unsigned *cell_count = nullptr, *cell_start = nullptr, *bcell_start = nullptr, *block_sums = nullptr;
+    float4* bpos = nullptr;
+    float* bvol = nullptr;
+    unsigned* borig = nullptr;
+    unsigned *nbr_f = nullptr, *cnt_f = nullptr, *nbr_b = nullptr, *cnt_b = nullptr;
+    DevState* st = nullptr;
+    DevState* st_host = nullptr; /* pinned mirror */
+    double* accum = nullptr;
+    size_t accum_len = 0;
+    int grid_density = 0, grid_div = 0, grid_pcisph = 0;
+    DevState last{};
+    bool lists_valid = false;
+};
+
+namespace {
+
+int fail(sph_ctx* c, int code, const std::string& msg)
+{
+    if (c) c->err = msg;
+    else g_global_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(ctx, expr)                                                                          \
+    do {                                                                                             \
+        cudaError_t e_ = (expr);                                                                     \
+        if (e_ != cudaSuccess)                                                                       \
+            return fail(ctx, SPH_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+
+template <typename T> int dalloc(sph_ctx* c, T** p, size_t count)
+{
+    void* v = nullptr;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&v, bytes);
+    if (e != cudaSuccess) return fail(c, SPH_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    e = cudaMemsetAsync(v, 0, bytes, c->stream);
+    if (e != cudaSuccess) return fail(c, SPH_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+    c->allocations.push_back(v);
+    *p = static_cast<T*>(v);
+    return SPH_OK;
+}
+
+void free_all(sph_ctx* c)
+{
+    for (void* p : c->allocations) cudaFree(p);
+    c->allocations.clear();
+    if (c->st_host) { cudaFreeHost(c->st_host); c->st_host = nullptr; }
+}
+
+/* CubicSpline::gradW on the host, operation for operation (CubicSpline.h:52-74) */
+void host_gradW(float x, float y, float z, float h, float l, float* out)
+{
+    out[0] = out[1] = out[2] = 0.0f;
+    const float rl = std::sqrt((x * x + y * y) + z * z);
+    const float q = rl / h;
+    if (((double)rl > 1.0e-9) && (q <= 1.0f)) {
+        float gx = x / rl, gy = y / rl, gz = z / rl;
+        gx /= h; gy /= h; gz /= h;
+        float c;
+        if (q <= 0.5f) c = l * q * (3.0f * q - 2.0f);
+        else {
+            const float factor = 1.0f - q;
+            c = l * (-factor * factor);
+        }
+        out[0] = c * gx; out[1] = c * gy; out[2] = c * gz;
+    }
+}
+
+/* Kernel constants and solver parameters (SPHSimulation::initKernels / initMasses,
+   SPHSimulation.cpp:133-155; the kernels' setSupportRadius). */
+void derive_params(sph_ctx* c)
+{
+    const sph_scene_desc& d = c->desc;
+    SimParams& P = c->P;
+    const float pi = (float)M_PI;
+    P.r = d.particle_radius;
+    P.h = 4.0f * d.particle_radius;
+    const float h = P.h;
+    P.h2 = h * h;
+    P.inv_h = 1.0f / h;
+    P.rho0 = d.density0;
+    const float diameter = 2.0f * d.particle_radius;
+    const float volume = (float)std::pow((double)diameter, 3.0);
+    P.mass = d.density0 * volume;
+    const float h3 = h * h * h;
+    P.cs_k = 8.0f / (pi * h3);
+    P.cs_l = 48.0f / (pi * h3);
+    P.cs_l_h2 = P.cs_l / (h * h);
+    P.cs_l_h = P.cs_l / h;
+    const float h6 = h * h * h * h * h * h;
+    const float h9 = h * h * h * h * h * h * h * h * h;
+    P.coh_c1 = (float)(32.0 / M_PI) / h9;
+    P.coh_c2 = h6 / 64.0f;
+    P.lapl_c = 45.0f / (pi * h6);
+    P.gx = d.gravity[0]; P.gy = d.gravity[1]; P.gz = d.gravity[2];
+    P.stiffness = d.stiffness;
+    P.gamma = d.gamma;
+    P.kr_g = d.gamma != 0.0f ? d.stiffness * d.density0 / d.gamma : 0.0f;
+    P.h2_guard = (float)((double)h * (double)h * (1.0 + 1.0e-5));
+    P.eta = d.eta;
+    P.eta_v = d.eta_v;
+    P.cfl = d.cfl_factor;
+    const float min_fps_ts = 1.0f / d.fps;
+    P.min_ts = min_fps_ts < d.min_time_step ? min_fps_ts : d.min_time_step; /* TimeHelper.h:57 */
+    P.max_ts = d.max_time_step;
+    P.min_it = d.min_iterations;
+    P.max_it = d.max_iterations;
+    P.min_it_v = d.min_iterations_v;
+    P.max_it_v = d.max_iterations_v;
+    P.eps = 1.0e-5f;
+    /* forces exist only when the method is set and the coefficient non-zero
+       (SPHSimulation.cpp:380-387) */
+    P.visc_method = (d.viscosity_method > -1 && d.viscosity_method <= 2 && d.viscosity != 0.0f) ? d.viscosity_method : -1;
+    P.visc = d.viscosity;
+    P.bvisc = d.boundary_viscosity;
+    P.st_on = (d.surface_tension_method == SPH_SURFACE_TENSION_AKINCI && d.surface_tension != 0.0f) ? 1 : 0;
+    P.st = d.surface_tension;
+    P.adh_on = (d.adhesion_method == SPH_ADHESION_AKINCI && d.adhesion != 0.0f) ? 1 : 0;
+    P.adh = d.adhesion;
+    /* PCISPHSolver::computeScalingFactor (PCISPHSolver.cpp:403-436) at the initial dt */
+    float sg[3] = {0, 0, 0}, ssq = 0.0f;
+    for (int i = -1; i <= 1; i++)
+        for (int j = -1; j <= 1; j++)
+            for (int k = -1; k <= 1; k++) {
+                const float rx = (float)(-i) * diameter, ry = (float)(-j) * diameter, rz = (float)(-k) * diameter;
+                float g[3];
+                host_gradW(rx, ry, rz, h, P.cs_l, g);
+                sg[0] += g[0]; sg[1] += g[1]; sg[2] += g[2];
+                ssq += (g[0] * g[0] + g[1] * g[1]) + g[2] * g[2];
+            }
+    const float x = P.mass * d.time_step / d.density0;
+    const float beta = (float)(2.0 * std::pow((double)x, 2.0));
+    const float dot_sg = (sg[0] * sg[0] + sg[1] * sg[1]) + sg[2] * sg[2];
+    P.pcisph_delta = -1.0f / (beta * (-dot_sg - ssq));
+}
+
+DeviceArrays arrays(sph_ctx* c)
+{
+    DeviceArrays A;
+    A.pos = c->pos; A.vel = c->vel; A.pos_alt = c->pos2; A.vel_alt = c->vel2;
+    A.acc = c->acc; A.normal = c->normal; A.predr = c->predr; A.pacc = c->pacc;
+    A.rho = c->rho; A.alpha = c->alpha; A.k = c->k; A.kws = c->kws; A.kvws = c->kvws; A.press = c->press;
+    A.cell_start = c->cell_start; A.cell_sorted = c->cell_sorted;
+    A.bpos = c->bpos; A.bcell_start = c->bcell_start;
+    A.nbr_f = c->nbr_f; A.cnt_f = c->cnt_f; A.nbr_b = c->nbr_b; A.cnt_b = c->cnt_b;
+    A.accum = c->accum; A.st = c->st;
+    return A;
+}
+
+int check_launch(sph_ctx* c, const char* what)
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(c, SPH_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return SPH_OK;
+}
+
+int alloc_lists(sph_ctx* c)
+{
+    int rc;
+    if ((rc = dalloc(c, &c->nbr_f, (size_t)c->P.capF * c->nf)) != SPH_OK) return rc;
+    if ((rc = dalloc(c, &c->nbr_b, (size_t)c->P.capB * c->nf)) != SPH_OK) return rc;
+    return SPH_OK;
+}
+
+/* Sort the fluid into cells and rebuild the neighbour lists. */
+int neighbor_search(sph_ctx* c)
+{
+    GatherSet g{};
+    g.orig_out = c->orig2;
+    g.cell_out = c->cell_sorted;
+    g.v4_in[0] = c->pos; g.v4_out[0] = c->pos2;
+    g.v4_in[1] = c->vel; g.v4_out[1] = c->vel2;
+    if (c->desc.simulation_method == SPH_DFSPH) {
+        g.f_in[0] = c->kws; g.f_out[0] = c->kws2;
+        g.f_in[1] = c->kvws; g.f_out[1] = c->kvws2;
+    }
+    launch_sort(c->P, (int)c->nf, c->pos, c->cell_count, c->cell_start, c->block_sums, c->cell_of, c->slot,
+                c->tmp_key, c->tmp_src, c->orig, g, c->stream);
+    std::swap(c->pos, c->pos2);
+    std::swap(c->vel, c->vel2);
+    std::swap(c->orig, c->orig2);
+    if (c->desc.simulation_method == SPH_DFSPH) {
+        std::swap(c->kws, c->kws2);
+        std::swap(c->kvws, c->kvws2);
+    }
+    launch_build_lists(c->P, c->pos, c->cell_start, c->bpos, c->bcell_start, c->nbr_f, c->cnt_f, c->nbr_b, c->cnt_b,
+                       c->st, c->stream);
+    c->lists_valid = true;
+    return check_launch(c, "neighbour search");
+}
+
+int zero_accum(sph_ctx* c)
+{
+    CUDA_TRY(c, cudaMemsetAsync(c->accum, 0, c->accum_len * sizeof(double), c->stream));
+    return SPH_OK;
+}
+
+int step_wcsph(sph_ctx* c)
+{
+    int rc;
+    if ((rc = neighbor_search(c)) != SPH_OK) return rc;
+    DeviceArrays A = arrays(c);
+    launch_density(c->P, A, false, true, c->stream);
+    if (c->P.st_on) launch_normals(c->P, A, c->stream);
+    launch_forces(c->P, A, FORCE_WCSPH, c->stream);
+    std::swap(c->pos, c->pos2);
+    std::swap(c->vel, c->vel2);
+    c->lists_valid = false;
+    return check_launch(c, "wcsph step");
+}
+
+int step_pcisph(sph_ctx* c)
+{
+    int rc;
+    if ((rc = neighbor_search(c)) != SPH_OK) return rc;
+    DeviceArrays A = arrays(c);
+    launch_density(c->P, A, false, false, c->stream);
+    if (c->P.st_on) launch_normals(c->P, A, c->stream);
+    launch_forces(c->P, A, FORCE_NP, c->stream);
+    if ((rc = zero_accum(c)) != SPH_OK) return rc;
+    const int e = launch_pcisph_solve(c->P, A, c->grid_pcisph, c->stream);
+    if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("pcisph solver launch: ") + cudaGetErrorString((cudaError_t)e));
+    c->lists_valid = true;
+    return check_launch(c, "pcisph step");
+}
+
+int step_dfsph(sph_ctx* c)
+{
+    int rc;
+    DeviceArrays A = arrays(c);
+    if (c->P.st_on) launch_normals(c->P, A, c->stream);
+    launch_forces(c->P, A, FORCE_NP_CFL, c->stream);
+    if ((rc = zero_accum(c)) != SPH_OK) return rc;
+    int e = launch_dfsph_solve(c->P, A, false, c->grid_density, c->stream);
+    if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph density solver launch: ") + cudaGetErrorString((cudaError_t)e));
+    if ((rc = neighbor_search(c)) != SPH_OK) return rc;
+    A = arrays(c);
+    launch_density(c->P, A, true, false, c->stream);
+    A.accum = c->accum + c->accum_len / 2;
+    e = launch_dfsph_solve(c->P, A, true, c->grid_div, c->stream);
+    if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph divergence solver launch: ") + cudaGetErrorString((cudaError_t)e));
+    return check_launch(c, "dfsph step");
+}
+
+int read_state(sph_ctx* c, DevState* out)
+{
+    CUDA_TRY(c, cudaMemcpyAsync(c->st_host, c->st, sizeof(DevState), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    *out = *c->st_host;
+    return SPH_OK;
+}
+
+int status_from_state(sph_ctx* c, const DevState& s)
+{
+    if (s.err & ERRBIT_TIMEOUT) return fail(c, SPH_ERR_TIMEOUT, "a bounded device-side barrier gave up");
+    if (s.err & ERRBIT_NAN) return fail(c, SPH_ERR_NAN, "non-finite particle position");
+    if (s.err & ERRBIT_OVERFLOW) return fail(c, SPH_ERR_NEIGHBOR_OVERFLOW, "neighbour list capacity exceeded");
+    return SPH_OK;
+}
+
+/* After an overflow: clear the flag and grow the lists for later steps. */
+int recover_overflow(sph_ctx* c)
+{
+    int zero = 0;
+    unsigned uzero = 0;
+    CUDA_TRY(c, cudaMemcpyAsync(&c->st->err, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(&c->st->overflow, &uzero, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    auto drop = [&](unsigned* p) {
+        auto it = std::find(c->allocations.begin(), c->allocations.end(), (void*)p);
+        if (it != c->allocations.end()) { cudaFree(p); c->allocations.erase(it); }
+    };
+    drop(c->nbr_f);
+    drop(c->nbr_b);
+    c->P.capF = c->P.capF + c->P.capF / 2;
+    c->P.capB = c->P.capB + c->P.capB / 2;
+    c->lists_valid = false;
+    return alloc_lists(c);
+}
+
+int fill_stats(sph_ctx* c, const DevState& before, const DevState& now, sph_step_stats* out)
+{
+    if (!out) return SPH_OK;
+    std::memset(out, 0, sizeof *out);
+    out->time = now.time;
+    out->dt = now.dt;
+    out->avg_density_error = now.avg_dens;
+    out->avg_divergence_error = now.avg_div;
+    out->max_velocity = now.last_vmax;
+    out->iterations = now.its;
+    out->iterations_v = now.its_v;
+    out->total_iterations = now.sum_its - before.sum_its;
+    out->total_iterations_v = now.sum_its_v - before.sum_its_v;
+    out->steps = now.steps - before.steps;
+    out->neighbor_overflows = now.overflow;
+    (void)c;
+    return SPH_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int sph_create(const sph_scene_desc* desc, sph_ctx** out)
+{
+    if (!desc || !out) return fail(nullptr, SPH_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (desc->simulation_method < SPH_WCSPH || desc->simulation_method > SPH_DFSPH)
+        return fail(nullptr, SPH_ERR_ARG, "simulation_method must be 0, 1 or 2");
+    if (desc->boundary_method != SPH_BOUNDARY_AKINCI)
+        return fail(nullptr, SPH_ERR_ARG, "only the Akinci boundary method (2) is implemented");
+    if (!(desc->particle_radius > 0.0f) || !(desc->density0 > 0.0f) || !(desc->time_step > 0.0f) || !(desc->fps > 0.0f))
+        return fail(nullptr, SPH_ERR_ARG, "particle_radius, density0, time_step and fps must be positive");
+    if (desc->simulation_method == SPH_WCSPH && !(desc->gamma != 0.0f))
+        return fail(nullptr, SPH_ERR_ARG, "WCSPH needs a non-zero gamma");
+    if (desc->simulation_method != SPH_WCSPH && desc->max_iterations > 100000)
+        return fail(nullptr, SPH_ERR_ARG, "max_iterations above 100000");
+    if (desc->flags != 0) return fail(nullptr, SPH_ERR_ARG, "flags must be 0");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, SPH_ERR_NO_DEVICE, "no CUDA device available");
+    sph_ctx* c = new (std::nothrow) sph_ctx();
+    if (!c) return fail(nullptr, SPH_ERR_ARG, "out of host memory");
+    c->desc = *desc;
+    cudaGetDevice(&c->device);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(nullptr, SPH_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    }
+    derive_params(c);
+    *out = c;
+    return SPH_OK;
+}
+
+int sph_set_fluid(sph_ctx* c, unsigned n, const float* xyz, const float* v)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (c->initialized) return fail(c, SPH_ERR_STATE, "sph_set_fluid after sph_init; use sph_set_state");
+    if (n > 0 && !xyz) return fail(c, SPH_ERR_ARG, "null positions");
+    c->nf = n;
+    c->h_fluid.assign(xyz, xyz + 3ull * n);
+    if (v) c->h_vel.assign(v, v + 3ull * n);
+    else c->h_vel.assign(3ull * n, 0.0f);
+    return SPH_OK;
+}
+
+int sph_set_boundary(sph_ctx* c, unsigned n, const float* xyz)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (c->initialized) return fail(c, SPH_ERR_STATE, "sph_set_boundary after sph_init");
+    if (n > 0 && !xyz) return fail(c, SPH_ERR_ARG, "null positions");
+    c->nb = n;
+    c->h_bound.assign(xyz, xyz + 3ull * n);
+    return SPH_OK;
+}
+
+int sph_init(sph_ctx* c)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (c->initialized) return fail(c, SPH_ERR_STATE, "sph_init called twice");
+    if (c->nf == 0) return fail(c, SPH_ERR_ARG, "no fluid particles");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    SimParams& P = c->P;
+    P.nf = (int)c->nf;
+    P.nb = (int)c->nb;
+
+    /* grid over the particle bounding box (+ hint), 2 cells of margin */
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    auto grow = [&](const std::vector<float>& a) {
+        for (size_t i = 0; i + 2 < a.size(); i += 3)
+            for (int k = 0; k < 3; ++k) {
+                if (!std::isfinite(a[i + k])) continue;
+                lo[k] = std::min(lo[k], (double)a[i + k]);
+                hi[k] = std::max(hi[k], (double)a[i + k]);
+            }
+    };
+    grow(c->h_fluid);
+    grow(c->h_bound);
+    const sph_scene_desc& d = c->desc;
+    if (d.domain_min[0] != 0 || d.domain_min[1] != 0 || d.domain_min[2] != 0 || d.domain_max[0] != 0 ||
+        d.domain_max[1] != 0 || d.domain_max[2] != 0)
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], (double)d.domain_min[k]);
+            hi[k] = std::max(hi[k], (double)d.domain_max[k]);
+        }
+    int cmin[3], dim[3];
+    for (int k = 0; k < 3; ++k) {
+        const int a = (int)std::floor(lo[k] / P.h) - 2;
+        const int b = (int)std::floor(hi[k] / P.h) + 2;
+        cmin[k] = a;
+        dim[k] = ((b - a + 1) + 3) / 4 * 4;
+    }
+    const unsigned long long ncells = (unsigned long long)dim[0] * dim[1] * dim[2];
+    if (ncells > (1ull << 27))
+        return fail(c, SPH_ERR_CAPACITY, "domain too large: more than 2^27 grid cells of size h");
+    P.cminx = cmin[0]; P.cminy = cmin[1]; P.cminz = cmin[2];
+    P.dimx = dim[0]; P.dimy = dim[1]; P.dimz = dim[2];
+    P.nbx = dim[0] / 4; P.nby = dim[1] / 4;
+    P.ncells = (unsigned)((ncells + 4095) / 4096 * 4096);
+    P.capF = 64;
+    P.capB = 64;
+
+    const size_t nf = c->nf, nb = c->nb, nmax = std::max(nf, nb);
+    int rc = SPH_OK;
+#define ALLOC(ptr, count) if ((rc = dalloc(c, &c->ptr, (count))) != SPH_OK) return rc
+    ALLOC(pos, nf); ALLOC(vel, nf); ALLOC(pos2, nf); ALLOC(vel2, nf);
+    ALLOC(orig, nf); ALLOC(orig2, nf);
+    ALLOC(kws, nf); ALLOC(kws2, nf); ALLOC(kvws, nf); ALLOC(kvws2, nf);
+    ALLOC(acc, nf); ALLOC(rho, nf); ALLOC(alpha, nf); ALLOC(k, nf); ALLOC(press, nf);
+    ALLOC(normal, nf); ALLOC(predr, nf); ALLOC(pacc, nf);
+    ALLOC(cell_of, nmax); ALLOC(slot, nmax); ALLOC(tmp_key, nmax); ALLOC(tmp_src, nmax); ALLOC(cell_sorted, nmax);
+    ALLOC(cell_count, (size_t)P.ncells); ALLOC(cell_start, (size_t)P.ncells + 1);
+    ALLOC(bcell_start, (size_t)P.ncells + 1); ALLOC(block_sums, (size_t)P.ncells / 4096 + 1);
+    ALLOC(bpos, nb); ALLOC(bvol, nb); ALLOC(borig, nb);
+    ALLOC(cnt_f, nf); ALLOC(cnt_b, nf);
+    ALLOC(st, 1);
+#undef ALLOC
+    if ((rc = alloc_lists(c)) != SPH_OK) return rc;
+    c->accum_len = 2 * ((size_t)P.max_it + 2);
+    if ((rc = dalloc(c, &c->accum, c->accum_len)) != SPH_OK) return rc;
+    CUDA_TRY(c, cudaMallocHost((void**)&c->st_host, sizeof(DevState)));
+
+    c->grid_density = persistent_grid(false, false);
+    c->grid_div = persistent_grid(false, true);
+    c->grid_pcisph = persistent_grid(true, false);
+    if (c->grid_density <= 0 || c->grid_div <= 0 || c->grid_pcisph <= 0)
+        return fail(c, SPH_ERR_CUDA, "cannot size the persistent solver grid");
+
+    /* upload: fluid in caller order becomes the first "unsorted" state */
+    float* stage = nullptr;
+    const size_t stage_n = 3 * std::max<size_t>(nmax, 1);
+    CUDA_TRY(c, cudaMalloc(&stage, stage_n * sizeof(float)));
+    c->allocations.push_back(stage);
+    CUDA_TRY(c, cudaMemcpyAsync(stage, c->h_fluid.data(), 3 * nf * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    launch_pack_v3((int)nf, stage, c->pos, 0.0f, c->stream);
+    CUDA_TRY(c, cudaMemcpyAsync(stage, c->h_vel.data(), 3 * nf * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    launch_pack_v3((int)nf, stage, c->vel, 0.0f, c->stream);
+    launch_iota((int)nf, c->orig, c->stream);
+
+    /* boundary: sort once, volumes (SPHSolver::init, SPHSolver.cpp:21-38) */
+    if (nb > 0) {
+        float4* braw = nullptr;
+        unsigned* bid = nullptr;
+        if ((rc = dalloc(c, &braw, nb)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &bid, nb)) != SPH_OK) return rc;
+        CUDA_TRY(c, cudaMemcpyAsync(stage, c->h_bound.data(), 3 * nb * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        launch_pack_v3((int)nb, stage, braw, 0.0f, c->stream);
+        launch_iota((int)nb, bid, c->stream);
+        GatherSet g{};
+        g.orig_out = c->borig;
+        g.v4_in[0] = braw;
+        g.v4_out[0] = c->bpos;
+        launch_sort(P, (int)nb, braw, c->cell_count, c->bcell_start, c->block_sums, c->cell_of, c->slot, c->tmp_key,
+                    c->tmp_src, bid, g, c->stream);
+        launch_boundary_volume(P, c->bpos, c->bcell_start, c->bvol, c->stream);
+    } else {
+        CUDA_TRY(c, cudaMemsetAsync(c->bcell_start, 0, ((size_t)P.ncells + 1) * sizeof(unsigned), c->stream));
+    }
+
+    /* solver state */
+    DevState s0{};
+    s0.dt = d.time_step;
+    CUDA_TRY(c, cudaMemcpyAsync(c->st, &s0, sizeof s0, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = neighbor_search(c)) != SPH_OK) return rc;
+    if (d.simulation_method == SPH_DFSPH) {
+        /* DFSPHSolver::init: densities and alpha at the initial positions */
+        launch_density(P, arrays(c), true, false, c->stream);
+    }
+    if ((rc = check_launch(c, "init")) != SPH_OK) return rc;
+    DevState now{};
+    if ((rc = read_state(c, &now)) != SPH_OK) return rc;
+    c->last = now;
+    c->initialized = true;
+    if ((rc = status_from_state(c, now)) != SPH_OK) return rc;
+    return SPH_OK;
+}
+
+int sph_step_async(sph_ctx* c, int nsteps)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_step before sph_init");
+    if (nsteps < 0) return fail(c, SPH_ERR_ARG, "negative step count");
+    for (int s = 0; s < nsteps; ++s) {
+        int rc;
+        switch (c->desc.simulation_method) {
+        case SPH_WCSPH: rc = step_wcsph(c); break;
+        case SPH_PCISPH: rc = step_pcisph(c); break;
+        default: rc = step_dfsph(c); break;
+        }
+        if (rc != SPH_OK) return rc;
+    }
+    return SPH_OK;
+}
+
+int sph_sync(sph_ctx* c, sph_step_stats* out)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_sync before sph_init");
+    DevState now{};
+    int rc = read_state(c, &now);
+    if (rc != SPH_OK) return rc;
+    fill_stats(c, c->last, now, out);
+    c->last = now;
+    rc = status_from_state(c, now);
+    if (rc == SPH_ERR_NEIGHBOR_OVERFLOW) {
+        const int r2 = recover_overflow(c);
+        if (r2 != SPH_OK) return r2;
+        c->last.err = 0;
+        c->last.overflow = 0;
+        c->err = "neighbour list capacity exceeded; capacity grown for later steps";
+    }
+    return rc;
+}
+
+int sph_step(sph_ctx* c, int nsteps, sph_step_stats* out)
+{
+    const int rc = sph_step_async(c, nsteps);
+    if (rc != SPH_OK) return rc;
+    return sph_sync(c, out);
+}
+
+int sph_get_state(sph_ctx* c, float* xyz, float* v, float* rho)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_get_state before sph_init");
+    const size_t nf = c->nf;
+    float* tmp = nullptr;
+    CUDA_TRY(c, cudaMallocAsync((void**)&tmp, 3 * nf * sizeof(float), c->stream));
+    int rc = SPH_OK;
+    auto copy_out = [&](float* dst, size_t count) -> int {
+        CUDA_TRY(c, cudaMemcpyAsync(dst, tmp, count * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        return SPH_OK;
+    };
+    if (xyz) { launch_unsort_v4((int)nf, c->orig, c->pos, tmp, c->stream); rc = copy_out(xyz, 3 * nf); }
+    if (rc == SPH_OK && v) { launch_unsort_v4((int)nf, c->orig, c->vel, tmp, c->stream); rc = copy_out(v, 3 * nf); }
+    if (rc == SPH_OK && rho) { launch_unsort_f((int)nf, c->orig, c->rho, tmp, c->stream); rc = copy_out(rho, nf); }
+    cudaFreeAsync(tmp, c->stream);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (rc != SPH_OK) return rc;
+    return check_launch(c, "get_state");
+}
+
+int sph_set_state(sph_ctx* c, const float* xyz, const float* v)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_set_state before sph_init");
+    const size_t nf = c->nf;
+    float* tmp = nullptr;
+    CUDA_TRY(c, cudaMallocAsync((void**)&tmp, 3 * nf * sizeof(float), c->stream));
+    if (xyz) {
+        CUDA_TRY(c, cudaMemcpyAsync(tmp, xyz, 3 * nf * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        launch_sort_v3((int)nf, c->orig, tmp, c->pos, c->stream);
+    }
+    if (v) {
+        CUDA_TRY(c, cudaMemcpyAsync(tmp, v, 3 * nf * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        launch_sort_v3((int)nf, c->orig, tmp, c->vel, c->stream);
+    }
+    cudaFreeAsync(tmp, c->stream);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->lists_valid = false;
+    if (xyz && c->desc.simulation_method == SPH_DFSPH) {
+        /* DFSPH keeps densities/alpha of the current positions between steps */
+        int rc = neighbor_search(c);
+        if (rc != SPH_OK) return rc;
+        launch_density(c->P, arrays(c), true, false, c->stream);
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    }
+    return check_launch(c, "set_state");
+}
+
+int sph_get_boundary_volume(sph_ctx* c, float* vol)
+{
+    if (!c || !vol) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_get_boundary_volume before sph_init");
+    if (c->nb == 0) return SPH_OK;
+    float* tmp = nullptr;
+    CUDA_TRY(c, cudaMallocAsync((void**)&tmp, c->nb * sizeof(float), c->stream));
+    launch_unsort_f((int)c->nb, c->borig, c->bvol, tmp, c->stream);
+    CUDA_TRY(c, cudaMemcpyAsync(vol, tmp, c->nb * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    cudaFreeAsync(tmp, c->stream);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_launch(c, "get_boundary_volume");
+}
+
+int sph_get_time(sph_ctx* c, double* time, float* dt)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_get_time before sph_init");
+    DevState s{};
+    const int rc = read_state(c, &s);
+    if (rc != SPH_OK) return rc;
+    if (time) *time = s.time;
+    if (dt) *dt = s.dt;
+    return SPH_OK;
+}
+
+unsigned sph_num_fluid(const sph_ctx* c) { return c ? c->nf : 0u; }
+unsigned sph_num_boundary(const sph_ctx* c) { return c ? c->nb : 0u; }
+const char* sph_last_error(const sph_ctx* c) { return c ? c->err.c_str() : "null context"; }
+const char* sph_global_error(void) { return g_global_error.c_str(); }
+
+int sph_destroy(sph_ctx* c)
+{
+    if (!c) return SPH_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_all(c);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return SPH_OK;
+}
+
+int sph_compute_phase(sph_ctx* c, int phase, float* out)
+{
+    if (!c || !out) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_compute_phase before sph_init");
+    if (phase < SPH_PHASE_DENSITY || phase > SPH_PHASE_PRESSURE_ACC) return fail(c, SPH_ERR_ARG, "unknown phase");
+    if ((phase == SPH_PHASE_PRESSURE || phase == SPH_PHASE_PRESSURE_ACC) && c->desc.simulation_method != SPH_WCSPH)
+        return fail(c, SPH_ERR_ARG, "pressure phases exist for WCSPH only");
+    int rc = neighbor_search(c);
+    if (rc != SPH_OK) return rc;
+    DeviceArrays A = arrays(c);
+    const bool eos = phase == SPH_PHASE_PRESSURE || phase == SPH_PHASE_PRESSURE_ACC;
+    launch_density(c->P, A, phase == SPH_PHASE_ALPHA || c->desc.simulation_method == SPH_DFSPH, eos, c->stream);
+    const size_t nf = c->nf;
+    float* tmp = nullptr;
+    CUDA_TRY(c, cudaMallocAsync((void**)&tmp, 3 * nf * sizeof(float), c->stream));
+    size_t count = nf;
+    switch (phase) {
+    case SPH_PHASE_DENSITY: launch_unsort_f((int)nf, c->orig, c->rho, tmp, c->stream); break;
+    case SPH_PHASE_ALPHA: launch_unsort_f((int)nf, c->orig, c->alpha, tmp, c->stream); break;
+    case SPH_PHASE_PRESSURE: launch_unsort_f((int)nf, c->orig, c->press, tmp, c->stream); break;
+    case SPH_PHASE_NONPRESSURE_ACC:
+        if (c->P.st_on) launch_normals(c->P, A, c->stream);
+        launch_forces(c->P, A, FORCE_NP, c->stream);
+        launch_unsort_v4((int)nf, c->orig, c->acc, tmp, c->stream);
+        count = 3 * nf;
+        break;
+    default:
+        launch_forces(c->P, A, FORCE_PRESSURE, c->stream);
+        launch_unsort_v4((int)nf, c->orig, c->acc, tmp, c->stream);
+        count = 3 * nf;
+        break;
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(out, tmp, count * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    if (phase == SPH_PHASE_NONPRESSURE_ACC || phase == SPH_PHASE_PRESSURE_ACC)
+        CUDA_TRY(c, cudaMemsetAsync(c->acc, 0, nf * sizeof(float4), c->stream));
+    cudaFreeAsync(tmp, c->stream);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_launch(c, "compute_phase");
+}
+
+int sph_debug_neighbors(sph_ctx* c, unsigned* f_offsets, unsigned* f_index, size_t f_cap, unsigned* b_offsets,
+                        unsigned* b_index, size_t b_cap, size_t* nf_total, size_t* nb_total)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_debug_neighbors before sph_init");
+    int rc = neighbor_search(c);
+    if (rc != SPH_OK) return rc;
+    const size_t nf = c->nf, nb = c->nb;
+    std::vector<unsigned> cntf(nf), cntb(nf), orig(nf), borig(nb);
+    std::vector<unsigned> nbrf((size_t)c->P.capF * nf), nbrb((size_t)c->P.capB * nf);
+    CUDA_TRY(c, cudaMemcpyAsync(cntf.data(), c->cnt_f, nf * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(cntb.data(), c->cnt_b, nf * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(orig.data(), c->orig, nf * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (nb) CUDA_TRY(c, cudaMemcpyAsync(borig.data(), c->borig, nb * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(nbrf.data(), c->nbr_f, nbrf.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(nbrb.data(), c->nbr_b, nbrb.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    DevState s{};
+    if ((rc = read_state(c, &s)) != SPH_OK) return rc;
+    if (s.err & ERRBIT_OVERFLOW) return fail(c, SPH_ERR_NEIGHBOR_OVERFLOW, "neighbour list capacity exceeded");
+    std::vector<size_t> slot_of(nf);
+    for (size_t i = 0; i < nf; ++i) slot_of[orig[i]] = i;
+    size_t tf = 0, tb = 0;
+    for (size_t o = 0; o < nf; ++o) {
+        const size_t i = slot_of[o];
+        if (f_offsets) f_offsets[o] = (unsigned)tf;
+        if (b_offsets) b_offsets[o] = (unsigned)tb;
+        for (unsigned k = 0; k < cntf[i]; ++k, ++tf)
+            if (f_index && tf < f_cap) f_index[tf] = orig[nbrf[(size_t)k * nf + i]];
+        for (unsigned k = 0; k < cntb[i]; ++k, ++tb)
+            if (b_index && tb < b_cap) b_index[tb] = borig[nbrb[(size_t)k * nf + i]];
+    }
+    if (f_offsets) f_offsets[nf] = (unsigned)tf;
+    if (b_offsets) b_offsets[nf] = (unsigned)tb;
+    if (nf_total) *nf_total = tf;
+    if (nb_total) *nb_total = tb;
+    if ((f_index && tf > f_cap) || (b_index && tb > b_cap)) return fail(c, SPH_ERR_ARG, "index arrays too small");
+    return SPH_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,353 @@
+/*
+ * Neighbour search on the GPU: the B200 replacement of SPH2O's spatial hash
+ * (HashTable::insertFluidParticle / neighborhoodSearch, src/SPH2O/HashTable.cpp:3-86;
+ * SPHSolver::insertFluidParticles / neighborhoodSearch, src/SPH2O/SPHSolver/SPHSolver.cpp:170-219).
+ *
+ * Per step:
+ *   1. ns_count        cell key floor(x / h) -> brick-Morton cell index,
+ *                      per-cell population by atomicAdd (slot = old count)
+ *   2. scan_*          exclusive scan of the populations -> cellStart[ncells+1]
+ *                      (the scan zeroes the populations for the next step)
+ *   3. ns_scatter      (orig id, source index) into its cell segment
+ *   4. ns_rank_gather  rank inside the cell by orig id (deterministic, equal
+ *                      to the reference's insertion order: ascending index),
+ *                      then gather the carried state into sorted order
+ *   5. ns_build_lists  for each particle, the 27 cells in the reference's
+ *                      offset order (x outermost, HashTable.cpp:59-65), keep
+ *                      candidates with |xi - xj| <= h (exact IEEE test), in
+ *                      column-major neighbour lists
+ * The static boundary is sorted once at init with steps 1-4 into its own
+ * cellStart table, and AkinciBoundaryObject::computeVolume
+ * (src/SPH2O/BoundaryObject/AkinciBoundaryObject.cpp:10-34) runs on it.
+ */
+#include "sph_device.cuh"
+#include "sph_internal.h"
+
+namespace sph {
+
+__global__ void __launch_bounds__(256) k_ns_count(SimParams P, int n, const float4* __restrict__ pos,
+                                                  unsigned* __restrict__ cell_count, unsigned* __restrict__ cell_of,
+                                                  unsigned* __restrict__ slot)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned c = cell_index(pos[i], P);
+    cell_of[i] = c;
+    slot[i] = atomicAdd(&cell_count[c], 1u);
+}
+
+/* Exclusive scan, phase 1: each 1024-thread block scans 4096 populations,
+   writes block-local exclusive offsets and zeroes the populations. */
+__global__ void __launch_bounds__(1024) k_scan_local(unsigned* __restrict__ count, unsigned* __restrict__ start,
+                                                     unsigned* __restrict__ block_sums)
+{
+    __shared__ unsigned warp_tot[32];
+    const size_t base = (size_t)blockIdx.x * 4096 + (size_t)threadIdx.x * 4;
+    uint4 c = *reinterpret_cast<const uint4*>(count + base);
+    *reinterpret_cast<uint4*>(count + base) = make_uint4(0, 0, 0, 0);
+    const unsigned t = c.x + c.y + c.z + c.w;
+    unsigned incl = t;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned w = warp_tot[lane];
+        unsigned wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned v = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += v;
+        }
+        warp_tot[lane] = wi - w;
+        if (lane == 31) block_sums[blockIdx.x] = wi;
+    }
+    __syncthreads();
+    const unsigned ex = warp_tot[wid] + incl - t;
+    *reinterpret_cast<uint4*>(start + base) = make_uint4(ex, ex + c.x, ex + c.x + c.y, ex + c.x + c.y + c.z);
+}
+
+/* Phase 2: one block scans the block totals (any count, 1024 at a time). */
+__global__ void __launch_bounds__(1024) k_scan_blocks(unsigned* __restrict__ block_sums, int nblocks,
+                                                      unsigned* __restrict__ total_out)
+{
+    __shared__ unsigned warp_tot[32];
+    __shared__ unsigned carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int base = 0; base < nblocks; base += 1024) {
+        const int i = base + threadIdx.x;
+        const unsigned v0 = i < nblocks ? block_sums[i] : 0u;
+        unsigned incl = v0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) warp_tot[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            const unsigned w = warp_tot[lane];
+            unsigned wi = w;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned v = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += v;
+            }
+            warp_tot[lane] = wi - w;
+        }
+        __syncthreads();
+        const unsigned ex = carry + warp_tot[wid] + incl - v0;
+        if (i < nblocks) block_sums[i] = ex;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = ex + v0;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total_out = carry;
+}
+
+/* Phase 3: add the block offsets. */
+__global__ void __launch_bounds__(1024) k_scan_add(unsigned* __restrict__ start, const unsigned* __restrict__ block_sums)
+{
+    const size_t base = (size_t)blockIdx.x * 4096 + (size_t)threadIdx.x * 4;
+    const unsigned off = block_sums[blockIdx.x];
+    uint4 s = *reinterpret_cast<uint4*>(start + base);
+    s.x += off; s.y += off; s.z += off; s.w += off;
+    *reinterpret_cast<uint4*>(start + base) = s;
+}
+
+__global__ void __launch_bounds__(256) k_ns_scatter(int n, const unsigned* __restrict__ cell_of,
+                                                    const unsigned* __restrict__ slot,
+                                                    const unsigned* __restrict__ cell_start,
+                                                    const unsigned* __restrict__ orig,
+                                                    unsigned* __restrict__ tmp_key, unsigned* __restrict__ tmp_src)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned p = cell_start[cell_of[i]] + slot[i];
+    tmp_key[p] = orig[i];
+    tmp_src[p] = (unsigned)i;
+}
+
+/* Rank inside the cell by caller-order id, then move the carried state. */
+__global__ void __launch_bounds__(256) k_ns_rank_gather(int n, const unsigned* __restrict__ cell_of,
+                                                        const unsigned* __restrict__ cell_start,
+                                                        const unsigned* __restrict__ tmp_key,
+                                                        const unsigned* __restrict__ tmp_src, GatherSet g)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const unsigned src = tmp_src[p];
+    const unsigned c = cell_of[src];
+    const unsigned key = tmp_key[p];
+    const unsigned s = cell_start[c], e = cell_start[c + 1];
+    unsigned rank = 0;
+    for (unsigned q = s; q < e; ++q) rank += tmp_key[q] < key ? 1u : 0u;
+    const unsigned dst = s + rank;
+    g.orig_out[dst] = key;
+    if (g.cell_out) g.cell_out[dst] = c;
+    if (g.v4_in[0]) g.v4_out[0][dst] = g.v4_in[0][src];
+    if (g.v4_in[1]) g.v4_out[1][dst] = g.v4_in[1][src];
+    if (g.f_in[0]) g.f_out[0][dst] = g.f_in[0][src];
+    if (g.f_in[1]) g.f_out[1][dst] = g.f_in[1][src];
+}
+
+/* Neighbour lists in the reference's candidate order, filtered at |r| <= h. */
+__global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, const float4* __restrict__ pos,
+                                                        const unsigned* __restrict__ cell_start,
+                                                        const float4* __restrict__ bpos,
+                                                        const unsigned* __restrict__ bcell_start,
+                                                        unsigned* __restrict__ nbr_f, unsigned* __restrict__ cnt_f,
+                                                        unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b,
+                                                        DevState* st)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.nf) return;
+    const float4 xi = pos[i];
+    const int cx = cell_coord(xi.x, P.h, P.cminx, P.dimx);
+    const int cy = cell_coord(xi.y, P.h, P.cminy, P.dimy);
+    const int cz = cell_coord(xi.z, P.h, P.cminz, P.dimz);
+    const size_t nf = (size_t)P.nf;
+    unsigned nF = 0, nB = 0;
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int x = cx + dx;
+        if (x < 0 || x >= P.dimx) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = cy + dy;
+            if (y < 0 || y >= P.dimy) continue;
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int z = cz + dz;
+                if (z < 0 || z >= P.dimz) continue;
+                const unsigned c = brick_morton(x, y, z, P);
+                const unsigned s = cell_start[c], e = cell_start[c + 1];
+                for (unsigned q = s; q < e; ++q) {
+                    if (within_h_exact(xi, pos[q], P.h)) {
+                        if (nF < P.capF) nbr_f[(size_t)nF * nf + i] = q;
+                        ++nF;
+                    }
+                }
+                if (P.nb > 0) {
+                    const unsigned bs = bcell_start[c], be = bcell_start[c + 1];
+                    for (unsigned q = bs; q < be; ++q) {
+                        if (within_h_exact(xi, bpos[q], P.h)) {
+                            if (nB < P.capB) nbr_b[(size_t)nB * nf + i] = q;
+                            ++nB;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    cnt_f[i] = min(nF, P.capF);
+    cnt_b[i] = min(nB, P.capB);
+    if (nF > P.capF || nB > P.capB) {
+        atomicAdd(&st->overflow, 1u);
+        atomicOr(&st->err, ERRBIT_OVERFLOW);
+    }
+}
+
+/* Akinci boundary volume V_b = 1 / sum_b' W(x_b - x_b') over the 27 cells
+   (AkinciBoundaryObject.cpp:10-34); k_boundary_psi then stores
+   psi = rho0 V_b in bpos.w for the fluid kernels. */
+__global__ void __launch_bounds__(128) k_boundary_volume(SimParams P, const float4* __restrict__ bpos,
+                                                         const unsigned* __restrict__ bcell_start,
+                                                         float* __restrict__ bvol)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= P.nb) return;
+    const float4 xb = bpos[b];
+    const int cx = cell_coord(xb.x, P.h, P.cminx, P.dimx);
+    const int cy = cell_coord(xb.y, P.h, P.cminy, P.dimy);
+    const int cz = cell_coord(xb.z, P.h, P.cminz, P.dimz);
+    float delta = 0.0f;
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int x = cx + dx;
+        if (x < 0 || x >= P.dimx) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = cy + dy;
+            if (y < 0 || y >= P.dimy) continue;
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int z = cz + dz;
+                if (z < 0 || z >= P.dimz) continue;
+                const unsigned c = brick_morton(x, y, z, P);
+                for (unsigned q = bcell_start[c]; q < bcell_start[c + 1]; ++q) {
+                    const float s2 = dist2_exact(xb, bpos[q]);
+                    if (s2 <= P.h2_guard) delta = __fadd_rn(delta, cs_W_exact(s2, P));
+                }
+            }
+        }
+    }
+    bvol[b] = __fdiv_rn(1.0f, delta);
+}
+
+__global__ void __launch_bounds__(256) k_boundary_psi(SimParams P, float4* __restrict__ bpos,
+                                                      const float* __restrict__ bvol)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < P.nb) bpos[b].w = __fmul_rn(P.rho0, bvol[b]);
+}
+
+/* out[orig[i]] = in[i]: sorted order -> caller order */
+__global__ void k_unsort_v4(int n, const unsigned* __restrict__ orig, const float4* __restrict__ in,
+                            float* __restrict__ out3)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 v = in[i];
+    const size_t o = (size_t)orig[i] * 3;
+    out3[o] = v.x;
+    out3[o + 1] = v.y;
+    out3[o + 2] = v.z;
+}
+
+__global__ void k_unsort_f(int n, const unsigned* __restrict__ orig, const float* __restrict__ in,
+                           float* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[orig[i]] = in[i];
+}
+
+/* caller order -> sorted slots (set_state between steps) */
+__global__ void k_sort_v3(int n, const unsigned* __restrict__ orig, const float* __restrict__ in3,
+                          float4* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t o = (size_t)orig[i] * 3;
+    out[i] = make_float4(in3[o], in3[o + 1], in3[o + 2], 0.0f);
+}
+
+__global__ void k_pack_v3(int n, const float* __restrict__ in3, float4* __restrict__ out, float w)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = make_float4(in3[3 * (size_t)i], in3[3 * (size_t)i + 1], in3[3 * (size_t)i + 2], w);
+}
+
+__global__ void k_iota(int n, unsigned* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (unsigned)i;
+}
+
+static inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
+
+void launch_sort(const SimParams& P, int n, const float4* pos_for_keys, unsigned* cell_count, unsigned* cell_start,
+                 unsigned* block_sums, unsigned* cell_of, unsigned* slot, unsigned* tmp_key, unsigned* tmp_src,
+                 const unsigned* orig_in, const GatherSet& g, cudaStream_t s)
+{
+    if (n <= 0) {
+        /* an empty set still needs an all-zero start table */
+        cudaMemsetAsync(cell_start, 0, ((size_t)P.ncells + 1) * sizeof(unsigned), s);
+        return;
+    }
+    k_ns_count<<<blocks_for(n, 256), 256, 0, s>>>(P, n, pos_for_keys, cell_count, cell_of, slot);
+    const int nblk = (int)(P.ncells / 4096);
+    k_scan_local<<<nblk, 1024, 0, s>>>(cell_count, cell_start, block_sums);
+    k_scan_blocks<<<1, 1024, 0, s>>>(block_sums, nblk, cell_start + P.ncells);
+    k_scan_add<<<nblk, 1024, 0, s>>>(cell_start, block_sums);
+    k_ns_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, cell_of, slot, cell_start, orig_in, tmp_key, tmp_src);
+    k_ns_rank_gather<<<blocks_for(n, 256), 256, 0, s>>>(n, cell_of, cell_start, tmp_key, tmp_src, g);
+}
+
+void launch_build_lists(const SimParams& P, const float4* pos, const unsigned* cell_start, const float4* bpos,
+                        const unsigned* bcell_start, unsigned* nbr_f, unsigned* cnt_f, unsigned* nbr_b,
+                        unsigned* cnt_b, DevState* st, cudaStream_t s)
+{
+    if (P.nf <= 0) return;
+    k_ns_build_lists<<<blocks_for(P.nf, 128), 128, 0, s>>>(P, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f,
+                                                            nbr_b, cnt_b, st);
+}
+
+void launch_boundary_volume(const SimParams& P, float4* bpos, const unsigned* bcell_start, float* bvol,
+                            cudaStream_t s)
+{
+    if (P.nb <= 0) return;
+    k_boundary_volume<<<blocks_for(P.nb, 128), 128, 0, s>>>(P, bpos, bcell_start, bvol);
+    k_boundary_psi<<<blocks_for(P.nb, 256), 256, 0, s>>>(P, bpos, bvol);
+}
+
+void launch_unsort_v4(int n, const unsigned* orig, const float4* in, float* out3, cudaStream_t s)
+{
+    if (n > 0) k_unsort_v4<<<blocks_for(n, 256), 256, 0, s>>>(n, orig, in, out3);
+}
+void launch_unsort_f(int n, const unsigned* orig, const float* in, float* out, cudaStream_t s)
+{
+    if (n > 0) k_unsort_f<<<blocks_for(n, 256), 256, 0, s>>>(n, orig, in, out);
+}
+void launch_sort_v3(int n, const unsigned* orig, const float* in3, float4* out, cudaStream_t s)
+{
+    if (n > 0) k_sort_v3<<<blocks_for(n, 256), 256, 0, s>>>(n, orig, in3, out);
+}
+void launch_pack_v3(int n, const float* in3, float4* out, float w, cudaStream_t s)
+{
+    if (n > 0) k_pack_v3<<<blocks_for(n, 256), 256, 0, s>>>(n, in3, out, w);
+}
+void launch_iota(int n, unsigned* out, cudaStream_t s)
+{
+    if (n > 0) k_iota<<<blocks_for(n, 256), 256, 0, s>>>(n, out);
+}
+
+} // namespace sph

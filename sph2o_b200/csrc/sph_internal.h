@@ -1,0 +1,87 @@
+/*
+ * Host-side declarations of the kernel launchers (one CUDA stream each).
+ * Kernels live in sph_grid.cu (neighbour search, sort, boundary volumes) and
+ * sph_solvers.cu (density, forces, WCSPH / PCISPH / DFSPH steps).
+ */
+#ifndef SPH2O_INTERNAL_H
+#define SPH2O_INTERNAL_H
+
+#include <cuda_runtime.h>
+
+#include "sph_device.cuh"
+
+namespace sph {
+
+/* Arrays moved by the rank/gather step of the sort (NULL entries skipped). */
+struct GatherSet {
+    unsigned* orig_out;
+    unsigned* cell_out;
+    const float4* v4_in[2];
+    float4* v4_out[2];
+    const float* f_in[2];
+    float* f_out[2];
+};
+
+/* Device pointers of one scene, handed to the solver launchers. */
+struct DeviceArrays {
+    float4* pos;
+    float4* vel;
+    float4* pos_alt;      /* WCSPH integrate target */
+    float4* vel_alt;
+    float4* acc;
+    float4* normal;
+    float4* predr;        /* PCISPH predicted position */
+    float4* pacc;         /* PCISPH pressure acceleration */
+    float* rho;
+    float* alpha;
+    float* k;
+    float* kws;
+    float* kvws;
+    float* press;
+    const unsigned* cell_start;
+    const unsigned* cell_sorted;   /* cell index of each sorted slot */
+    const float4* bpos;
+    const unsigned* bcell_start;
+    const unsigned* nbr_f;
+    const unsigned* cnt_f;
+    const unsigned* nbr_b;
+    const unsigned* cnt_b;
+    double* accum;        /* per-iteration residual accumulators, zeroed per solve */
+    DevState* st;
+};
+
+/* sph_grid.cu */
+void launch_sort(const SimParams& P, int n, const float4* pos_for_keys, unsigned* cell_count, unsigned* cell_start,
+                 unsigned* block_sums, unsigned* cell_of, unsigned* slot, unsigned* tmp_key, unsigned* tmp_src,
+                 const unsigned* orig_in, const GatherSet& g, cudaStream_t s);
+void launch_build_lists(const SimParams& P, const float4* pos, const unsigned* cell_start, const float4* bpos,
+                        const unsigned* bcell_start, unsigned* nbr_f, unsigned* cnt_f, unsigned* nbr_b,
+                        unsigned* cnt_b, DevState* st, cudaStream_t s);
+void launch_boundary_volume(const SimParams& P, float4* bpos, const unsigned* bcell_start, float* bvol,
+                            cudaStream_t s);
+void launch_unsort_v4(int n, const unsigned* orig, const float4* in, float* out3, cudaStream_t s);
+void launch_unsort_f(int n, const unsigned* orig, const float* in, float* out, cudaStream_t s);
+void launch_sort_v3(int n, const unsigned* orig, const float* in3, float4* out, cudaStream_t s);
+void launch_pack_v3(int n, const float* in3, float4* out, float w, cudaStream_t s);
+void launch_iota(int n, unsigned* out, cudaStream_t s);
+
+/* sph_solvers.cu */
+enum ForceMode : int {
+    FORCE_NP = 0,          /* non-pressure forces -> acc                      */
+    FORCE_NP_CFL = 1,      /* + DFSPH CFL speed |v + (a + g) dt| -> st->vmax   */
+    FORCE_WCSPH = 2,       /* pressure + non-pressure + symplectic Euler       */
+    FORCE_PRESSURE = 3     /* pressure acceleration only -> acc (phase access) */
+};
+
+void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool eos, cudaStream_t s);
+void launch_normals(const SimParams& P, const DeviceArrays& A, cudaStream_t s);
+void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, cudaStream_t s);
+int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s);
+int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s);
+/* co-resident grid size of the persistent solver kernels (0 on error) */
+int persistent_grid(bool pcisph, bool divergence);
+constexpr int kSolverBlock = 256;
+
+} // namespace sph
+
+#endif

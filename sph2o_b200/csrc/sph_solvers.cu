@@ -1,0 +1,649 @@
+/*
+ * Particle-pass kernels of the WCSPH / PCISPH / DFSPH steps (sm_100a).
+ *
+ * Every pass is one thread per fluid particle walking that particle's
+ * neighbour lists (built once per step by sph_grid.cu); positions and
+ * velocities of neighbours are gathered as float4 from the cell-sorted
+ * arrays, so a warp's gathers fall on a few cache lines of nearby cells.
+ * The DFSPH and PCISPH iteration loops each run as ONE persistent,
+ * cooperative kernel: phases are separated by a bounded grid barrier and
+ * the convergence residual is reduced in FP64 on the device (warp shuffles,
+ * a block reduction, one atomicAdd per block), so no host round trip occurs
+ * inside a step.
+ *
+ * Reference correspondence (file:line in SPH2O):
+ *   k_density            SPHSolver::computeFluidDensities     SPHSolver.cpp:42-89
+ *                        DFSPHSolver::computeAlpha            DFSPHSolver.cpp:109-178
+ *                        WCSPHSolver::computeFluidPressures   WCSPHSolver.cpp:80-95
+ *   k_normals            SurfaceTensionAkinci::step, pass 1   SurfaceTensionAkinci.cpp:14-31
+ *   k_forces             ArtificialViscosity::step            ArtificialViscosity.cpp:6-54
+ *                        StandardViscosityForce::step         StandardViscosity.cpp:5-50
+ *                        XSPHViscosity::step                  XSPHViscosity.cpp:6-43
+ *                        SurfaceTensionAkinci::step, pass 2   SurfaceTensionAkinci.cpp:33-70
+ *                        AdhesionForce::step                  AdhesionForce.cpp:5-33
+ *                        WCSPHSolver::computePressureForce    WCSPHSolver.cpp:132-188
+ *                        SPHSolver::integrate                 SPHSolver.cpp:139-168
+ *   k_dfsph_solve<false> updateTimeStep, predictVelocities, densityWarmStart,
+ *                        correctDensityError, updatePositions DFSPHSolver.cpp:1090-1162,
+ *                                                              180-224, 851-955, 414-536
+ *   k_dfsph_solve<true>  divergenceWarmStart, correctDivergenceError,
+ *                        computeDivergenceError               DFSPHSolver.cpp:957-1059, 730-849, 538-621
+ *   k_pcisph_solve       initPressure, pressureSolver, predictVelocityAndPosition,
+ *                        predictFluidDensities, updatePressure, computePressureAcc,
+ *                        integrate                            PCISPHSolver.cpp:82-401, 459-488
+ */
+#include "sph_device.cuh"
+#include "sph_internal.h"
+
+
+
+namespace sph {
+
+struct Pair {
+    float rx, ry, rz, s, rl, inv_rl;
+};
+
+__device__ __forceinline__ Pair make_pair(float4 a, float4 b)
+{
+    Pair p;
+    p.rx = a.x - b.x;
+    p.ry = a.y - b.y;
+    p.rz = a.z - b.z;
+    p.s = (p.rx * p.rx + p.ry * p.ry) + p.rz * p.rz;
+    len_inv(p.s, p.rl, p.inv_rl);
+    return p;
+}
+
+/* ---------------------------------------------------------------------- */
+
+template <bool ALPHA, bool EOS>
+__global__ void __launch_bounds__(256) k_density(SimParams P, DeviceArrays A)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.nf) return;
+    const size_t nf = (size_t)P.nf;
+    const float4 xi = A.pos[i];
+    float rho = 0.0f, sgx = 0.0f, sgy = 0.0f, sgz = 0.0f, ssq = 0.0f;
+    const unsigned nF = A.cnt_f[i];
+    for (unsigned kk = 0; kk < nF; ++kk) {
+        const unsigned j = A.nbr_f[kk * nf + i];
+        const float4 xj = A.pos[j];
+        rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(dist2_exact(xi, xj), P)));
+        if (ALPHA) {
+            const Pair p = make_pair(xi, xj);
+            const float f = P.mass * cs_gradf(p.rl, p.inv_rl, P);
+            const float gx = f * p.rx, gy = f * p.ry, gz = f * p.rz;
+            sgx += gx; sgy += gy; sgz += gz;
+            ssq += (gx * gx + gy * gy) + gz * gz;
+        }
+    }
+    const unsigned nB = A.cnt_b[i];
+    for (unsigned kk = 0; kk < nB; ++kk) {
+        const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
+        rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(dist2_exact(xi, xb), P)));
+        if (ALPHA) {
+            const Pair p = make_pair(xi, xb);
+            const float f = xb.w * cs_gradf(p.rl, p.inv_rl, P);
+            sgx += f * p.rx; sgy += f * p.ry; sgz += f * p.rz;
+        }
+    }
+    A.rho[i] = rho;
+    if (ALPHA) {
+        const float denom = ((sgx * sgx + sgy * sgy) + sgz * sgz) + ssq;
+        A.alpha[i] = denom > P.eps ? rho / denom : 0.0f;
+    }
+    if (EOS) A.press[i] = tait_pressure(rho, P, P.kr_g);
+}
+
+__global__ void __launch_bounds__(256) k_normals(SimParams P, DeviceArrays A)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.nf) return;
+    const size_t nf = (size_t)P.nf;
+    const float4 xi = A.pos[i];
+    float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+    const unsigned nF = A.cnt_f[i];
+    for (unsigned kk = 0; kk < nF; ++kk) {
+        const unsigned j = A.nbr_f[kk * nf + i];
+        const Pair p = make_pair(xi, A.pos[j]);
+        const float f = (P.mass / A.rho[j]) * cs_gradf(p.rl, p.inv_rl, P);
+        nx += f * p.rx; ny += f * p.ry; nz += f * p.rz;
+    }
+    A.normal[i] = make_float4(nx * P.h, ny * P.h, nz * P.h, 0.0f);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_forces(SimParams P, DeviceArrays A)
+{
+    __shared__ float s_red[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < P.nf;
+    const size_t nf = (size_t)P.nf;
+    const float dt = A.st->dt;
+    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+    float4 xi = make_float4(0, 0, 0, 0), vi = xi;
+    if (active) {
+        xi = A.pos[i];
+        vi = A.vel[i];
+        const float rho_i = A.rho[i];
+        const unsigned nF = A.cnt_f[i], nB = A.cnt_b[i];
+        const bool pressure = MODE == FORCE_WCSPH || MODE == FORCE_PRESSURE;
+        const bool np = MODE != FORCE_PRESSURE;
+        const int vm = np ? P.visc_method : -1;
+        const bool st_on = np && P.st_on;
+        const float dpi = pressure ? A.press[i] / (rho_i * rho_i) : 0.0f;
+        const float dpb = pressure ? A.press[i] / (P.rho0 * P.rho0) : 0.0f;
+        const float4 ni = st_on ? A.normal[i] : make_float4(0, 0, 0, 0);
+        const float eps_h2 = 0.01f * P.h2;
+        float svx = 0.0f, svy = 0.0f, svz = 0.0f; /* standard viscosity sum */
+        for (unsigned kk = 0; kk < nF; ++kk) {
+            const unsigned j = A.nbr_f[kk * nf + i];
+            const float4 xj = A.pos[j];
+            const Pair p = make_pair(xi, xj);
+            const float rho_j = A.rho[j];
+            const float f = cs_gradf(p.rl, p.inv_rl, P);
+            if (pressure) {
+                const float pj = A.press[j];
+                const float c = P.mass * (dpi + pj / (rho_j * rho_j)) * f;
+                ax -= c * p.rx; ay -= c * p.ry; az -= c * p.rz;
+            }
+            if (vm >= 0) {
+                const float4 vj = A.vel[j];
+                const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+                if (vm == 1) {
+                    const float dot = (dvx * p.rx + dvy * p.ry) + dvz * p.rz;
+                    const float c = P.visc * (P.mass / rho_j) * dot / (p.s + eps_h2) * f;
+                    ax += c * p.rx; ay += c * p.ry; az += c * p.rz;
+                } else if (vm == 0) {
+                    const float c = P.mass / rho_j * visco_lapl(p.rl, P);
+                    svx -= c * dvx; svy -= c * dvy; svz -= c * dvz;
+                } else {
+                    const float c = P.visc * (P.mass / rho_j) * cs_W(p.rl * P.inv_h, P) / dt;
+                    ax -= c * dvx; ay -= c * dvy; az -= c * dvz;
+                }
+            }
+            if (st_on && p.s > 0.0f) {
+                const float4 nj = A.normal[j];
+                const float kij = 2.0f * P.rho0 / (rho_i + rho_j);
+                const float c = P.st * P.mass * cohesion_W(p.rl, P) * p.inv_rl;
+                ax += kij * (-c * p.rx - P.st * (ni.x - nj.x));
+                ay += kij * (-c * p.ry - P.st * (ni.y - nj.y));
+                az += kij * (-c * p.rz - P.st * (ni.z - nj.z));
+            }
+        }
+        if (vm == 0) {
+            const float c = P.visc / rho_i;
+            ax += svx * c; ay += svy * c; az += svz * c;
+        }
+        const bool bvisc = vm >= 0 && P.bvisc != 0.0f;
+        if (pressure || bvisc || (np && P.adh_on)) {
+            float bvx = 0.0f, bvy = 0.0f, bvz = 0.0f;
+            for (unsigned kk = 0; kk < nB; ++kk) {
+                const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
+                const Pair p = make_pair(xi, xb);
+                const float psi = xb.w;
+                const float f = cs_gradf(p.rl, p.inv_rl, P);
+                if (pressure) {
+                    const float c = psi * (dpi + dpb) * f;
+                    ax -= c * p.rx; ay -= c * p.ry; az -= c * p.rz;
+                }
+                if (bvisc) {
+                    if (vm == 1) {
+                        const float dot = (vi.x * p.rx + vi.y * p.ry) + vi.z * p.rz;
+                        const float c = P.bvisc * (psi / rho_i) * dot / (p.s + eps_h2) * f;
+                        ax += c * p.rx; ay += c * p.ry; az += c * p.rz;
+                    } else if (vm == 0) {
+                        const float c = psi / rho_i * visco_lapl(p.rl, P);
+                        bvx -= c * vi.x; bvy -= c * vi.y; bvz -= c * vi.z;
+                    } else {
+                        const float c = P.bvisc * (psi / rho_i) * cs_W(p.rl * P.inv_h, P) / dt;
+                        ax -= c * vi.x; ay -= c * vi.y; az -= c * vi.z;
+                    }
+                }
+                if (np && P.adh_on && p.s > 0.0f) {
+                    const float c = P.adh * psi * adhesion_W(p.rl, P) * p.inv_rl;
+                    ax -= c * p.rx; ay -= c * p.ry; az -= c * p.rz;
+                }
+            }
+            if (bvisc && vm == 0) {
+                const float c = P.bvisc / rho_i;
+                ax += bvx * c; ay += bvy * c; az += bvz * c;
+            }
+        }
+    }
+
+    if (MODE == FORCE_WCSPH) {
+        if (active) {
+            /* SPHSolver::integrate: a += g; v += a dt; x += v dt (unfused, as the reference rounds) */
+            ax = __fadd_rn(ax, P.gx); ay = __fadd_rn(ay, P.gy); az = __fadd_rn(az, P.gz);
+            const float nvx = __fadd_rn(vi.x, __fmul_rn(ax, dt)), nvy = __fadd_rn(vi.y, __fmul_rn(ay, dt)),
+                        nvz = __fadd_rn(vi.z, __fmul_rn(az, dt));
+            const float px = __fadd_rn(xi.x, __fmul_rn(nvx, dt)), py = __fadd_rn(xi.y, __fmul_rn(nvy, dt)),
+                        pz = __fadd_rn(xi.z, __fmul_rn(nvz, dt));
+            A.vel_alt[i] = make_float4(nvx, nvy, nvz, 0.0f);
+            A.pos_alt[i] = make_float4(px, py, pz, 0.0f);
+            if (!isfinite(px) || !isfinite(py) || !isfinite(pz)) atomicOr(&A.st->err, ERRBIT_NAN);
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            A.st->time += (double)dt;
+            A.st->steps += 1u;
+        }
+        return;
+    }
+    if (active) A.acc[i] = make_float4(ax, ay, az, 0.0f);
+    if (MODE == FORCE_NP_CFL) {
+        float speed = 0.0f;
+        if (active) {
+            const float cx = __fadd_rn(vi.x, __fmul_rn(__fadd_rn(ax, P.gx), dt));
+            const float cy = __fadd_rn(vi.y, __fmul_rn(__fadd_rn(ay, P.gy), dt));
+            const float cz = __fadd_rn(vi.z, __fmul_rn(__fadd_rn(az, P.gz), dt));
+            speed = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(cx, cx), __fmul_rn(cy, cy)), __fmul_rn(cz, cz)));
+            if (!(speed == speed)) speed = 3.0e38f;
+        }
+        const float m = block_max(speed, s_red);
+        if (threadIdx.x == 0) atomicMax(&A.st->vmax_bits, __float_as_uint(m));
+    }
+}
+
+/* ---------------------------------------------------------------------- */
+/* DFSPH pieces                                                             */
+
+/* predicted density (DIV=false) or divergence error (DIV=true) of particle i */
+template <bool DIV>
+__device__ __forceinline__ float dfsph_residual(const SimParams& P, const DeviceArrays& A, int i, size_t nf,
+                                                float dt)
+{
+    const float4 xi = A.pos[i];
+    const float4 vi = A.vel[i];
+    float sum = 0.0f;
+    const unsigned nF = A.cnt_f[i], nB = A.cnt_b[i];
+    for (unsigned kk = 0; kk < nF; ++kk) {
+        const unsigned j = A.nbr_f[kk * nf + i];
+        const Pair p = make_pair(xi, A.pos[j]);
+        const float4 vj = A.vel[j];
+        const float f = cs_gradf(p.rl, p.inv_rl, P);
+        sum += P.mass * (f * (((vi.x - vj.x) * p.rx + (vi.y - vj.y) * p.ry) + (vi.z - vj.z) * p.rz));
+    }
+    for (unsigned kk = 0; kk < nB; ++kk) {
+        const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
+        const Pair p = make_pair(xi, xb);
+        const float f = cs_gradf(p.rl, p.inv_rl, P);
+        sum += xb.w * (f * ((vi.x * p.rx + vi.y * p.ry) + vi.z * p.rz));
+    }
+    if (DIV) {
+        /* particles with fewer than 20 neighbours within h are not corrected
+           (DFSPHSolver.cpp:608-611); the lists hold exactly those neighbours */
+        if (nF + nB < 20u) return 0.0f;
+        return fmaxf(sum, 0.0f);
+    }
+    /* rho_i + dt * change, rounded as the reference rounds it: the result
+       enters (rho* - rho0), where a contracted FMA would shift it by an ulp */
+    return fmaxf(__fadd_rn(A.rho[i], __fmul_rn(sum, dt)), P.rho0);
+}
+
+/* v_i -= dt * sum_j m (k_i + k_j) gradW  (+ boundary with k_i) */
+__device__ __forceinline__ void dfsph_correct(const SimParams& P, const DeviceArrays& A, const float* __restrict__ K,
+                                              int i, size_t nf, float dt)
+{
+    const float4 xi = A.pos[i];
+    const float ki = K[i];
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    const unsigned nF = A.cnt_f[i];
+    for (unsigned kk = 0; kk < nF; ++kk) {
+        const unsigned j = A.nbr_f[kk * nf + i];
+        const float ks = ki + K[j];
+        if (fabsf(ks) > P.eps) {
+            const Pair p = make_pair(xi, A.pos[j]);
+            const float c = P.mass * ks * cs_gradf(p.rl, p.inv_rl, P);
+            sx += c * p.rx; sy += c * p.ry; sz += c * p.rz;
+        }
+    }
+    if (fabsf(ki) > P.eps) {
+        const unsigned nB = A.cnt_b[i];
+        for (unsigned kk = 0; kk < nB; ++kk) {
+            const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
+            const Pair p = make_pair(xi, xb);
+            const float c = xb.w * ki * cs_gradf(p.rl, p.inv_rl, P);
+            sx += c * p.rx; sy += c * p.ry; sz += c * p.rz;
+        }
+    }
+    float4 v = A.vel[i];
+    v.x = __fsub_rn(v.x, __fmul_rn(dt, sx));
+    v.y = __fsub_rn(v.y, __fmul_rn(dt, sy));
+    v.z = __fsub_rn(v.z, __fmul_rn(dt, sz));
+    A.vel[i] = v;
+}
+
+template <bool DIV>
+__global__ void __launch_bounds__(kSolverBlock, 4) k_dfsph_solve(SimParams P, DeviceArrays A)
+{
+    __shared__ double s_red[32];
+    DevState* st = A.st;
+    const int nfi = P.nf;
+    const size_t nf = (size_t)nfi;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthr = gridDim.x * blockDim.x;
+
+    float dt;
+    float vmax = 0.0f;
+    if (!DIV) {
+        /* DFSPHSolver::updateTimeStep: CFL bound and iteration-count rule */
+        const float dt_old = st->dt;
+        vmax = __uint_as_float(st->vmax_bits);
+        if (vmax < 1.0e-9f) vmax = 1.0e-9f;
+        const float cfl_ts = P.cfl * 0.4f * (2.0f * P.r) / vmax;
+        const unsigned its = max(st->its, st->its_v);
+        float hs = dt_old;
+        if (its > 6u) hs *= 0.9f;
+        else if (its < 4u) hs *= 1.05f;
+        hs = fminf(hs, cfl_ts);
+        hs = fmaxf(hs, P.min_ts);
+        hs = fminf(hs, P.max_ts);
+        dt = hs;
+        /* DFSPHSolver::predictVelocities */
+        for (int i = tid; i < nfi; i += nthr) {
+            const float4 a = A.acc[i];
+            float4 v = A.vel[i];
+            v.x = __fadd_rn(v.x, __fmul_rn(__fadd_rn(a.x, P.gx), dt));
+            v.y = __fadd_rn(v.y, __fmul_rn(__fadd_rn(a.y, P.gy), dt));
+            v.z = __fadd_rn(v.z, __fmul_rn(__fadd_rn(a.z, P.gz), dt));
+            A.vel[i] = v;
+            A.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        if (!grid_barrier(st)) return;
+    } else {
+        dt = st->dt;
+    }
+    const float ts2 = dt * dt;
+    float* kws = DIV ? A.kvws : A.kws;
+
+    /* warm start: residual at the current velocities, keep the previous
+       step's accumulated k only where the residual is positive */
+    for (int i = tid; i < nfi; i += nthr) {
+        const float r = dfsph_residual<DIV>(P, A, i, nf, dt);
+        if (DIV) kws[i] = r > 0.0f ? kws[i] / dt : 0.0f;
+        else kws[i] = r > P.rho0 ? kws[i] / ts2 : 0.0f;
+    }
+    if (!grid_barrier(st)) return;
+    for (int i = tid; i < nfi; i += nthr) dfsph_correct(P, A, kws, i, nf, dt);
+    if (!grid_barrier(st)) return;
+    for (int i = tid; i < nfi; i += nthr) kws[i] = 0.0f;
+
+    const double limit = DIV ? (double)(P.eta_v / dt) : (double)P.eta;
+    const unsigned min_it = DIV ? P.min_it_v : P.min_it;
+    /* the divergence loop is capped by maxIterations, not maxIterationsV
+       (DFSPHSolver.cpp:746) */
+    const unsigned max_it = P.max_it;
+    unsigned it = 0;
+    double avg = 0.0;
+    while ((avg > limit || it < min_it) && it < max_it) {
+        double local = 0.0;
+        for (int i = tid; i < nfi; i += nthr) {
+            const float r = dfsph_residual<DIV>(P, A, i, nf, dt);
+            float k;
+            if (DIV) {
+                k = r * A.alpha[i] / (dt * A.rho[i]);
+                local += (double)(r / P.rho0);
+            } else {
+                k = __fdiv_rn(__fmul_rn(__fsub_rn(r, P.rho0), A.alpha[i]), __fmul_rn(ts2, A.rho[i]));
+                local += (double)((r - P.rho0) / P.rho0);
+            }
+            A.k[i] = k;
+            kws[i] += k;
+        }
+        const double bs = block_sum(local, s_red);
+        if (threadIdx.x == 0) atomicAdd(&A.accum[it], bs);
+        if (!grid_barrier(st)) return;
+        avg = *(volatile double*)&A.accum[it] / (double)nfi;
+        for (int i = tid; i < nfi; i += nthr) dfsph_correct(P, A, A.k, i, nf, dt);
+        if (!grid_barrier(st)) return;
+        ++it;
+    }
+
+    const float scale = DIV ? dt : ts2;
+    for (int i = tid; i < nfi; i += nthr) kws[i] *= scale;
+    if (!DIV) {
+        /* DFSPHSolver::updatePositions */
+        bool bad = false;
+        for (int i = tid; i < nfi; i += nthr) {
+            const float4 v = A.vel[i];
+            float4 x = A.pos[i];
+            x.x = __fadd_rn(x.x, __fmul_rn(v.x, dt));
+            x.y = __fadd_rn(x.y, __fmul_rn(v.y, dt));
+            x.z = __fadd_rn(x.z, __fmul_rn(v.z, dt));
+            A.pos[i] = x;
+            bad |= !isfinite(x.x) || !isfinite(x.y) || !isfinite(x.z);
+        }
+        if (bad) atomicOr(&st->err, ERRBIT_NAN);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (!DIV) {
+            st->dt = dt;
+            st->its = it;
+            st->avg_dens = avg;
+            st->sum_its += it;
+            st->last_vmax = vmax;
+        } else {
+            st->its_v = it;
+            st->avg_div = avg;
+            st->sum_its_v += it;
+            st->time += (double)dt;
+            st->steps += 1u;
+            st->vmax_bits = 0u;
+        }
+    }
+}
+
+/* ---------------------------------------------------------------------- */
+/* PCISPH                                                                   */
+
+__global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, DeviceArrays A)
+{
+    __shared__ double s_red[32];
+    DevState* st = A.st;
+    const int nfi = P.nf;
+    const size_t nf = (size_t)nfi;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthr = gridDim.x * blockDim.x;
+    const float dt = st->dt;
+
+    /* PCISPHSolver::initPressure */
+    for (int i = tid; i < nfi; i += nthr) {
+        A.press[i] = 0.0f;
+        A.pacc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    unsigned it = 0;
+    /* the first test uses the residual left by the previous step (PCISPHSolver.cpp:374) */
+    double avg = st->pcisph_avg;
+    while ((avg > (double)P.eta || it < P.min_it) && it < P.max_it) {
+        /* predictVelocityAndPosition */
+        for (int i = tid; i < nfi; i += nthr) {
+            const float4 a = A.acc[i], pa = A.pacc[i], v = A.vel[i], x = A.pos[i];
+            /* acc = (a + pacc) + g; predV = v + acc dt; predR = r + predV dt */
+            const float vx = __fadd_rn(v.x, __fmul_rn(__fadd_rn(__fadd_rn(a.x, pa.x), P.gx), dt));
+            const float vy = __fadd_rn(v.y, __fmul_rn(__fadd_rn(__fadd_rn(a.y, pa.y), P.gy), dt));
+            const float vz = __fadd_rn(v.z, __fmul_rn(__fadd_rn(__fadd_rn(a.z, pa.z), P.gz), dt));
+            A.predr[i] = make_float4(__fadd_rn(x.x, __fmul_rn(vx, dt)), __fadd_rn(x.y, __fmul_rn(vy, dt)),
+                                     __fadd_rn(x.z, __fmul_rn(vz, dt)), 0.0f);
+        }
+        if (!grid_barrier(st)) return;
+        /* predictFluidDensities over the start-of-step candidates of the 27
+           cells around the particle's current cell, then updatePressure */
+        double local = 0.0;
+        for (int i = tid; i < nfi; i += nthr) {
+            const float4 xi = A.pos[i];
+            const float4 pi = A.predr[i];
+            const int cx = cell_coord(xi.x, P.h, P.cminx, P.dimx);
+            const int cy = cell_coord(xi.y, P.h, P.cminy, P.dimy);
+            const int cz = cell_coord(xi.z, P.h, P.cminz, P.dimz);
+            /* all fluid candidates of the 27 cells first, then all boundary
+               candidates: the reference's summation order (PCISPHSolver.cpp:180-206) */
+            float rho = 0.0f;
+            for (int pass = 0; pass < 2; ++pass) {
+                if (pass == 1 && P.nb == 0) break;
+                const unsigned* __restrict__ cs = pass == 0 ? A.cell_start : A.bcell_start;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int x = cx + dx;
+                    if (x < 0 || x >= P.dimx) continue;
+                    for (int dy = -1; dy <= 1; ++dy) {
+                        const int y = cy + dy;
+                        if (y < 0 || y >= P.dimy) continue;
+                        for (int dz = -1; dz <= 1; ++dz) {
+                            const int z = cz + dz;
+                            if (z < 0 || z >= P.dimz) continue;
+                            const unsigned c = brick_morton(x, y, z, P);
+                            const unsigned e = cs[c + 1];
+                            if (pass == 0) {
+                                for (unsigned q = cs[c]; q < e; ++q) {
+                                    const float s2 = dist2_exact(pi, A.predr[q]);
+                                    if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(s2, P)));
+                                }
+                            } else {
+                                for (unsigned q = cs[c]; q < e; ++q) {
+                                    const float4 xb = A.bpos[q];
+                                    const float s2 = dist2_exact(pi, xb);
+                                    if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(s2, P)));
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            A.rho[i] = rho;
+            const float err = fmaxf(0.0f, __fsub_rn(rho, P.rho0));
+            A.press[i] = __fadd_rn(A.press[i], __fmul_rn(P.pcisph_delta, err));
+            local += (double)(err / P.rho0);
+        }
+        const double bs = block_sum(local, s_red);
+        if (threadIdx.x == 0) atomicAdd(&A.accum[it], bs);
+        if (!grid_barrier(st)) return;
+        avg = *(volatile double*)&A.accum[it] / (double)nfi;
+        /* computePressureAcc at the current positions, with the reference's
+           exact gradient arithmetic: the result feeds the next predicted
+           positions, whose densities enter the ill-conditioned p update */
+        for (int i = tid; i < nfi; i += nthr) {
+            const float4 xi = A.pos[i];
+            const float rho_i = A.rho[i];
+            const float dpi = __fdiv_rn(A.press[i], __fmul_rn(rho_i, rho_i));
+            float ax = 0.0f, ay = 0.0f, az = 0.0f;
+            const unsigned nF = A.cnt_f[i], nB = A.cnt_b[i];
+            for (unsigned kk = 0; kk < nF; ++kk) {
+                const unsigned j = A.nbr_f[kk * nf + i];
+                const float4 xj = A.pos[j];
+                const float rho_j = A.rho[j];
+                float gx, gy, gz;
+                cs_gradW_exact(__fsub_rn(xi.x, xj.x), __fsub_rn(xi.y, xj.y), __fsub_rn(xi.z, xj.z), P, gx, gy, gz);
+                const float c = __fmul_rn(P.mass, __fadd_rn(dpi, __fdiv_rn(A.press[j], __fmul_rn(rho_j, rho_j))));
+                ax = __fsub_rn(ax, __fmul_rn(c, gx));
+                ay = __fsub_rn(ay, __fmul_rn(c, gy));
+                az = __fsub_rn(az, __fmul_rn(c, gz));
+            }
+            for (unsigned kk = 0; kk < nB; ++kk) {
+                const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
+                float gx, gy, gz;
+                cs_gradW_exact(__fsub_rn(xi.x, xb.x), __fsub_rn(xi.y, xb.y), __fsub_rn(xi.z, xb.z), P, gx, gy, gz);
+                const float c = __fmul_rn(xb.w, dpi);
+                ax = __fsub_rn(ax, __fmul_rn(c, gx));
+                ay = __fsub_rn(ay, __fmul_rn(c, gy));
+                az = __fsub_rn(az, __fmul_rn(c, gz));
+            }
+            A.pacc[i] = make_float4(ax, ay, az, 0.0f);
+        }
+        ++it;
+    }
+    if (!grid_barrier(st)) return;
+    /* PCISPHSolver::integrate */
+    bool bad = false;
+    for (int i = tid; i < nfi; i += nthr) {
+        const float4 a = A.acc[i], pa = A.pacc[i];
+        float4 v = A.vel[i], x = A.pos[i];
+        /* a += g + pacc; v += a dt; x += v dt */
+        const float axx = __fadd_rn(a.x, __fadd_rn(P.gx, pa.x));
+        const float ayy = __fadd_rn(a.y, __fadd_rn(P.gy, pa.y));
+        const float azz = __fadd_rn(a.z, __fadd_rn(P.gz, pa.z));
+        v.x = __fadd_rn(v.x, __fmul_rn(axx, dt)); v.y = __fadd_rn(v.y, __fmul_rn(ayy, dt));
+        v.z = __fadd_rn(v.z, __fmul_rn(azz, dt));
+        x.x = __fadd_rn(x.x, __fmul_rn(v.x, dt)); x.y = __fadd_rn(x.y, __fmul_rn(v.y, dt));
+        x.z = __fadd_rn(x.z, __fmul_rn(v.z, dt));
+        A.vel[i] = v;
+        A.pos[i] = x;
+        A.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        bad |= !isfinite(x.x) || !isfinite(x.y) || !isfinite(x.z);
+    }
+    if (bad) atomicOr(&st->err, ERRBIT_NAN);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->its = it;
+        st->pcisph_avg = avg;
+        st->avg_dens = avg;
+        st->sum_its += it;
+        st->time += (double)dt;
+        st->steps += 1u;
+    }
+}
+
+/* ---------------------------------------------------------------------- */
+
+static inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
+
+void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool eos, cudaStream_t s)
+{
+    if (P.nf <= 0) return;
+    const int g = blocks_for(P.nf, 256);
+    if (alpha && eos) k_density<true, true><<<g, 256, 0, s>>>(P, A);
+    else if (alpha) k_density<true, false><<<g, 256, 0, s>>>(P, A);
+    else if (eos) k_density<false, true><<<g, 256, 0, s>>>(P, A);
+    else k_density<false, false><<<g, 256, 0, s>>>(P, A);
+}
+
+void launch_normals(const SimParams& P, const DeviceArrays& A, cudaStream_t s)
+{
+    if (P.nf <= 0) return;
+    k_normals<<<blocks_for(P.nf, 256), 256, 0, s>>>(P, A);
+}
+
+void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, cudaStream_t s)
+{
+    const int g = P.nf > 0 ? blocks_for(P.nf, 128) : 1;
+    switch (mode) {
+    case FORCE_NP: k_forces<FORCE_NP><<<g, 128, 0, s>>>(P, A); break;
+    case FORCE_NP_CFL: k_forces<FORCE_NP_CFL><<<g, 128, 0, s>>>(P, A); break;
+    case FORCE_WCSPH: k_forces<FORCE_WCSPH><<<g, 128, 0, s>>>(P, A); break;
+    default: k_forces<FORCE_PRESSURE><<<g, 128, 0, s>>>(P, A); break;
+    }
+}
+
+int persistent_grid(bool pcisph, bool divergence)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    const void* fn = pcisph ? (const void*)k_pcisph_solve
+                            : divergence ? (const void*)k_dfsph_solve<true> : (const void*)k_dfsph_solve<false>;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolverBlock, 0) != cudaSuccess) return 0;
+    return per_sm * sms;
+}
+
+static int coop_launch(const void* fn, const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s)
+{
+    SimParams p = P;
+    DeviceArrays a = A;
+    void* args[] = {&p, &a};
+    return (int)cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kSolverBlock), args, 0, s);
+}
+
+int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s)
+{
+    const int need = blocks_for(P.nf > 0 ? P.nf : 1, kSolverBlock);
+    const int g = grid < need ? grid : need;
+    return coop_launch(divergence ? (const void*)k_dfsph_solve<true> : (const void*)k_dfsph_solve<false>, P, A,
+                       g > 0 ? g : 1, s);
+}
+
+int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s)
+{
+    const int need = blocks_for(P.nf > 0 ? P.nf : 1, kSolverBlock);
+    const int g = grid < need ? grid : need;
+    return coop_launch((const void*)k_pcisph_solve, P, A, g > 0 ? g : 1, s);
+}
+
+} // namespace sph

@@ -1,0 +1,313 @@
+/*
+ * Scene JSON loading and particle generation on the host.
+ *
+ * Restates, in this project's own code, what SPH2O does between reading a
+ * scene file and the first solver step:
+ *   - SceneLoader::readSceneInfo/readFluidInfo/readBoundaryInfo
+ *     (src/SPH2O/SceneLoader.cpp:40-209): same keys, same conditional reads;
+ *   - SPHSimulation::importScene (src/SPH2O/SPHSimulation.cpp:299-481): one
+ *     fluid model, Akinci boundary objects built box-then-sphere per object;
+ *   - FluidObject::build (src/SPH2O/FluidObject/FluidObject.cpp:30-61);
+ *   - AkinciBoundaryObject::sampleCube / sampleSphere
+ *     (src/SPH2O/BoundaryObject/AkinciBoundaryObject.cpp:97-153).
+ * The arithmetic keeps SPH2O's types operation by operation (float where the
+ * reference computes in float, double where its unqualified pow/sin/cos/
+ * round/floor calls resolve to the double overloads), so the generated
+ * particles are bit-identical to the reference's. This file is compiled with
+ * -ffp-contract=off for that reason.
+ *
+ * Not supported (rejected with SPH_ERR_ARG): more than one fluid model,
+ * emitters, boundary methods other than Akinci, OBJ "geometry" boundaries.
+ */
+#include "../../include/sph2o_cuda.h"
+#include "json_lite.h"
+#include "scene_rng.h"
+
+#include <cmath>
+#include <fstream>
+#include <math.h>
+#include <sstream>
+#include <string>
+#include <vector>
+
+struct sph_scene {
+    sph_scene_desc desc;
+    std::vector<float> fluid;     /* n*3 */
+    std::vector<float> fluid_v;   /* n*3 */
+    std::vector<float> boundary;  /* nb*3 */
+    std::string path;
+};
+
+namespace {
+
+thread_local std::string g_scene_error;
+
+struct V3 { float x, y, z; };
+
+float num(const sphjson::Value& v, const char* what) { return (float)v.as_number(what); }
+
+V3 vec3(const sphjson::Value& v, const char* what)
+{
+    if (!v.is_array() || v.size() < 3) throw sphjson::JsonError(std::string("expected [x,y,z] for ") + what);
+    return {num(v.at(0), what), num(v.at(1), what), num(v.at(2), what)};
+}
+
+/* FluidObject::build (FluidObject.cpp:30-61): lattice at spacing 2r,
+   origin min + r, count floor((max - min) / 2r + 1e-5) per axis, k fastest. */
+void build_lattice(const std::vector<std::pair<V3, V3>>& blocks, float radius, std::vector<float>& out)
+{
+    const float dist = 2.0f * radius;
+    for (const auto& b : blocks) {
+        const V3& lo = b.first;
+        const V3& hi = b.second;
+        const unsigned nx = (unsigned)::floor((double)((hi.x - lo.x) / dist + 1e-5f));
+        const unsigned ny = (unsigned)::floor((double)((hi.y - lo.y) / dist + 1e-5f));
+        const unsigned nz = (unsigned)::floor((double)((hi.z - lo.z) / dist + 1e-5f));
+        const float ox = lo.x + radius, oy = lo.y + radius, oz = lo.z + radius;
+        for (unsigned i = 0; i < nx; ++i)
+            for (unsigned j = 0; j < ny; ++j)
+                for (unsigned k = 0; k < nz; ++k) {
+                    out.push_back((float)i * dist + ox);
+                    out.push_back((float)j * dist + oy);
+                    out.push_back((float)k * dist + oz);
+                }
+    }
+}
+
+/* AkinciBoundaryObject::sampleCube (AkinciBoundaryObject.cpp:97-123):
+   single-layer hollow box, ceil(l / 2r) intervals per axis. */
+void sample_cube(V3 lo, V3 hi, float radius, std::vector<float>& out)
+{
+    const float lx = std::fabs(lo.x - hi.x), ly = std::fabs(lo.y - hi.y), lz = std::fabs(lo.z - hi.z);
+    const float two_r = 2.0f * radius;
+    const float nx = std::ceil(lx / two_r), ny = std::ceil(ly / two_r), nz = std::ceil(lz / two_r);
+    const float dx = lx / nx, dy = ly / ny, dz = lz / nz;
+    for (unsigned i = 0; (float)i <= nx; i++)
+        for (unsigned j = 0; (float)j <= ny; j++)
+            for (unsigned k = 0; (float)k <= nz; k++)
+                if ((i == 0 || (float)i == nx) || (j == 0 || (float)j == ny) || (k == 0 || (float)k == nz)) {
+                    out.push_back((float)i * dx + lo.x);
+                    out.push_back((float)j * dy + lo.y);
+                    out.push_back((float)k * dz + lo.z);
+                }
+}
+
+/* AkinciBoundaryObject::sampleSphere (AkinciBoundaryObject.cpp:125-153):
+   equal-area points with 1.5x overlap; the trigonometry runs in double
+   exactly where the reference's unqualified calls do. */
+void sample_sphere(V3 c, float radius, float particle_radius, std::vector<float>& out)
+{
+    const float separation = 1.5f;
+    const unsigned num_parts = (unsigned)::floor(4.0 * M_PI * (double)radius * (double)radius /
+                                                 (M_PI * (double)particle_radius * (double)particle_radius) *
+                                                 (double)separation);
+    if (num_parts == 0) return;
+    const float a = (float)(4.0 * M_PI) / (float)num_parts;
+    const float d = (float)::sqrt((double)a);
+    const unsigned m_theta = (unsigned)::round(M_PI / (double)d);
+    const float d_theta = (float)M_PI / (float)m_theta;
+    const float d_phi = a / d_theta;
+    for (unsigned m = 0; m < m_theta; ++m) {
+        const float theta = (float)(M_PI * ((double)m + 0.5)) / (float)m_theta;
+        const unsigned m_phi = (unsigned)::round(2.0 * M_PI * ::sin((double)theta) / (double)d_phi);
+        for (unsigned n = 0; n < m_phi; ++n) {
+            const float phi = (float)(2.0 * M_PI) * (float)n / (float)m_phi;
+            const float x = (float)(::sin((double)theta) * ::cos((double)phi));
+            const float y = (float)(::sin((double)theta) * ::sin((double)phi));
+            const float z = (float)::cos((double)theta);
+            out.push_back(radius * x + c.x);
+            out.push_back(radius * y + c.y);
+            out.push_back(radius * z + c.z);
+        }
+    }
+}
+
+unsigned uint_field(const sphjson::Value& cfg, const char* key)
+{
+    const double d = cfg.get(key).as_number(key);
+    if (d < 0) throw sphjson::JsonError(std::string(key) + " must be non-negative");
+    return (unsigned)d;
+}
+
+sph_scene* build_scene(const std::string& text, const std::string& path)
+{
+    const sphjson::Value root = sphjson::parse(text);
+    auto scene = std::make_unique<sph_scene>();
+    sph_scene_desc& d = scene->desc;
+    std::memset(&d, 0, sizeof d);
+    scene->path = path;
+
+    /* SceneLoader::readSceneInfo (SceneLoader.cpp:40-78) */
+    const sphjson::Value& c = root.get("Configuration");
+    d.start_time = num(c.get("startTime"), "startTime");
+    d.end_time = num(c.get("endTime"), "endTime");
+    d.time_step = num(c.get("timeStep"), "timeStep");
+    d.fps = num(c.get("fps"), "fps");
+    d.min_time_step = num(c.get("minTimeStep"), "minTimeStep");
+    d.max_time_step = num(c.get("maxTimeStep"), "maxTimeStep");
+    d.cfl_factor = num(c.get("cflFactor"), "cflFactor");
+    d.particle_radius = num(c.get("particleRadius"), "particleRadius");
+    d.boundary_method = (int)c.get("boundaryMethod").as_number("boundaryMethod");
+    d.simulation_method = (int)c.get("simulationMethod").as_number("simulationMethod");
+    const V3 g = vec3(c.get("gravity"), "gravity");
+    d.gravity[0] = g.x; d.gravity[1] = g.y; d.gravity[2] = g.z;
+    if (d.simulation_method == SPH_WCSPH) {
+        d.stiffness = num(c.get("stiffness"), "stiffness");
+        d.gamma = num(c.get("gamma"), "gamma");
+    } else if (d.simulation_method == SPH_PCISPH) {
+        d.eta = num(c.get("eta"), "eta");
+        d.min_iterations = uint_field(c, "minIterations");
+        d.max_iterations = uint_field(c, "maxIterations");
+    } else if (d.simulation_method == SPH_DFSPH) {
+        d.eta = num(c.get("eta"), "eta");
+        d.eta_v = num(c.get("etaV"), "etaV");
+        d.min_iterations = uint_field(c, "minIterations");
+        d.max_iterations = uint_field(c, "maxIterations");
+        d.min_iterations_v = uint_field(c, "minIterationsV");
+        d.max_iterations_v = uint_field(c, "maxIterationsV");
+    } else {
+        throw sphjson::JsonError("simulationMethod must be 0 (WCSPH), 1 (PCISPH) or 2 (DFSPH)");
+    }
+    if (d.boundary_method != SPH_BOUNDARY_AKINCI)
+        throw std::invalid_argument("only boundaryMethod 2 (Akinci) is implemented");
+
+    /* SceneLoader::readFluidInfo (SceneLoader.cpp:80-146) */
+    const sphjson::Value& fl = root.get("Fluid");
+    d.viscosity_method = (int)fl.get("viscosityMethod").as_number("viscosityMethod");
+    d.surface_tension_method = (int)fl.get("surfaceTensionMethod").as_number("surfaceTensionMethod");
+    d.adhesion_method = (int)fl.get("adhesionMethod").as_number("adhesionMethod");
+    const sphjson::Value& models = fl.get("FluidModel");
+    if (models.size() != 1) throw std::invalid_argument("exactly one FluidModel is supported");
+    const sphjson::Value& fm = models.at(0);
+    d.density0 = num(fm.get("density0"), "density0");
+    if (d.viscosity_method > -1) {
+        d.viscosity = num(fm.get("viscosity"), "viscosity");
+        d.boundary_viscosity = num(fm.get("boundaryViscosity"), "boundaryViscosity");
+    }
+    if (d.surface_tension_method > -1) d.surface_tension = num(fm.get("surfaceTension"), "surfaceTension");
+    if (d.adhesion_method > -1) d.adhesion = num(fm.get("adhesion"), "adhesion");
+    if (const sphjson::Value* em = fm.find("emitters"))
+        if (em->size() > 0) throw std::invalid_argument("emitters are not supported");
+    std::vector<std::pair<V3, V3>> blocks;
+    const sphjson::Value& fb = fm.get("fluidBlocks");
+    for (size_t i = 0; i < fb.size(); ++i)
+        blocks.push_back({vec3(fb.at(i).get("min"), "fluidBlocks.min"), vec3(fb.at(i).get("max"), "fluidBlocks.max")});
+
+    build_lattice(blocks, d.particle_radius, scene->fluid);
+    scene->fluid_v.assign(scene->fluid.size(), 0.0f);
+
+    /* seeded jitter (scene_rng.h); absent keys leave the lattice as is */
+    if (const sphjson::Value* jit = c.find("jitter")) {
+        const float amp = (float)jit->as_number("jitter");
+        const sphjson::Value* sv = c.find("jitterSeed");
+        const uint64_t seed = sv ? (uint64_t)sv->as_number("jitterSeed") : 0ull;
+        if (amp != 0.0f) {
+            const size_t n = scene->fluid.size() / 3;
+            for (size_t i = 0; i < n; ++i)
+                for (int k = 0; k < 3; ++k)
+                    scene->fluid[3 * i + k] += sph_jitter_offset(seed, i, k, amp, d.particle_radius);
+        }
+    }
+
+    /* SceneLoader::readBoundaryInfo (SceneLoader.cpp:148-209) + importScene (:407-426) */
+    if (const sphjson::Value* bnd = root.find("Boundary")) {
+        for (size_t i = 0; i < bnd->size(); ++i) {
+            const sphjson::Value& b = bnd->at(i);
+            if (const sphjson::Value* boxes = b.find("box"))
+                for (size_t j = 0; j < boxes->size(); ++j)
+                    sample_cube(vec3(boxes->at(j).get("min"), "box.min"), vec3(boxes->at(j).get("max"), "box.max"),
+                                d.particle_radius, scene->boundary);
+            if (const sphjson::Value* sph = b.find("sphere"))
+                for (size_t j = 0; j < sph->size(); ++j)
+                    sample_sphere(vec3(sph->at(j).get("pos"), "sphere.pos"),
+                                  num(sph->at(j).get("radius"), "sphere.radius"), d.particle_radius, scene->boundary);
+            if (const sphjson::Value* geo = b.find("geometry"))
+                if (geo->size() > 0) throw std::invalid_argument("OBJ geometry boundaries are not supported");
+        }
+    }
+    return scene.release();
+}
+
+int load_common(const std::string& text, const std::string& path, sph_scene** out)
+{
+    if (!out) { g_scene_error = "null output pointer"; return SPH_ERR_ARG; }
+    *out = nullptr;
+    try {
+        *out = build_scene(text, path);
+        g_scene_error.clear();
+        return SPH_OK;
+    } catch (const sphjson::JsonError& e) {
+        g_scene_error = e.what();
+        return SPH_ERR_IO;
+    } catch (const std::invalid_argument& e) {
+        g_scene_error = e.what();
+        return SPH_ERR_ARG;
+    } catch (const std::exception& e) {
+        g_scene_error = e.what();
+        return SPH_ERR_IO;
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+int sph_scene_load(const char* json_path, sph_scene** out)
+{
+    if (!json_path) { g_scene_error = "null path"; return SPH_ERR_ARG; }
+    std::ifstream f(json_path);
+    if (!f) { g_scene_error = std::string("cannot read ") + json_path; return SPH_ERR_IO; }
+    std::stringstream ss;
+    ss << f.rdbuf();
+    return load_common(ss.str(), json_path, out);
+}
+
+int sph_scene_parse(const char* json_text, sph_scene** out)
+{
+    if (!json_text) { g_scene_error = "null text"; return SPH_ERR_ARG; }
+    return load_common(json_text, "", out);
+}
+
+int sph_scene_get_desc(const sph_scene* s, sph_scene_desc* out)
+{
+    if (!s || !out) return SPH_ERR_ARG;
+    *out = s->desc;
+    return SPH_OK;
+}
+
+unsigned sph_scene_num_fluid(const sph_scene* s) { return s ? (unsigned)(s->fluid.size() / 3) : 0u; }
+unsigned sph_scene_num_boundary(const sph_scene* s) { return s ? (unsigned)(s->boundary.size() / 3) : 0u; }
+
+int sph_scene_get_fluid(const sph_scene* s, float* xyz, float* v)
+{
+    if (!s) return SPH_ERR_ARG;
+    if (xyz) std::memcpy(xyz, s->fluid.data(), s->fluid.size() * sizeof(float));
+    if (v) std::memcpy(v, s->fluid_v.data(), s->fluid_v.size() * sizeof(float));
+    return SPH_OK;
+}
+
+int sph_scene_get_boundary(const sph_scene* s, float* xyz)
+{
+    if (!s) return SPH_ERR_ARG;
+    if (xyz) std::memcpy(xyz, s->boundary.data(), s->boundary.size() * sizeof(float));
+    return SPH_OK;
+}
+
+const char* sph_scene_error(void) { return g_scene_error.c_str(); }
+
+void sph_scene_free(sph_scene* s) { delete s; }
+
+int sph_create_from_scene(const sph_scene* s, sph_ctx** out)
+{
+    if (!s || !out) return SPH_ERR_ARG;
+    int rc = sph_create(&s->desc, out);
+    if (rc != SPH_OK) return rc;
+    sph_ctx* ctx = *out;
+    if ((rc = sph_set_fluid(ctx, sph_scene_num_fluid(s), s->fluid.data(), s->fluid_v.data())) != SPH_OK ||
+        (rc = sph_set_boundary(ctx, sph_scene_num_boundary(s), s->boundary.data())) != SPH_OK ||
+        (rc = sph_init(ctx)) != SPH_OK)
+        return rc; /* the context stays valid; sph_last_error(ctx) explains */
+    return SPH_OK;
+}
+
+} // extern "C"

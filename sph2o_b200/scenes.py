@@ -1,0 +1,239 @@
+"""Seeded synthetic scenes in SPH2O's scene-JSON schema.
+
+The schema is the one SPH2O's loader reads (src/SPH2O/SceneLoader.cpp:40-209):
+"Configuration", "Fluid" {"viscosityMethod", "surfaceTensionMethod",
+"adhesionMethod", "FluidModel": [...]}, "Boundary": [{"box", "sphere",
+"geometry"}]. Every boundary carries "sphere" and "geometry" lists even when
+empty, because the reference indexes both keys unconditionally
+(SceneLoader.cpp:161-162). Two extra "Configuration" keys, "jitter" and
+"jitterSeed", describe the seeded lattice perturbation (host/scene_rng.h);
+the reference loader ignores them.
+
+All real values are rounded to float32 before they are written, so the FP32
+and FP64 builds of the reference read the same numbers.
+
+Workloads (fluid kept at the stated particle counts; tanks enlarged where the
+fluid would otherwise touch or cross the walls, fluid placed 4r from walls):
+  dam_break_wcsph_8k     WCSPH, 20^3 lattice, r=0.025, Tait k=400 gamma=7,
+                         artificial viscosity 0.01, dt=1e-4 fixed
+  dam_break_dfsph_125k   DFSPH + Akinci surface tension 0.05, 50^3, r=0.01
+  double_dam_break_1m    DFSPH or PCISPH, 2 x 100x100x50 blocks, r=0.005,
+                         4x2x2 m tank with a sphere obstacle R=0.2
+  adjoint_wcsph_32k      WCSPH, 32^3, r=0.02
+"""
+from __future__ import annotations
+
+import json
+import math
+
+import numpy as np
+
+WCSPH, PCISPH, DFSPH = 0, 1, 2
+BOUNDARY_CUBE, BOUNDARY_PCISPH, BOUNDARY_AKINCI = 0, 1, 2
+VISC_STANDARD, VISC_ARTIFICIAL, VISC_XSPH = 0, 1, 2
+SURFACE_TENSION_AKINCI = 3
+ADHESION_AKINCI = 4
+
+
+def f32(x):
+    """Round to float32 and return a Python float holding that exact value."""
+    if isinstance(x, (list, tuple)):
+        return [f32(v) for v in x]
+    return float(np.float32(x))
+
+
+def scene(
+    *,
+    method: int,
+    radius: float,
+    blocks,
+    tank,
+    spheres=(),
+    gravity=(0.0, 0.0, -9.81),
+    time_step=1e-4,
+    min_time_step=1e-6,
+    max_time_step=1e-3,
+    fps=60.0,
+    end_time=1000.0,
+    stiffness=400.0,
+    gamma=7.0,
+    eta=1e-3,
+    eta_v=1e-3,
+    min_iterations=2,
+    max_iterations=100,
+    min_iterations_v=1,
+    max_iterations_v=100,
+    cfl=1.0,
+    viscosity_method=VISC_ARTIFICIAL,
+    viscosity=0.01,
+    boundary_viscosity=0.0,
+    surface_tension_method=-1,
+    surface_tension=0.0,
+    adhesion_method=-1,
+    adhesion=0.0,
+    density0=1000.0,
+    jitter=0.01,
+    seed=1,
+):
+    """Build one scene dict. `blocks` are (min, max) pairs; `tank` is (min, max)."""
+    cfg = {
+        "startTime": 0.0,
+        "endTime": f32(end_time),
+        "timeStep": f32(time_step),
+        "fps": f32(fps),
+        "minTimeStep": f32(min_time_step),
+        "maxTimeStep": f32(max_time_step),
+        "gravity": f32(list(gravity)),
+        "particleRadius": f32(radius),
+        "simulationMethod": int(method),
+        "boundaryMethod": BOUNDARY_AKINCI,
+        "cflFactor": f32(cfl),
+        "jitter": f32(jitter),
+        "jitterSeed": int(seed),
+    }
+    if method == WCSPH:
+        cfg.update(stiffness=f32(stiffness), gamma=f32(gamma))
+    elif method == PCISPH:
+        cfg.update(eta=f32(eta), minIterations=int(min_iterations), maxIterations=int(max_iterations))
+    else:
+        cfg.update(
+            eta=f32(eta),
+            etaV=f32(eta_v),
+            minIterations=int(min_iterations),
+            maxIterations=int(max_iterations),
+            minIterationsV=int(min_iterations_v),
+            maxIterationsV=int(max_iterations_v),
+        )
+    fluid_model = {
+        "density0": f32(density0),
+        "viscosity": f32(viscosity),
+        "boundaryViscosity": f32(boundary_viscosity),
+        "surfaceTension": f32(surface_tension),
+        "adhesion": f32(adhesion),
+        "fluidBlocks": [{"min": f32(list(lo)), "max": f32(list(hi))} for lo, hi in blocks],
+    }
+    return {
+        "Configuration": cfg,
+        "Fluid": {
+            "viscosityMethod": int(viscosity_method),
+            "surfaceTensionMethod": int(surface_tension_method),
+            "adhesionMethod": int(adhesion_method),
+            "FluidModel": [fluid_model],
+        },
+        "Boundary": [
+            {
+                "box": [{"min": f32(list(tank[0])), "max": f32(list(tank[1]))}],
+                "sphere": [{"pos": f32(list(c)), "radius": f32(rad)} for c, rad in spheres],
+                "geometry": [],
+            }
+        ],
+    }
+
+
+def block(n, radius, lo):
+    """Lattice block of n = (nx, ny, nz) particles at spacing 2r starting at lo.
+    The max corner sits half a spacing beyond the last particle so that the
+    reference's count floor((max - min) / 2r + 1e-5) (FluidObject.cpp:38) is n
+    without depending on float rounding."""
+    d = 2.0 * radius
+    lo = [float(np.float32(v)) for v in lo]
+    return (lo, [lo[k] + (n[k] + 0.5) * d for k in range(3)])
+
+
+def dam_break_wcsph_8k(seed=1):
+    r = 0.025
+    return scene(
+        method=WCSPH, radius=r, blocks=[block((20, 20, 20), r, (4 * r,) * 3)],
+        tank=((0, 0, 0), (2.0, 1.2, 1.2)), time_step=1e-4, stiffness=400.0, gamma=7.0,
+        viscosity=0.01, seed=seed,
+    )
+
+
+def dam_break_dfsph_125k(seed=2):
+    r = 0.01
+    return scene(
+        method=DFSPH, radius=r, blocks=[block((50, 50, 50), r, (4 * r,) * 3)],
+        tank=((0, 0, 0), (2.0, 1.08, 1.08)), time_step=1e-4, min_time_step=1e-6,
+        max_time_step=1e-3, eta=1e-4, eta_v=1e-3, viscosity=0.01,
+        surface_tension_method=SURFACE_TENSION_AKINCI, surface_tension=0.05, seed=seed,
+    )
+
+
+def double_dam_break_1m(method=DFSPH, seed=3):
+    r = 0.005
+    a = block((100, 100, 50), r, (4 * r, 4 * r, 4 * r))
+    b = block((100, 100, 50), r, (4.0 - 4 * r - 1.0, 2.0 - 4 * r - 1.0, 4 * r))
+    return scene(
+        method=method, radius=r, blocks=[a, b], tank=((0, 0, 0), (4.0, 2.0, 2.0)),
+        spheres=[((2.0, 1.0, 0.3), 0.2)], time_step=1e-4 if method == DFSPH else 5e-4,
+        min_time_step=1e-6, max_time_step=1e-3,
+        eta=1e-4 if method == DFSPH else 0.01, eta_v=1e-3, viscosity=0.01, seed=seed,
+    )
+
+
+def adjoint_wcsph_32k(seed=5):
+    r = 0.02
+    return scene(
+        method=WCSPH, radius=r, blocks=[block((32, 32, 32), r, (4 * r,) * 3)],
+        tank=((0, 0, 0), (2.5, 1.28 + 8 * r, 1.28 + 8 * r)), time_step=2e-4,
+        stiffness=400.0, gamma=7.0, viscosity=0.01, seed=seed,
+    )
+
+
+def small(method=DFSPH, n=(10, 10, 10), radius=0.025, surface_tension=0.0,
+          viscosity_method=VISC_ARTIFICIAL, viscosity=0.01, boundary_viscosity=0.0,
+          adhesion=0.0, sphere=False, seed=11, **kw):
+    """Small tank scene for parity tests: n lattice block at 4r inset in a tank
+    2 x the block plus margins along x."""
+    r = radius
+    blk = block(n, r, (4 * r,) * 3)
+    ext = [n[k] * 2 * r for k in range(3)]
+    tank = ((0, 0, 0), (2 * ext[0] + 8 * r, ext[1] + 8 * r, ext[2] + 8 * r))
+    spheres = [((ext[0] + 8 * r, 0.5 * tank[1][1], 4 * r + 0.25 * ext[2]), 0.15 * ext[2])] if sphere else []
+    return scene(
+        method=method, radius=r, blocks=[blk], tank=tank, spheres=spheres,
+        viscosity_method=viscosity_method, viscosity=viscosity,
+        boundary_viscosity=boundary_viscosity,
+        surface_tension_method=SURFACE_TENSION_AKINCI if surface_tension else -1,
+        surface_tension=surface_tension,
+        adhesion_method=ADHESION_AKINCI if adhesion else -1, adhesion=adhesion,
+        seed=seed, **kw,
+    )
+
+
+def batched_scene_params(count=256, seed=4):
+    """Per-scene parameters of the batched workload: N_f log-uniform in
+    [2000, 40000], block aspect ratios uniform in [0.5, 2] (normalised so the
+    lattice holds about N_f particles), viscosity uniform in [0.005, 0.05],
+    r = 0.01, each in its own tank sized to the block."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nf = math.exp(rng.uniform(math.log(2000), math.log(40000)))
+        ax, ay = rng.uniform(0.5, 2.0, size=2)
+        visc = float(rng.uniform(0.005, 0.05))
+        # nx : ny : nz = ax : ay : 1 with nx*ny*nz ~= nf
+        nz = (nf / (ax * ay)) ** (1.0 / 3.0)
+        dims = (max(2, int(round(ax * nz))), max(2, int(round(ay * nz))), max(2, int(round(nz))))
+        out.append({"dims": dims, "viscosity": visc})
+    return out
+
+
+def batched_scenes(count=256, method=WCSPH, seed=4):
+    r = 0.01
+    scenes = []
+    for i, p in enumerate(batched_scene_params(count, seed)):
+        nx, ny, nz = p["dims"]
+        ext = (nx * 2 * r, ny * 2 * r, nz * 2 * r)
+        tank = ((0, 0, 0), (max(1.0, 2 * ext[0] + 8 * r), max(1.0, ext[1] + 8 * r), max(1.0, ext[2] + 8 * r)))
+        scenes.append(scene(
+            method=method, radius=r, blocks=[block((nx, ny, nz), r, (4 * r,) * 3)], tank=tank,
+            time_step=1e-4, viscosity=p["viscosity"], eta=1e-3, eta_v=1e-3, seed=1000 + i,
+        ))
+    return scenes
+
+
+def write(scene_dict, path):
+    with open(path, "w") as f:
+        json.dump(scene_dict, f, indent=1)
+    return path
