@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 particle pipeline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Default workload: the large single-scene double dam break, DFSPH, 1,000,000
+fluid + 409,599 Akinci boundary particles (r = 0.005 m, 4 x 2 x 2 m tank,
+sphere obstacle R = 0.2 m), seeded synthetic lattice. One "step" is one
+DFSPH time step of the whole scene. `value` is fluid particle-steps/s with
+the state resident in HBM, timed with CUDA events recorded by the library on
+the stream its kernels run on; `e2e` is the same metric through the public C
+ABI with host buffers (state uploaded from pinned host memory at the start,
+stats read back every step, state read back at the end).
+
+With N > 1 (torchrun) every rank runs an independent replica of the scene
+(the single-scene path does not shard): weak scaling, value = all ranks'
+particle-steps / max-over-ranks device time.
+
+--impl reference times SPH2O's own OpenMP CPU path (the reference sources
+built by oracle/Makefile, fast-math + OpenMP variant) on the host cores for
+the same scene; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s (DFSPH 1M, batched 256 scenes, WCSPH adjoint) at ≤0.1% ρ err"
+UNIT = "particle-steps/s"
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "sph2o_ref_fast")
+FALLBACK_HBM_GBS = 6650.0
+
+# Algorithmic HBM bytes per fluid particle for each timed phase (FP32, vec3 =
+# 12 B, each quantity read/written once per unavoidable global dependency).
+# Boundary traffic is counted per pass as 16 B per boundary particle that has
+# a fluid neighbour; it is added by bytes_per_launch().
+BYTES = {
+    "sort": 52,            # read pos+vel 24, write reordered 24, cell offset 4
+    "lists": 52 + 4,       # read pos 12 (+ 4 B count), neighbour indices written: counted separately
+    "density": 20,         # read pos 12, write rho + alpha 8
+    "normals": 28,         # read pos, rho -> n
+    "forces": 52,          # read pos, v, rho, n -> a (viscosity + surface tension)
+    "predict": 36,         # read v, a; write v
+    "warm_start": 76,      # residual 36 + correction 40
+    "iteration": 84,       # residual + k 44, correction 40
+    "positions": 36,       # read x, v; write x
+}
+
+
+def workloads():
+    from sph2o_b200 import scenes as S
+    return {
+        "double_dam_break_dfsph_1m": ("double dam break DFSPH, 1,000,000 fluid + 409,599 boundary particles, "
+                                      "r=0.005 m, 4x2x2 m tank, sphere R=0.2 m", lambda: S.double_dam_break_1m()),
+        "double_dam_break_pcisph_1m": ("double dam break PCISPH, 1,000,000 fluid + 409,599 boundary particles",
+                                       lambda: S.double_dam_break_1m(method=S.PCISPH)),
+        "dam_break_dfsph_125k": ("DFSPH dam break + Akinci surface tension, 125,000 fluid, r=0.01 m",
+                                 lambda: S.dam_break_dfsph_125k()),
+        "dam_break_wcsph_8k": ("WCSPH dam break, 8,000 fluid, r=0.025 m", lambda: S.dam_break_wcsph_8k()),
+        "wcsph_32k": ("WCSPH block, 32,768 fluid, r=0.02 m", lambda: S.adjoint_wcsph_32k()),
+    }
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+               "-i", str(self.gpu_id)]
+        self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 8:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=5)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[0]) for r in self.rows if num(r[0]) is not None]
+        mx = [num(r[1]) for r in self.rows if num(r[1]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[4 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_run(scene_dict, steps, warmup, threads=None):
+    """Time SPH2O's OpenMP CPU path on this host for the given scene."""
+    if not os.path.exists(REF_BIN):
+        return None, "reference build missing (oracle/_ref/sph2o_ref_fast; run make -C oracle)"
+    threads = threads or os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close", OMP_PLACES="cores")
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "scene.json")
+        with open(path, "w") as f:
+            json.dump(scene_dict, f)
+        r = subprocess.run([REF_BIN, "-c", path, "--mode", "time", "--steps", str(steps), "--warmup", str(warmup),
+                            "--threads", str(threads)], capture_output=True, text=True, env=env, timeout=1800)
+    if r.returncode != 0:
+        return None, f"reference run failed: {r.stderr.strip()[-200:]}"
+    line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
+    out = json.loads(line)
+    out["threads"] = threads
+    return out, None
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def bytes_per_launch(phase, nf, nb_active, its):
+    if phase == "density_solve":
+        per = BYTES["predict"] + BYTES["warm_start"] + its * BYTES["iteration"] + BYTES["positions"]
+        passes = 2 + 2 * its
+    elif phase == "divergence_solve":
+        per = BYTES["warm_start"] + its * BYTES["iteration"]
+        passes = 2 + 2 * its
+    else:
+        per = BYTES.get(phase, 0)
+        passes = 1
+    return nf * per + 16 * nb_active * passes
+
+
+def run_reference_arm(args, name, desc, scene_dict, world, rank):
+    if rank != 0:
+        return 0
+    steps = max(1, min(args.steps, 10))
+    warm = max(1, min(args.warmup, 2))
+    res, err = reference_run(scene_dict, steps, warm)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return 0
+    v = res["particle_steps_per_s"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": warm, "ms_per_step": 1e3 * res["seconds"] / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": desc, "fluid_particles": res["fluid_particles"],
+                   "boundary_particles": res["boundary_particles"], "mean_iterations": res["mean_iterations"],
+                   "mean_iterations_v": res["mean_iterations_v"]},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": res["threads"], "kind": "reference",
+                         "sample": f"{steps} timed steps after {warm} warm-up steps of the same scene, "
+                                   f"SPH2O sources built -O3 -ffast-math -fopenmp, {cpu_model()}"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="double_dam_break_dfsph_1m")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    name = args.workload
+    desc, make = workloads()[name]
+    scene_dict = make()
+
+    if args.impl == "reference":
+        return run_reference_arm(args, name, desc, scene_dict, world, rank)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from sph2o_b200.api import Scene, Simulation, select_device
+
+    select_device(local)
+    scene = Scene.from_dict(scene_dict)
+    sim = Simulation.from_scene(scene)
+    nf, nb = sim.nf, sim.nb
+    warm_stats = sim.step(args.warmup) if args.warmup > 0 else None
+
+    gpu_uuid = torch.cuda.get_device_properties(local).uuid
+    sampler = ClockSampler(f"GPU-{gpu_uuid}" if gpu_uuid else local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    sim.profile(True)
+    t0 = time.perf_counter()
+    stats = sim.step(args.steps)
+    wall = time.perf_counter() - t0
+    prof = sim.profile_read()
+    sim.profile(False)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+
+    dev_ms = stats["device_ms"]
+    t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * nf * args.steps / (max_ms / 1e3)
+    its = stats["total_iterations"] / max(args.steps, 1)
+    itsv = stats["total_iterations_v"] / max(args.steps, 1)
+
+    # roofline of the dominant kernel (largest device time in the timed region)
+    peak, peak_kind = hbm_peak()
+    dom = max((k for k in prof if prof[k]["launches"]), key=lambda k: prof[k]["ms"])
+    launches = prof[dom]["launches"]
+    avg_ms = prof[dom]["ms"] / launches
+    it_for = its if dom == "density_solve" else itsv
+    nb_active = nb  # upper bound of boundary particles with a fluid neighbour
+    algo = bytes_per_launch(dom, nf, nb_active, it_for)
+    achieved = algo / (avg_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": dom, "peak_kind": f"of {peak_kind}",
+                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": avg_ms}
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    ke = min(args.steps, 50)
+    x, v, _ = sim.state()
+    px = torch.empty((nf, 3), dtype=torch.float32, pin_memory=True).numpy()
+    pv = torch.empty((nf, 3), dtype=torch.float32, pin_memory=True).numpy()
+    pr = torch.empty(nf, dtype=torch.float32, pin_memory=True).numpy()
+    px[:] = x
+    pv[:] = v
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    sim.set_state(px, pv)
+    for _ in range(ke):
+        sim.step(1)
+    from sph2o_b200.api import _fptr, lib
+    rc = lib().sph_get_state(sim._h, _fptr(px), _fptr(pv), _fptr(pr))
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    if rc == 0:
+        e2e = {"value": world * nf * ke / float(te.item()), "unit": UNIT,
+               "h2d_bytes_per_step": (nf * 24) // ke,
+               "d2h_bytes_per_step": 112 + (nf * 28) // ke,
+               "steps": ke}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res, err = reference_run(scene_dict, 3, 1)
+        if res is not None:
+            cpu = {"value": res["particle_steps_per_s"], "unit": UNIT, "cores": res["threads"], "kind": "reference",
+                   "sample": f"3 timed steps after 1 warm-up step of the same scene (SPH2O sources, -O3 "
+                             f"-ffast-math -fopenmp, {cpu_model()}); mean iterations {res['mean_iterations']:.2f}"
+                             f" + {res['mean_iterations_v']:.2f}"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference", "sample": err}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": desc, "fluid_particles": nf, "boundary_particles": nb,
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "mean_iterations": its, "mean_iterations_v": itsv,
+                   "last_avg_density_error": stats["avg_density_error"],
+                   "density_error_gate": bool(stats["avg_density_error"] <= 1e-3),
+                   "simulated_time_s": stats["time"], "dt": stats["dt"],
+                   "l2": "working set (particle state + neighbour lists) larger than the 126 MB L2",
+                   "wall_s": wall},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": stats["kernel_launches"],
+        "clocks": clocks,
+        "phases_ms_per_step": {k: prof[k]["ms"] / args.steps for k in prof if prof[k]["launches"]},
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    sim.close()
+    scene.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

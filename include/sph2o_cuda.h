@@ -89,11 +89,33 @@ typedef struct sph_step_stats {
     unsigned long long total_iterations_v;
     unsigned steps;                 /* steps taken by this call */
     unsigned neighbor_overflows;    /* particles whose neighbour list was truncated */
+    double device_ms;               /* device time of the steps of this call (CUDA
+                                       events on the context stream) */
+    unsigned long long kernel_launches; /* kernels this call launched */
 } sph_step_stats;
+
+/* Per-phase device timing (CUDA events around each phase on the context
+   stream). Phases of one step, in launch order: */
+enum sph_profile_phase {
+    SPH_PROF_SORT = 0,        /* cell keys, counting sort, reorder        */
+    SPH_PROF_LISTS = 1,       /* neighbour-list build                      */
+    SPH_PROF_DENSITY = 2,     /* density (+alpha, +EOS)                    */
+    SPH_PROF_NORMALS = 3,     /* surface-tension normals                   */
+    SPH_PROF_FORCES = 4,      /* non-pressure forces (+WCSPH pressure, integrate) */
+    SPH_PROF_DENSITY_SOLVE = 5,  /* DFSPH density solver (persistent kernel) */
+    SPH_PROF_DIVERGENCE_SOLVE = 6,/* DFSPH divergence solver (persistent kernel) */
+    SPH_PROF_PRESSURE_SOLVE = 7, /* PCISPH pressure solver (persistent kernel) */
+    SPH_PROF_COUNT = 8
+};
 
 typedef struct sph_ctx sph_ctx;
 
 /* ---- context lifecycle ------------------------------------------------ */
+
+/* Make `device` the current CUDA device of the calling thread for this
+   library (contexts created afterwards live on it). No reference counterpart:
+   SPH2O is CPU-only. */
+int sph_select_device(int device);
 
 /* Replaces SPHSimulation::setSimulationMethod + the solver constructors
    (SPHSimulation.cpp:216-239, 316-350). Selects the device with
@@ -126,6 +148,12 @@ int sph_step(sph_ctx* ctx, int nsteps, sph_step_stats* out);
    the status of everything queued since the last wait. */
 int sph_step_async(sph_ctx* ctx, int nsteps);
 int sph_sync(sph_ctx* ctx, sph_step_stats* out);
+
+/* Enable (1) or disable (0) per-phase event timing; enabling clears the totals. */
+int sph_profile_enable(sph_ctx* ctx, int enable);
+/* Accumulated per-phase device milliseconds and launch counts since enabling
+   (arrays of SPH_PROF_COUNT; either may be NULL). Waits for queued work. */
+int sph_profile_read(sph_ctx* ctx, double* ms, unsigned long long* launches);
 
 /* Fluid state in the caller's particle order. Any pointer may be NULL.
    rho is FluidObject::density as SPH2O leaves it after a step. */
@@ -177,6 +205,13 @@ int sph_compute_phase(sph_ctx* ctx, int phase, float* out);
 int sph_debug_neighbors(sph_ctx* ctx, unsigned* f_offsets, unsigned* f_index, size_t f_cap,
                         unsigned* b_offsets, unsigned* b_index, size_t b_cap,
                         size_t* nf_total, size_t* nb_total);
+
+/* Test hook for the bounded device-side waits (no reference counterpart):
+   launches a two-block cooperative kernel in which one block never reaches
+   the grid barrier. The waiting block gives up after its spin limit (about
+   a second), records the timeout and returns; the call then reports
+   SPH_ERR_TIMEOUT and clears the flag, leaving the context usable. */
+int sph_debug_barrier_timeout(sph_ctx* ctx);
 
 /* ---- host scene loading (SceneLoader + object builders) --------------- */
 

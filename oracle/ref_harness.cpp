@@ -203,18 +203,22 @@ void load_state(SPHSimulation* sim, const std::string& path)
     }
 }
 
+/* Replace the boundary particle set: all injected points go to boundary
+   object 0 (volumes are computed over the neighbours of every object alike,
+   AkinciBoundaryObject.cpp:22-29, so the split between objects does not
+   matter); the other objects are emptied. The FP64 build samples boxes with
+   a different particle count, so it cannot be overwritten in place. */
 void load_boundary(SPHSimulation* sim, const std::string& path)
 {
     auto arrs = read_sphd(path);
     const Array& p = arrs.at("bpos");
-    uint64_t off = 0;
-    for (uint b = 0; b < sim->numberBoundaryModels(); ++b) {
-        BoundaryObject* bo = sim->getBoundaryModel(b);
-        for (uint i = 0; i < bo->getSize(); ++i, ++off)
-            for (int k = 0; k < 3; ++k) bo->getPosition(i)[k] = (Real)elem(p, 3 * off + k);
-    }
-    if (off != p.shape[0]) { fprintf(stderr, "boundary count mismatch %llu vs %llu\n",
-                                     (unsigned long long)off, (unsigned long long)p.shape[0]); exit(2); }
+    if (sim->numberBoundaryModels() == 0) { fprintf(stderr, "scene has no boundary object\n"); exit(2); }
+    const uint n = (uint)p.shape[0];
+    for (uint b = 1; b < sim->numberBoundaryModels(); ++b) sim->getBoundaryModel(b)->resize(0);
+    BoundaryObject* bo = sim->getBoundaryModel(0);
+    bo->resize(n);
+    for (uint i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) bo->getPosition(i)[k] = (Real)elem(p, 3ull * i + k);
 }
 
 std::vector<Real> fluid_vec3(FluidObject* fo, int which)

@@ -27,6 +27,9 @@ STATUS = {
     -7: "SPH_ERR_NO_DEVICE", -8: "SPH_ERR_IO", -9: "SPH_ERR_CAPACITY",
 }
 PHASE_DENSITY, PHASE_ALPHA, PHASE_NONPRESSURE_ACC, PHASE_PRESSURE, PHASE_PRESSURE_ACC = range(5)
+PROF_NAMES = ["sort", "lists", "density", "normals", "forces", "density_solve", "divergence_solve",
+              "pressure_solve"]
+PROF_COUNT = len(PROF_NAMES)
 
 
 class SceneDesc(C.Structure):
@@ -52,6 +55,7 @@ class StepStats(C.Structure):
         ("dt", C.c_float), ("max_velocity", C.c_float), ("iterations", C.c_uint), ("iterations_v", C.c_uint),
         ("total_iterations", C.c_ulonglong), ("total_iterations_v", C.c_ulonglong),
         ("steps", C.c_uint), ("neighbor_overflows", C.c_uint),
+        ("device_ms", C.c_double), ("kernel_launches", C.c_ulonglong),
     ]
 
     def as_dict(self):
@@ -77,6 +81,7 @@ def lib():
     L = C.CDLL(LIB_PATH)
     P, U, I, F = C.c_void_p, C.c_uint, C.c_int, C.POINTER(C.c_float)
     sigs = {
+        "sph_select_device": (I, [I]),
         "sph_create": (I, [C.POINTER(SceneDesc), C.POINTER(P)]),
         "sph_set_fluid": (I, [P, U, F, F]),
         "sph_set_boundary": (I, [P, U, F]),
@@ -96,6 +101,9 @@ def lib():
         "sph_compute_phase": (I, [P, I, F]),
         "sph_debug_neighbors": (I, [P, C.POINTER(U), C.POINTER(U), C.c_size_t, C.POINTER(U), C.POINTER(U),
                                     C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+        "sph_debug_barrier_timeout": (I, [P]),
+        "sph_profile_enable": (I, [P, I]),
+        "sph_profile_read": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
         "sph_scene_load": (I, [C.c_char_p, C.POINTER(P)]),
         "sph_scene_parse": (I, [C.c_char_p, C.POINTER(P)]),
         "sph_scene_get_desc": (I, [P, C.POINTER(SceneDesc)]),
@@ -121,6 +129,12 @@ def _fptr(a):
 
 def _uptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_uint)) if a is not None else None
+
+
+def select_device(device: int):
+    rc = lib().sph_select_device(int(device))
+    if rc != SPH_OK:
+        raise SphError(rc, lib().sph_global_error().decode())
 
 
 class Scene:
@@ -244,6 +258,15 @@ class Simulation:
         out = np.zeros((self.nf, 3) if vec else self.nf, np.float32)
         self._check(lib().sph_compute_phase(self._h, int(phase), _fptr(out)))
         return out
+
+    def profile(self, enable=True):
+        self._check(lib().sph_profile_enable(self._h, 1 if enable else 0))
+
+    def profile_read(self):
+        ms = (C.c_double * PROF_COUNT)()
+        n = (C.c_ulonglong * PROF_COUNT)()
+        self._check(lib().sph_profile_read(self._h, ms, n))
+        return {PROF_NAMES[i]: {"ms": ms[i], "launches": n[i]} for i in range(PROF_COUNT)}
 
     def neighbors(self):
         """CSR neighbour sets (caller order): (f_off, f_idx, b_off, b_idx)."""

@@ -69,6 +69,16 @@ struct sph_ctx {
     int grid_density = 0, grid_div = 0, grid_pcisph = 0;
     DevState last{};
     bool lists_valid = false;
+    /* timing: batch events + per-phase profiling */
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+    bool batch_open = false;
+    unsigned long long launches = 0, launches_at_open = 0;
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    struct Pending { int phase; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    double prof_ms[SPH_PROF_COUNT] = {};
+    unsigned long long prof_launch[SPH_PROF_COUNT] = {};
 };
 
 namespace {
@@ -214,6 +224,54 @@ int check_launch(sph_ctx* c, const char* what)
     return SPH_OK;
 }
 
+cudaEvent_t take_event(sph_ctx* c)
+{
+    if (!c->ev_pool.empty()) {
+        cudaEvent_t e = c->ev_pool.back();
+        c->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+/* Brackets one phase with events when profiling; counts its kernel launches. */
+struct Phase {
+    sph_ctx* c;
+    int phase;
+    int kernels;
+    cudaEvent_t a = nullptr;
+    Phase(sph_ctx* ctx, int ph, int nk) : c(ctx), phase(ph), kernels(nk)
+    {
+        if (c->prof) {
+            a = take_event(c);
+            cudaEventRecord(a, c->stream);
+        }
+    }
+    ~Phase()
+    {
+        c->launches += (unsigned long long)kernels;
+        if (c->prof) {
+            cudaEvent_t b = take_event(c);
+            cudaEventRecord(b, c->stream);
+            c->pending.push_back({phase, a, b});
+            c->prof_launch[phase] += (unsigned long long)kernels;
+        }
+    }
+};
+
+void drain_profile(sph_ctx* c)
+{
+    for (auto& p : c->pending) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) c->prof_ms[p.phase] += ms;
+        c->ev_pool.push_back(p.a);
+        c->ev_pool.push_back(p.b);
+    }
+    c->pending.clear();
+}
+
 int alloc_lists(sph_ctx* c)
 {
     int rc;
@@ -234,8 +292,11 @@ int neighbor_search(sph_ctx* c)
         g.f_in[0] = c->kws; g.f_out[0] = c->kws2;
         g.f_in[1] = c->kvws; g.f_out[1] = c->kvws2;
     }
-    launch_sort(c->P, (int)c->nf, c->pos, c->cell_count, c->cell_start, c->block_sums, c->cell_of, c->slot,
-                c->tmp_key, c->tmp_src, c->orig, g, c->stream);
+    {
+        Phase ph(c, SPH_PROF_SORT, 6);
+        launch_sort(c->P, (int)c->nf, c->pos, c->cell_count, c->cell_start, c->block_sums, c->cell_of, c->slot,
+                    c->tmp_key, c->tmp_src, c->orig, g, c->stream);
+    }
     std::swap(c->pos, c->pos2);
     std::swap(c->vel, c->vel2);
     std::swap(c->orig, c->orig2);
@@ -243,8 +304,11 @@ int neighbor_search(sph_ctx* c)
         std::swap(c->kws, c->kws2);
         std::swap(c->kvws, c->kvws2);
     }
-    launch_build_lists(c->P, c->pos, c->cell_start, c->bpos, c->bcell_start, c->nbr_f, c->cnt_f, c->nbr_b, c->cnt_b,
-                       c->st, c->stream);
+    {
+        Phase ph(c, SPH_PROF_LISTS, 1);
+        launch_build_lists(c->P, c->pos, c->cell_start, c->bpos, c->bcell_start, c->nbr_f, c->cnt_f, c->nbr_b,
+                           c->cnt_b, c->st, c->stream);
+    }
     c->lists_valid = true;
     return check_launch(c, "neighbour search");
 }
@@ -260,9 +324,9 @@ int step_wcsph(sph_ctx* c)
     int rc;
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     DeviceArrays A = arrays(c);
-    launch_density(c->P, A, false, true, c->stream);
-    if (c->P.st_on) launch_normals(c->P, A, c->stream);
-    launch_forces(c->P, A, FORCE_WCSPH, c->stream);
+    { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, false, true, c->stream); }
+    if (c->P.st_on) { Phase ph(c, SPH_PROF_NORMALS, 1); launch_normals(c->P, A, c->stream); }
+    { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_WCSPH, c->stream); }
     std::swap(c->pos, c->pos2);
     std::swap(c->vel, c->vel2);
     c->lists_valid = false;
@@ -274,11 +338,12 @@ int step_pcisph(sph_ctx* c)
     int rc;
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     DeviceArrays A = arrays(c);
-    launch_density(c->P, A, false, false, c->stream);
-    if (c->P.st_on) launch_normals(c->P, A, c->stream);
-    launch_forces(c->P, A, FORCE_NP, c->stream);
+    { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, false, false, c->stream); }
+    if (c->P.st_on) { Phase ph(c, SPH_PROF_NORMALS, 1); launch_normals(c->P, A, c->stream); }
+    { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_NP, c->stream); }
     if ((rc = zero_accum(c)) != SPH_OK) return rc;
-    const int e = launch_pcisph_solve(c->P, A, c->grid_pcisph, c->stream);
+    int e;
+    { Phase ph(c, SPH_PROF_PRESSURE_SOLVE, 1); e = launch_pcisph_solve(c->P, A, c->grid_pcisph, c->stream); }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("pcisph solver launch: ") + cudaGetErrorString((cudaError_t)e));
     c->lists_valid = true;
     return check_launch(c, "pcisph step");
@@ -288,16 +353,17 @@ int step_dfsph(sph_ctx* c)
 {
     int rc;
     DeviceArrays A = arrays(c);
-    if (c->P.st_on) launch_normals(c->P, A, c->stream);
-    launch_forces(c->P, A, FORCE_NP_CFL, c->stream);
+    if (c->P.st_on) { Phase ph(c, SPH_PROF_NORMALS, 1); launch_normals(c->P, A, c->stream); }
+    { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_NP_CFL, c->stream); }
     if ((rc = zero_accum(c)) != SPH_OK) return rc;
-    int e = launch_dfsph_solve(c->P, A, false, c->grid_density, c->stream);
+    int e;
+    { Phase ph(c, SPH_PROF_DENSITY_SOLVE, 1); e = launch_dfsph_solve(c->P, A, false, c->grid_density, c->stream); }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph density solver launch: ") + cudaGetErrorString((cudaError_t)e));
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     A = arrays(c);
-    launch_density(c->P, A, true, false, c->stream);
+    { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, true, false, c->stream); }
     A.accum = c->accum + c->accum_len / 2;
-    e = launch_dfsph_solve(c->P, A, true, c->grid_div, c->stream);
+    { Phase ph(c, SPH_PROF_DIVERGENCE_SOLVE, 1); e = launch_dfsph_solve(c->P, A, true, c->grid_div, c->stream); }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph divergence solver launch: ") + cudaGetErrorString((cudaError_t)e));
     return check_launch(c, "dfsph step");
 }
@@ -360,6 +426,13 @@ int fill_stats(sph_ctx* c, const DevState& before, const DevState& now, sph_step
 } // namespace
 
 extern "C" {
+
+int sph_select_device(int device)
+{
+    const cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(nullptr, SPH_ERR_NO_DEVICE, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    return SPH_OK;
+}
 
 int sph_create(const sph_scene_desc* desc, sph_ctx** out)
 {
@@ -480,6 +553,8 @@ int sph_init(sph_ctx* c)
     c->accum_len = 2 * ((size_t)P.max_it + 2);
     if ((rc = dalloc(c, &c->accum, c->accum_len)) != SPH_OK) return rc;
     CUDA_TRY(c, cudaMallocHost((void**)&c->st_host, sizeof(DevState)));
+    CUDA_TRY(c, cudaEventCreate(&c->ev_begin));
+    CUDA_TRY(c, cudaEventCreate(&c->ev_end));
 
     c->grid_density = persistent_grid(false, false);
     c->grid_div = persistent_grid(false, true);
@@ -541,6 +616,11 @@ int sph_step_async(sph_ctx* c, int nsteps)
     if (!c) return SPH_ERR_ARG;
     if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_step before sph_init");
     if (nsteps < 0) return fail(c, SPH_ERR_ARG, "negative step count");
+    if (!c->batch_open) {
+        CUDA_TRY(c, cudaEventRecord(c->ev_begin, c->stream));
+        c->batch_open = true;
+        c->launches_at_open = c->launches;
+    }
     for (int s = 0; s < nsteps; ++s) {
         int rc;
         switch (c->desc.simulation_method) {
@@ -550,6 +630,7 @@ int sph_step_async(sph_ctx* c, int nsteps)
         }
         if (rc != SPH_OK) return rc;
     }
+    CUDA_TRY(c, cudaEventRecord(c->ev_end, c->stream));
     return SPH_OK;
 }
 
@@ -561,6 +642,13 @@ int sph_sync(sph_ctx* c, sph_step_stats* out)
     int rc = read_state(c, &now);
     if (rc != SPH_OK) return rc;
     fill_stats(c, c->last, now, out);
+    if (c->batch_open) {
+        float ms = 0.0f;
+        if (out && cudaEventElapsedTime(&ms, c->ev_begin, c->ev_end) == cudaSuccess) out->device_ms = ms;
+        if (out) out->kernel_launches = c->launches - c->launches_at_open;
+        c->batch_open = false;
+    }
+    drain_profile(c);
     c->last = now;
     rc = status_from_state(c, now);
     if (rc == SPH_ERR_NEIGHBOR_OVERFLOW) {
@@ -655,6 +743,28 @@ int sph_get_time(sph_ctx* c, double* time, float* dt)
     return SPH_OK;
 }
 
+int sph_profile_enable(sph_ctx* c, int enable)
+{
+    if (!c) return SPH_ERR_ARG;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    drain_profile(c);
+    c->prof = enable != 0;
+    for (int i = 0; i < SPH_PROF_COUNT; ++i) { c->prof_ms[i] = 0.0; c->prof_launch[i] = 0; }
+    return SPH_OK;
+}
+
+int sph_profile_read(sph_ctx* c, double* ms, unsigned long long* launches)
+{
+    if (!c) return SPH_ERR_ARG;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    drain_profile(c);
+    for (int i = 0; i < SPH_PROF_COUNT; ++i) {
+        if (ms) ms[i] = c->prof_ms[i];
+        if (launches) launches[i] = c->prof_launch[i];
+    }
+    return SPH_OK;
+}
+
 unsigned sph_num_fluid(const sph_ctx* c) { return c ? c->nf : 0u; }
 unsigned sph_num_boundary(const sph_ctx* c) { return c ? c->nb : 0u; }
 const char* sph_last_error(const sph_ctx* c) { return c ? c->err.c_str() : "null context"; }
@@ -664,6 +774,10 @@ int sph_destroy(sph_ctx* c)
 {
     if (!c) return SPH_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    drain_profile(c);
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    if (c->ev_begin) cudaEventDestroy(c->ev_begin);
+    if (c->ev_end) cudaEventDestroy(c->ev_end);
     free_all(c);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -708,6 +822,26 @@ int sph_compute_phase(sph_ctx* c, int phase, float* out)
     cudaFreeAsync(tmp, c->stream);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return check_launch(c, "compute_phase");
+}
+
+int sph_debug_barrier_timeout(sph_ctx* c)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_debug_barrier_timeout before sph_init");
+    const int e = launch_barrier_timeout_probe(c->st, c->stream);
+    if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("probe launch: ") + cudaGetErrorString((cudaError_t)e));
+    DevState s{};
+    int rc = read_state(c, &s);
+    if (rc != SPH_OK) return rc;
+    /* reset the barrier and the flag so the context stays usable */
+    DevState fix = s;
+    fix.err &= ~ERRBIT_TIMEOUT;
+    fix.bar_count = 0;
+    CUDA_TRY(c, cudaMemcpyAsync(c->st, &fix, sizeof fix, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->last = fix;
+    if (s.err & ERRBIT_TIMEOUT) return fail(c, SPH_ERR_TIMEOUT, "grid barrier wait ran out (probe)");
+    return SPH_OK;
 }
 
 int sph_debug_neighbors(sph_ctx* c, unsigned* f_offsets, unsigned* f_index, size_t f_cap, unsigned* b_offsets,

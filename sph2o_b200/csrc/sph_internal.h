@@ -78,6 +78,7 @@ void launch_normals(const SimParams& P, const DeviceArrays& A, cudaStream_t s);
 void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, cudaStream_t s);
 int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s);
 int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s);
+int launch_barrier_timeout_probe(DevState* st, cudaStream_t s);
 /* co-resident grid size of the persistent solver kernels (0 on error) */
 int persistent_grid(bool pcisph, bool divergence);
 constexpr int kSolverBlock = 256;

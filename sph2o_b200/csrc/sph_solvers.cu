@@ -581,6 +581,19 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
     }
 }
 
+/* Test kernel: block 1 never arrives, so block 0's wait must run out. */
+__global__ void k_barrier_timeout_probe(DevState* st)
+{
+    if (blockIdx.x == 1) return;
+    grid_barrier(st);
+}
+
+int launch_barrier_timeout_probe(DevState* st, cudaStream_t s)
+{
+    void* args[] = {&st};
+    return (int)cudaLaunchCooperativeKernel((const void*)k_barrier_timeout_probe, dim3(2), dim3(32), args, 0, s);
+}
+
 /* ---------------------------------------------------------------------- */
 
 static inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }

@@ -1,0 +1,72 @@
+"""Host scene loader (C ABI, no GPU): the particles it generates are
+bit-identical to the reference's FluidObject::build + jitter and
+AkinciBoundaryObject::sampleCube / sampleSphere, and malformed scenes fail
+with status codes instead of exceptions or asserts."""
+import copy
+import json
+
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+from sph2o_b200 import scenes as S
+from sph2o_b200.api import SPH_OK, Scene, SphError, lib
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_particles_bit_exact(name):
+    g = load_golden(name)
+    sc = Scene.from_dict(g["scene"])
+    x, v = sc.fluid()
+    assert np.array_equal(x, g["init_pos"])
+    assert np.array_equal(sc.boundary(), g["bpos"])
+    assert not v.any()
+
+
+def test_desc_fields():
+    sc = Scene.from_dict(S.dam_break_dfsph_125k())
+    d = sc.desc()
+    assert d.simulation_method == S.DFSPH and d.boundary_method == 2
+    assert d.surface_tension_method == 3 and abs(d.surface_tension - 0.05) < 1e-7
+    assert d.min_iterations == 2 and d.max_iterations == 100
+    assert abs(d.particle_radius - 0.01) < 1e-9
+
+
+def test_missing_sphere_geometry_keys_tolerated():
+    sc = S.small()
+    for b in sc["Boundary"]:
+        del b["sphere"]
+        del b["geometry"]
+    s2 = Scene.from_dict(sc)
+    assert s2.boundary().shape[0] > 0
+
+
+@pytest.mark.parametrize("mutate,code", [
+    (lambda d: d["Configuration"].pop("timeStep"), -8),
+    (lambda d: d["Fluid"]["FluidModel"].append(copy.deepcopy(d["Fluid"]["FluidModel"][0])), -1),
+    (lambda d: d["Configuration"].__setitem__("boundaryMethod", 0), -1),
+    (lambda d: d["Fluid"]["FluidModel"][0].__setitem__("emitters", [{"type": 0}]), -1),
+    (lambda d: d["Boundary"][0].__setitem__("geometry", [{"path": "x.obj", "spacing": 1.0}]), -1),
+    (lambda d: d["Configuration"].__setitem__("simulationMethod", 7), -8),
+])
+def test_bad_scenes_rejected(mutate, code):
+    d = S.small()
+    mutate(d)
+    with pytest.raises(SphError) as e:
+        Scene.from_dict(d)
+    assert e.value.code == code
+
+
+def test_malformed_json():
+    import ctypes as C
+    h = C.c_void_p()
+    rc = lib().sph_scene_parse(b'{"Configuration": [1, 2', C.byref(h))
+    assert rc == -8
+    assert b"parse error" in lib().sph_scene_error()
+
+
+def test_workload_counts():
+    """Fluid counts of the benchmark scenes (boundary counts from the reference sampler)."""
+    for make, nf in [(S.dam_break_wcsph_8k, 8000), (S.dam_break_dfsph_125k, 125000), (S.adjoint_wcsph_32k, 32768)]:
+        sc = Scene.from_dict(make())
+        assert sc.fluid()[0].shape[0] == nf
