@@ -213,6 +213,42 @@ int sph_debug_neighbors(sph_ctx* ctx, unsigned* f_offsets, unsigned* f_index, si
    SPH_ERR_TIMEOUT and clears the flag, leaving the context usable. */
 int sph_debug_barrier_timeout(sph_ctx* ctx);
 
+/* ---- allocation-free density evaluation ------------------------------- */
+
+/* Fixed capacity of sph_density_noalloc's scratch. */
+#define SPH_NOALLOC_MAX_FLUID 65536u
+#define SPH_NOALLOC_MAX_BOUNDARY 65536u
+#define SPH_NOALLOC_MAX_CELLS 262144u
+
+/* Densities of nf fluid particles, for callers that must not allocate GPU
+   memory: code running inside a host callback or an allocator hook, or in a
+   process whose device memory is pooled by a framework, or on a real-time
+   path that may not take the allocator's locks or its implicit
+   synchronisation. No counterpart in the reference (SPH2O is CPU-only); the
+   density is SPHSolver::computeFluidDensities' sum, equal bit for bit to
+   sph_compute_phase(SPH_PHASE_DENSITY) for the same particles.
+   Inputs and output are device pointers owned by the caller:
+     xyz      nf * 3 floats, fluid positions
+     bxyzpsi  nb * 4 floats, boundary x, y, z and psi = rho0 * V_b
+     rho_out  nf floats, written in the order of xyz
+   domain_min/max (host, 3 floats each) bound the particles; particles outside
+   still get correct densities, only slower. Work is queued on `stream`
+   (a cudaStream_t; NULL = the legacy default stream) and the call returns
+   without waiting. Nothing is allocated: the neighbour-search scratch is a
+   fixed file-scope device array of about 9.5 MiB that every GPU loading this
+   library keeps until exit. Sizes above SPH_NOALLOC_MAX_FLUID,
+   SPH_NOALLOC_MAX_BOUNDARY or SPH_NOALLOC_MAX_CELLS (cells of edge 4r over
+   the domain, padded) return SPH_ERR_CAPACITY with the reason in
+   sph_noalloc_error(). All calls on a device share that array: calls whose
+   work overlaps on the GPU race and must be serialised by the caller. The
+   first call on each device looks up the array's address
+   (cudaGetSymbolAddress) with that device current; make it before any stream
+   capture on that device. */
+int sph_density_noalloc(float particle_radius, float density0, const float* xyz, unsigned nf,
+                        const float* bxyzpsi, unsigned nb, const float domain_min[3],
+                        const float domain_max[3], float* rho_out, void* stream);
+const char* sph_noalloc_error(void);
+
 /* ---- host scene loading (SceneLoader + object builders) --------------- */
 
 typedef struct sph_scene sph_scene;

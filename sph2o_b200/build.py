@@ -21,7 +21,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libsph2o_cuda.so")
 DRIVER = os.path.join(HERE, "bin", "sph2o")
 
-CUDA_SOURCES = ["csrc/sph_grid.cu", "csrc/sph_solvers.cu", "csrc/sph_capi.cu"]
+CUDA_SOURCES = ["csrc/sph_grid.cu", "csrc/sph_solvers.cu", "csrc/sph_capi.cu", "csrc/sph_noalloc.cu"]
 HOST_SOURCES = ["host/scene.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
