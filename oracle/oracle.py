@@ -1,0 +1,106 @@
+"""ctypes binding of the CPU oracle (oracle/sph_oracle.cpp). Test
+infrastructure: only tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg use it, as the checker."""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_ref", "libsph2o_oracle.so")
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise RuntimeError(f"{LIB} missing: run make -C oracle oracle")
+        L = C.CDLL(LIB)
+        P, D, F, U = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_float), C.POINTER(C.c_uint)
+        L.sph_oracle_create.restype = P
+        L.sph_oracle_create.argtypes = [C.c_void_p, C.c_int]
+        L.sph_oracle_set_fluid.argtypes = [P, C.c_uint, F, F]
+        L.sph_oracle_set_boundary.argtypes = [P, C.c_uint, F]
+        L.sph_oracle_init.argtypes = [P]
+        L.sph_oracle_step.argtypes = [P, C.c_int, D]
+        L.sph_oracle_get_state.argtypes = [P, D, D, D]
+        L.sph_oracle_get_boundary_volume.argtypes = [P, D]
+        L.sph_oracle_phase.argtypes = [P, C.c_int, D]
+        L.sph_oracle_neighbors.argtypes = [P, U, U, C.c_size_t, U, U, C.c_size_t, C.POINTER(C.c_size_t),
+                                           C.POINTER(C.c_size_t)]
+        L.sph_oracle_destroy.argtypes = [P]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _f(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _u(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint))
+
+
+class Oracle:
+    """CPU restatement of the reference; fp64=False reproduces its FP32 build."""
+
+    def __init__(self, desc, fluid, boundary, vel=None, fp64=False):
+        L = lib()
+        self.h = L.sph_oracle_create(C.addressof(desc), 1 if fp64 else 0)
+        x = np.ascontiguousarray(fluid, np.float32)
+        b = np.ascontiguousarray(boundary, np.float32)
+        v = None if vel is None else np.ascontiguousarray(vel, np.float32)
+        self.nf, self.nb = x.shape[0], b.shape[0]
+        L.sph_oracle_set_fluid(self.h, self.nf, _f(x), _f(v))
+        L.sph_oracle_set_boundary(self.h, self.nb, _f(b))
+        L.sph_oracle_init(self.h)
+
+    def step(self, n=1):
+        st = np.zeros((n, 6), np.float64)
+        lib().sph_oracle_step(self.h, n, _d(st))
+        return st
+
+    def state(self):
+        x = np.zeros((self.nf, 3))
+        v = np.zeros((self.nf, 3))
+        r = np.zeros(self.nf)
+        lib().sph_oracle_get_state(self.h, _d(x), _d(v), _d(r))
+        return x, v, r
+
+    def boundary_volume(self):
+        out = np.zeros(self.nb)
+        lib().sph_oracle_get_boundary_volume(self.h, _d(out))
+        return out
+
+    def phase(self, phase):
+        vec = phase in (2, 4)
+        out = np.zeros((self.nf, 3) if vec else self.nf)
+        lib().sph_oracle_phase(self.h, phase, _d(out))
+        return out
+
+    def neighbors(self):
+        L = lib()
+        tf, tb = C.c_size_t(), C.c_size_t()
+        L.sph_oracle_neighbors(self.h, None, None, 0, None, None, 0, C.byref(tf), C.byref(tb))
+        fo = np.zeros(self.nf + 1, np.uint32)
+        bo = np.zeros(self.nf + 1, np.uint32)
+        fi = np.zeros(max(1, tf.value), np.uint32)
+        bi = np.zeros(max(1, tb.value), np.uint32)
+        L.sph_oracle_neighbors(self.h, _u(fo), _u(fi), fi.size, _u(bo), _u(bi), bi.size, C.byref(tf), C.byref(tb))
+        return fo, fi[: tf.value], bo, bi[: tb.value]
+
+    def close(self):
+        if self.h:
+            lib().sph_oracle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,44 @@
+/*
+ * CPU restatement of SPH2O's per-step particle path -- TEST INFRASTRUCTURE.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
+ * load this library, and only as the checker. It mirrors the C ABI of
+ * include/sph2o_cuda.h (same scene description, same caller particle order)
+ * so the same scenario can run through both. Real is float (fp64 = 0) or
+ * double (fp64 = 1); the float variant reproduces the reference's FP32
+ * arithmetic operation by operation, the double variant its FP64 build.
+ * Parity pinned: tests/test_oracle.py checks it against the golden vectors
+ * generated by running the reference itself (tests/golden/).
+ */
+#ifndef SPH2O_ORACLE_H
+#define SPH2O_ORACLE_H
+
+#include <stddef.h>
+
+#include "../include/sph2o_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sph_oracle sph_oracle;
+
+sph_oracle* sph_oracle_create(const sph_scene_desc* desc, int fp64);
+int sph_oracle_set_fluid(sph_oracle* o, unsigned n, const float* xyz, const float* v);
+int sph_oracle_set_boundary(sph_oracle* o, unsigned n, const float* xyz);
+int sph_oracle_init(sph_oracle* o);
+/* stats: [time, dt, iterations, iterationsV, avg density residual, avg divergence residual] per step */
+int sph_oracle_step(sph_oracle* o, int nsteps, double* stats);
+int sph_oracle_get_state(sph_oracle* o, double* xyz, double* v, double* rho);
+int sph_oracle_get_boundary_volume(sph_oracle* o, double* vol);
+/* phases as in sph_phase: density, alpha, non-pressure acc, pressure, pressure acc */
+int sph_oracle_phase(sph_oracle* o, int phase, double* out);
+/* CSR neighbour sets (|xi - xj| <= h over the 27 cells), caller order */
+int sph_oracle_neighbors(sph_oracle* o, unsigned* f_off, unsigned* f_idx, size_t f_cap, unsigned* b_off,
+                         unsigned* b_idx, size_t b_cap, size_t* nf_total, size_t* nb_total);
+void sph_oracle_destroy(sph_oracle* o);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
