@@ -169,6 +169,10 @@ int sph_get_boundary_volume(sph_ctx* ctx, float* vol);
 /* Simulated time and current dt (TimeHelper::getTime/getTimeStep). */
 int sph_get_time(sph_ctx* ctx, double* time, float* dt);
 
+/* Set simulated time and the current dt (TimeHelper::setTime / setTimeStep,
+   inc/SPH2O/TimeHelper.h:51-54), e.g. when resuming from a frame file. */
+int sph_set_time(sph_ctx* ctx, double time, float dt);
+
 unsigned sph_num_fluid(const sph_ctx* ctx);
 unsigned sph_num_boundary(const sph_ctx* ctx);
 

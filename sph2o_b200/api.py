@@ -93,6 +93,7 @@ def lib():
         "sph_set_state": (I, [P, F, F]),
         "sph_get_boundary_volume": (I, [P, F]),
         "sph_get_time": (I, [P, C.POINTER(C.c_double), F]),
+        "sph_set_time": (I, [P, C.c_double, C.c_float]),
         "sph_num_fluid": (U, [P]),
         "sph_num_boundary": (U, [P]),
         "sph_last_error": (C.c_char_p, [P]),
@@ -252,6 +253,9 @@ class Simulation:
         dt = C.c_float()
         self._check(lib().sph_get_time(self._h, C.byref(t), C.byref(dt)))
         return t.value, dt.value
+
+    def set_time(self, time, dt):
+        self._check(lib().sph_set_time(self._h, float(time), float(dt)))
 
     def phase(self, phase):
         vec = phase in (PHASE_NONPRESSURE_ACC, PHASE_PRESSURE_ACC)

@@ -765,6 +765,23 @@ int sph_profile_read(sph_ctx* c, double* ms, unsigned long long* launches)
     return SPH_OK;
 }
 
+int sph_set_time(sph_ctx* c, double time, float dt)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_set_time before sph_init");
+    if (!(dt > 0.0f)) return fail(c, SPH_ERR_ARG, "dt must be positive");
+    DevState s{};
+    int rc = read_state(c, &s);
+    if (rc != SPH_OK) return rc;
+    s.time = time;
+    s.dt = dt;
+    CUDA_TRY(c, cudaMemcpyAsync(c->st, &s, sizeof s, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->last.time = time;
+    c->last.dt = dt;
+    return SPH_OK;
+}
+
 unsigned sph_num_fluid(const sph_ctx* c) { return c ? c->nf : 0u; }
 unsigned sph_num_boundary(const sph_ctx* c) { return c ? c->nb : 0u; }
 const char* sph_last_error(const sph_ctx* c) { return c ? c->err.c_str() : "null context"; }
