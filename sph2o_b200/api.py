@@ -18,7 +18,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libsph2o_cuda.so")
+LIB_PATH = os.environ.get("SPH2O_LIBRARY") or os.path.join(HERE, "libsph2o_cuda.so")
 
 SPH_OK = 0
 STATUS = {

@@ -169,6 +169,9 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, const float
     const int cy = cell_coord(xi.y, P.h, P.cminy, P.dimy);
     const int cz = cell_coord(xi.z, P.h, P.cminz, P.dimz);
     const size_t nf = (size_t)P.nf;
+    /* a cheap float test settles clear cases; candidates within a relative
+       1e-5 band of h take the exact IEEE test that defines the set */
+    const float lo2 = P.h2 * (1.0f - 1.0e-5f), hi2 = P.h2 * (1.0f + 1.0e-5f);
     unsigned nF = 0, nB = 0;
     for (int dx = -1; dx <= 1; ++dx) {
         const int x = cx + dx;
@@ -182,7 +185,10 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, const float
                 const unsigned c = brick_morton(x, y, z, P);
                 const unsigned s = cell_start[c], e = cell_start[c + 1];
                 for (unsigned q = s; q < e; ++q) {
-                    if (within_h_exact(xi, pos[q], P.h)) {
+                    const float4 xq = pos[q];
+                    const float dx = xi.x - xq.x, dy = xi.y - xq.y, dz = xi.z - xq.z;
+                    const float d2 = dx * dx + dy * dy + dz * dz;
+                    if (d2 < lo2 || (d2 <= hi2 && within_h_exact(xi, xq, P.h))) {
                         if (nF < P.capF) nbr_f[(size_t)nF * nf + i] = q;
                         ++nF;
                     }

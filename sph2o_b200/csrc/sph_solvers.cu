@@ -57,7 +57,7 @@ __device__ __forceinline__ Pair make_pair(float4 a, float4 b)
 /* ---------------------------------------------------------------------- */
 
 template <bool ALPHA, bool EOS>
-__global__ void __launch_bounds__(256) k_density(SimParams P, DeviceArrays A)
+__global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.nf) return;
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(256) k_density(SimParams P, DeviceArrays A)
     if (EOS) A.press[i] = tait_pressure(rho, P, P.kr_g);
 }
 
-__global__ void __launch_bounds__(256) k_normals(SimParams P, DeviceArrays A)
+__global__ void __launch_bounds__(256, 8) k_normals(SimParams P, DeviceArrays A)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.nf) return;
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(256) k_normals(SimParams P, DeviceArrays A)
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(128) k_forces(SimParams P, DeviceArrays A)
+__global__ void __launch_bounds__(128, 12) k_forces(SimParams P, DeviceArrays A)
 {
     __shared__ float s_red[32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -314,8 +314,10 @@ __device__ __forceinline__ void dfsph_correct(const SimParams& P, const DeviceAr
     A.vel[i] = v;
 }
 
+/* 8 blocks of 256 per SM (32 registers): the passes are bound by the latency
+   of dependent neighbour gathers, and full occupancy hides most of it */
 template <bool DIV>
-__global__ void __launch_bounds__(kSolverBlock, 4) k_dfsph_solve(SimParams P, DeviceArrays A)
+__global__ void __launch_bounds__(kSolverBlock, 8) k_dfsph_solve(SimParams P, DeviceArrays A)
 {
     __shared__ double s_red[32];
     DevState* st = A.st;
