@@ -72,6 +72,51 @@ def workloads():
     }
 
 
+def batched_run(steps, warmup, method=0, count=256, loop_steps=None):
+    """Batched scenes vs the plain per-scene GPU loop on the same scenes.
+    Returns particle-steps/s of both (device events for the batch, wall clock
+    for both in the ratio) and the scene statistics."""
+    import time as _t
+
+    import torch
+
+    from sph2o_b200 import scenes as S
+    from sph2o_b200.api import Batch, Scene, Simulation
+
+    dicts = S.batched_scenes(count, method=method)
+    scs = [Scene.from_dict(d) for d in dicts]
+    batch = Batch(scs)
+    total = batch.nf
+    batch.step(warmup)
+    torch.cuda.synchronize()
+    t0 = _t.perf_counter()
+    st = batch.step(steps)
+    wall_batch = _t.perf_counter() - t0
+    dev_ms = st["device_ms"]
+    batch.close()
+    loop_steps = loop_steps or max(1, min(steps, 10))
+    sims = [Simulation.from_scene(sc) for sc in scs]
+    for sim in sims:
+        sim.step(warmup)
+    torch.cuda.synchronize()
+    t0 = _t.perf_counter()
+    for sim in sims:
+        sim.step(loop_steps)
+    torch.cuda.synchronize()
+    wall_loop = _t.perf_counter() - t0
+    for sim in sims:
+        sim.close()
+    for sc in scs:
+        sc.close()
+    batched = total * steps / (dev_ms / 1e3)
+    batched_wall = total * steps / wall_batch
+    loop = total * loop_steps / wall_loop
+    return {"scenes": count, "fluid_particles": total, "steps": steps, "value": batched,
+            "value_wall": batched_wall, "per_scene_loop": loop, "speedup_vs_loop": batched_wall / loop,
+            "ms_per_step": dev_ms / steps, "mean_iterations": st["total_iterations"] / max(1, steps) / count,
+            "method": "WCSPH" if method == 0 else "DFSPH"}
+
+
 def hbm_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -219,6 +264,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="double_dam_break_dfsph_1m")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-only", action="store_true", help="time only the batched-scenes workload")
+    ap.add_argument("--batch-method", type=int, default=0)
+    ap.add_argument("--batch-scenes", type=int, default=256)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     name = args.workload
@@ -227,6 +275,12 @@ def main():
 
     if args.impl == "reference":
         return run_reference_arm(args, name, desc, scene_dict, world, rank)
+    if args.batch_only:
+        import torch
+        torch.cuda.set_device(local)
+        res = batched_run(args.steps, args.warmup, method=args.batch_method, count=args.batch_scenes)
+        print(json.dumps(res))
+        return 0
 
     import numpy as np
     import torch

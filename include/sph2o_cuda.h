@@ -183,6 +183,28 @@ const char* sph_global_error(void);
 
 int sph_destroy(sph_ctx* ctx);
 
+/* ---- batches of independent scenes --------------------------------------
+   No reference counterpart (SPH2O runs one scene per process). A batch
+   steps many independent scenes in one launch per phase: scenes keep their
+   own coordinates, cell grids, boundaries, time steps, viscosity and DFSPH
+   convergence (a converged scene stops iterating while others continue).
+   All scenes share the method (WCSPH or DFSPH), particle radius, rest
+   density, gravity, force methods and solver tolerances; viscosity,
+   boundary viscosity and the initial time step may differ per scene.
+   A batch is a context: sph_init, sph_step, sph_sync, sph_get_state
+   (all scenes concatenated in scene order), sph_profile_* and
+   sph_compute_phase apply to it; sph_set_fluid/sph_set_boundary do not. */
+
+int sph_batch_create(const sph_scene_desc* descs, unsigned nscenes, sph_ctx** out);
+/* Particles of one scene (before sph_init); v and bxyz may be NULL. */
+int sph_batch_set_scene(sph_ctx* ctx, unsigned scene, unsigned nf, const float* xyz, const float* v, unsigned nb,
+                        const float* bxyz);
+unsigned sph_batch_num_scenes(const sph_ctx* ctx);
+/* The scene's fluid particles occupy [begin, end) of the concatenated order. */
+int sph_batch_scene_range(const sph_ctx* ctx, unsigned scene, unsigned* begin, unsigned* end);
+/* Per-scene time, dt, iterations and residuals (cumulative iteration totals). */
+int sph_batch_scene_stats(sph_ctx* ctx, unsigned scene, sph_step_stats* out);
+
 /* ---- phase access for parity checks ------------------------------------- */
 
 enum sph_phase {

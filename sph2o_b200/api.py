@@ -105,6 +105,11 @@ def lib():
         "sph_debug_barrier_timeout": (I, [P]),
         "sph_profile_enable": (I, [P, I]),
         "sph_profile_read": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
+        "sph_batch_create": (I, [C.POINTER(SceneDesc), U, C.POINTER(P)]),
+        "sph_batch_set_scene": (I, [P, U, U, F, F, U, F]),
+        "sph_batch_num_scenes": (U, [P]),
+        "sph_batch_scene_range": (I, [P, U, C.POINTER(U), C.POINTER(U)]),
+        "sph_batch_scene_stats": (I, [P, U, C.POINTER(StepStats)]),
         "sph_scene_load": (I, [C.c_char_p, C.POINTER(P)]),
         "sph_scene_parse": (I, [C.c_char_p, C.POINTER(P)]),
         "sph_scene_get_desc": (I, [P, C.POINTER(SceneDesc)]),
@@ -295,3 +300,42 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+class Batch(Simulation):
+    """Many independent scenes stepped together (sph_batch_*)."""
+
+    def __init__(self, scenes, vels=None):
+        L = lib()
+        descs = (SceneDesc * len(scenes))(*[sc.desc() for sc in scenes])
+        h = C.c_void_p()
+        rc = L.sph_batch_create(descs, len(scenes), C.byref(h))
+        if rc != SPH_OK:
+            raise SphError(rc, L.sph_global_error().decode())
+        self._h = h
+        self.desc = descs[0]
+        self.nscenes = len(scenes)
+        for s, sc in enumerate(scenes):
+            x, v = sc.fluid()
+            if vels is not None and vels[s] is not None:
+                v = np.ascontiguousarray(vels[s], np.float32)
+            b = sc.boundary()
+            self._check(L.sph_batch_set_scene(h, s, x.shape[0], _fptr(x), _fptr(v), b.shape[0], _fptr(b)))
+        self._check(L.sph_init(h))
+        self.nf = L.sph_num_fluid(h)
+        self.nb = L.sph_num_boundary(h)
+        self.ranges = []
+        for s in range(self.nscenes):
+            b0, e0 = C.c_uint(), C.c_uint()
+            L.sph_batch_scene_range(h, s, C.byref(b0), C.byref(e0))
+            self.ranges.append((b0.value, e0.value))
+
+    def scene_stats(self, scene):
+        st = StepStats()
+        self._check(lib().sph_batch_scene_stats(self._h, int(scene), C.byref(st)))
+        return st.as_dict()
+
+    def scene_state(self, scene):
+        x, v, r = self.state()
+        b0, e0 = self.ranges[scene]
+        return x[b0:e0], v[b0:e0], r[b0:e0]

@@ -79,6 +79,18 @@ struct sph_ctx {
     std::vector<Pending> pending;
     double prof_ms[SPH_PROF_COUNT] = {};
     unsigned long long prof_launch[SPH_PROF_COUNT] = {};
+    /* batch of independent scenes (nscenes > 0) */
+    unsigned nscenes = 0;
+    std::vector<sph_scene_desc> descs;
+    std::vector<std::vector<float>> sc_fluid, sc_vel, sc_bound;
+    std::vector<unsigned> fsplit, bsplit;
+    std::vector<SceneInfo> h_scenes;
+    SceneInfo* d_scenes = nullptr;
+    unsigned *d_scene_of = nullptr, *d_bscene_of = nullptr, *d_any = nullptr;
+    SceneState* d_sst = nullptr;
+    unsigned accum_stride = 0;
+    int grid_batch_density = 0, grid_batch_div = 0;
+    std::vector<SceneState> last_sst;
 };
 
 namespace {
@@ -206,7 +218,7 @@ void derive_params(sph_ctx* c)
 
 DeviceArrays arrays(sph_ctx* c)
 {
-    DeviceArrays A;
+    DeviceArrays A{};
     A.pos = c->pos; A.vel = c->vel; A.pos_alt = c->pos2; A.vel_alt = c->vel2;
     A.acc = c->acc; A.normal = c->normal; A.predr = c->predr; A.pacc = c->pacc;
     A.rho = c->rho; A.alpha = c->alpha; A.k = c->k; A.kws = c->kws; A.kvws = c->kvws; A.press = c->press;
@@ -214,6 +226,14 @@ DeviceArrays arrays(sph_ctx* c)
     A.bpos = c->bpos; A.bcell_start = c->bcell_start;
     A.nbr_f = c->nbr_f; A.cnt_f = c->cnt_f; A.nbr_b = c->nbr_b; A.cnt_b = c->cnt_b;
     A.accum = c->accum; A.st = c->st;
+    if (c->nscenes) {
+        A.sref.scenes = c->d_scenes;
+        A.sref.scene_of = c->d_scene_of;
+        A.sst = c->d_sst;
+        A.any_active = c->d_any;
+        A.nscenes = (int)c->nscenes;
+        A.accum_stride = c->accum_stride;
+    }
     return A;
 }
 
@@ -294,7 +314,7 @@ int neighbor_search(sph_ctx* c)
     }
     {
         Phase ph(c, SPH_PROF_SORT, 6);
-        launch_sort(c->P, (int)c->nf, c->pos, c->cell_count, c->cell_start, c->block_sums, c->cell_of, c->slot,
+        launch_sort(c->P, SceneRef{c->d_scenes, c->d_scene_of}, (int)c->nf, c->pos, c->cell_count, c->cell_start, c->block_sums, c->cell_of, c->slot,
                     c->tmp_key, c->tmp_src, c->orig, g, c->stream);
     }
     std::swap(c->pos, c->pos2);
@@ -306,7 +326,7 @@ int neighbor_search(sph_ctx* c)
     }
     {
         Phase ph(c, SPH_PROF_LISTS, 1);
-        launch_build_lists(c->P, c->pos, c->cell_start, c->bpos, c->bcell_start, c->nbr_f, c->cnt_f, c->nbr_b,
+        launch_build_lists(c->P, SceneRef{c->d_scenes, c->d_scene_of}, c->pos, c->cell_start, c->bpos, c->bcell_start, c->nbr_f, c->cnt_f, c->nbr_b,
                            c->cnt_b, c->st, c->stream);
     }
     c->lists_valid = true;
@@ -316,6 +336,7 @@ int neighbor_search(sph_ctx* c)
 int zero_accum(sph_ctx* c)
 {
     CUDA_TRY(c, cudaMemsetAsync(c->accum, 0, c->accum_len * sizeof(double), c->stream));
+    if (c->d_any) CUDA_TRY(c, cudaMemsetAsync(c->d_any, 0, 2 * ((size_t)c->P.max_it + 2) * sizeof(unsigned), c->stream));
     return SPH_OK;
 }
 
@@ -357,13 +378,22 @@ int step_dfsph(sph_ctx* c)
     { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_NP_CFL, c->stream); }
     if ((rc = zero_accum(c)) != SPH_OK) return rc;
     int e;
-    { Phase ph(c, SPH_PROF_DENSITY_SOLVE, 1); e = launch_dfsph_solve(c->P, A, false, c->grid_density, c->stream); }
+    {
+        Phase ph(c, SPH_PROF_DENSITY_SOLVE, 1);
+        e = c->nscenes ? launch_dfsph_solve_batch(c->P, A, false, c->grid_batch_density, c->stream)
+                       : launch_dfsph_solve(c->P, A, false, c->grid_density, c->stream);
+    }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph density solver launch: ") + cudaGetErrorString((cudaError_t)e));
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     A = arrays(c);
     { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, true, false, c->stream); }
     A.accum = c->accum + c->accum_len / 2;
-    { Phase ph(c, SPH_PROF_DIVERGENCE_SOLVE, 1); e = launch_dfsph_solve(c->P, A, true, c->grid_div, c->stream); }
+    if (c->d_any) A.any_active = c->d_any + ((size_t)c->P.max_it + 2);
+    {
+        Phase ph(c, SPH_PROF_DIVERGENCE_SOLVE, 1);
+        e = c->nscenes ? launch_dfsph_solve_batch(c->P, A, true, c->grid_batch_div, c->stream)
+                       : launch_dfsph_solve(c->P, A, true, c->grid_div, c->stream);
+    }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph divergence solver launch: ") + cudaGetErrorString((cudaError_t)e));
     return check_launch(c, "dfsph step");
 }
@@ -469,6 +499,7 @@ int sph_create(const sph_scene_desc* desc, sph_ctx** out)
 int sph_set_fluid(sph_ctx* c, unsigned n, const float* xyz, const float* v)
 {
     if (!c) return SPH_ERR_ARG;
+    if (c->nscenes) return fail(c, SPH_ERR_STATE, "batch contexts take particles through sph_batch_set_scene");
     if (c->initialized) return fail(c, SPH_ERR_STATE, "sph_set_fluid after sph_init; use sph_set_state");
     if (n > 0 && !xyz) return fail(c, SPH_ERR_ARG, "null positions");
     c->nf = n;
@@ -481,6 +512,7 @@ int sph_set_fluid(sph_ctx* c, unsigned n, const float* xyz, const float* v)
 int sph_set_boundary(sph_ctx* c, unsigned n, const float* xyz)
 {
     if (!c) return SPH_ERR_ARG;
+    if (c->nscenes) return fail(c, SPH_ERR_STATE, "batch contexts take particles through sph_batch_set_scene");
     if (c->initialized) return fail(c, SPH_ERR_STATE, "sph_set_boundary after sph_init");
     if (n > 0 && !xyz) return fail(c, SPH_ERR_ARG, "null positions");
     c->nb = n;
@@ -492,12 +524,69 @@ int sph_init(sph_ctx* c)
 {
     if (!c) return SPH_ERR_ARG;
     if (c->initialized) return fail(c, SPH_ERR_STATE, "sph_init called twice");
-    if (c->nf == 0) return fail(c, SPH_ERR_ARG, "no fluid particles");
+    if (c->nf == 0 && c->nscenes == 0) return fail(c, SPH_ERR_ARG, "no fluid particles");
     CUDA_TRY(c, cudaSetDevice(c->device));
     SimParams& P = c->P;
+    if (c->nscenes) {
+        /* concatenate the scenes in scene order */
+        c->fsplit.assign(1, 0u);
+        c->bsplit.assign(1, 0u);
+        c->h_fluid.clear(); c->h_vel.clear(); c->h_bound.clear();
+        for (unsigned s = 0; s < c->nscenes; ++s) {
+            if (c->sc_fluid[s].empty()) return fail(c, SPH_ERR_ARG, "scene " + std::to_string(s) + " has no fluid");
+            c->h_fluid.insert(c->h_fluid.end(), c->sc_fluid[s].begin(), c->sc_fluid[s].end());
+            c->h_vel.insert(c->h_vel.end(), c->sc_vel[s].begin(), c->sc_vel[s].end());
+            c->h_bound.insert(c->h_bound.end(), c->sc_bound[s].begin(), c->sc_bound[s].end());
+            c->fsplit.push_back((unsigned)(c->h_fluid.size() / 3));
+            c->bsplit.push_back((unsigned)(c->h_bound.size() / 3));
+        }
+        c->nf = c->fsplit.back();
+        c->nb = c->bsplit.back();
+    }
     P.nf = (int)c->nf;
     P.nb = (int)c->nb;
 
+    if (c->nscenes) {
+        /* one grid per scene, each owning a disjoint range of the cell table */
+        unsigned long long base = 0;
+        c->h_scenes.resize(c->nscenes);
+        for (unsigned s = 0; s < c->nscenes; ++s) {
+            double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+            for (const std::vector<float>* a : {&c->sc_fluid[s], &c->sc_bound[s]})
+                for (size_t i = 0; i + 2 < a->size(); i += 3)
+                    for (int k = 0; k < 3; ++k) {
+                        const float v = (*a)[i + k];
+                        if (!std::isfinite(v)) continue;
+                        lo[k] = std::min(lo[k], (double)v);
+                        hi[k] = std::max(hi[k], (double)v);
+                    }
+            SceneInfo& si = c->h_scenes[s];
+            int dim[3], cmin[3];
+            for (int k = 0; k < 3; ++k) {
+                cmin[k] = (int)std::floor(lo[k] / P.h) - 2;
+                const int b = (int)std::floor(hi[k] / P.h) + 2;
+                dim[k] = ((b - cmin[k] + 1) + 3) / 4 * 4;
+            }
+            si.grid.cminx = cmin[0]; si.grid.cminy = cmin[1]; si.grid.cminz = cmin[2];
+            si.grid.dimx = dim[0]; si.grid.dimy = dim[1]; si.grid.dimz = dim[2];
+            si.grid.nbx = dim[0] / 4; si.grid.nby = dim[1] / 4;
+            si.grid.base = (unsigned)base;
+            base += (unsigned long long)dim[0] * dim[1] * dim[2];
+            if (base > (1ull << 28)) return fail(c, SPH_ERR_CAPACITY, "batch too large: more than 2^28 grid cells");
+            const sph_scene_desc& ds = c->descs[s];
+            si.visc = ds.viscosity;
+            si.bvisc = ds.boundary_viscosity;
+            si.fbegin = c->fsplit[s]; si.fend = c->fsplit[s + 1];
+            si.bbegin = c->bsplit[s]; si.bend = c->bsplit[s + 1];
+        }
+        const SceneInfo& s0 = c->h_scenes[0];
+        P.cminx = s0.grid.cminx; P.cminy = s0.grid.cminy; P.cminz = s0.grid.cminz;
+        P.dimx = s0.grid.dimx; P.dimy = s0.grid.dimy; P.dimz = s0.grid.dimz;
+        P.nbx = s0.grid.nbx; P.nby = s0.grid.nby;
+        P.ncells = (unsigned)((base + 4095) / 4096 * 4096);
+        P.capF = 64;
+        P.capB = 64;
+    } else {
     /* grid over the particle bounding box (+ hint), 2 cells of margin */
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     auto grow = [&](const std::vector<float>& a) {
@@ -533,6 +622,7 @@ int sph_init(sph_ctx* c)
     P.ncells = (unsigned)((ncells + 4095) / 4096 * 4096);
     P.capF = 64;
     P.capB = 64;
+    }
 
     const size_t nf = c->nf, nb = c->nb, nmax = std::max(nf, nb);
     int rc = SPH_OK;
@@ -550,8 +640,34 @@ int sph_init(sph_ctx* c)
     ALLOC(st, 1);
 #undef ALLOC
     if ((rc = alloc_lists(c)) != SPH_OK) return rc;
-    c->accum_len = 2 * ((size_t)P.max_it + 2);
+    c->accum_len = 2 * ((size_t)P.max_it + 2) * std::max(1u, c->nscenes);
     if ((rc = dalloc(c, &c->accum, c->accum_len)) != SPH_OK) return rc;
+    if (c->nscenes) {
+        const unsigned ns = c->nscenes;
+        c->accum_stride = P.max_it + 2;
+        if ((rc = dalloc(c, &c->d_scenes, ns)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->d_sst, ns)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->d_scene_of, nf)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->d_bscene_of, std::max<size_t>(nb, 1))) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->d_any, 2 * ((size_t)P.max_it + 2))) != SPH_OK) return rc;
+        std::vector<unsigned> so(nf), bso(nb);
+        std::vector<SceneState> sst(ns);
+        for (unsigned s = 0; s < ns; ++s) {
+            for (unsigned i = c->fsplit[s]; i < c->fsplit[s + 1]; ++i) so[i] = s;
+            for (unsigned i = c->bsplit[s]; i < c->bsplit[s + 1]; ++i) bso[i] = s;
+            sst[s] = SceneState{};
+            sst[s].dt = c->descs[s].time_step;
+        }
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_scenes, c->h_scenes.data(), ns * sizeof(SceneInfo), cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_sst, sst.data(), ns * sizeof(SceneState), cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_scene_of, so.data(), nf * 4, cudaMemcpyHostToDevice, c->stream));
+        if (nb) CUDA_TRY(c, cudaMemcpyAsync(c->d_bscene_of, bso.data(), nb * 4, cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        c->grid_batch_density = persistent_grid(false, false, true);
+        c->grid_batch_div = persistent_grid(false, true, true);
+        if (c->grid_batch_density <= 0 || c->grid_batch_div <= 0)
+            return fail(c, SPH_ERR_CUDA, "cannot size the persistent batch solver grid");
+    }
     CUDA_TRY(c, cudaMallocHost((void**)&c->st_host, sizeof(DevState)));
     CUDA_TRY(c, cudaEventCreate(&c->ev_begin));
     CUDA_TRY(c, cudaEventCreate(&c->ev_end));
@@ -586,19 +702,20 @@ int sph_init(sph_ctx* c)
         g.orig_out = c->borig;
         g.v4_in[0] = braw;
         g.v4_out[0] = c->bpos;
-        launch_sort(P, (int)nb, braw, c->cell_count, c->bcell_start, c->block_sums, c->cell_of, c->slot, c->tmp_key,
-                    c->tmp_src, bid, g, c->stream);
-        launch_boundary_volume(P, c->bpos, c->bcell_start, c->bvol, c->stream);
+        const SceneRef bref{c->d_scenes, c->d_bscene_of};
+        launch_sort(P, bref, (int)nb, braw, c->cell_count, c->bcell_start, c->block_sums, c->cell_of, c->slot,
+                    c->tmp_key, c->tmp_src, bid, g, c->stream);
+        launch_boundary_volume(P, bref, c->bpos, c->bcell_start, c->bvol, c->stream);
     } else {
         CUDA_TRY(c, cudaMemsetAsync(c->bcell_start, 0, ((size_t)P.ncells + 1) * sizeof(unsigned), c->stream));
     }
 
     /* solver state */
     DevState s0{};
-    s0.dt = d.time_step;
+    s0.dt = c->desc.time_step;
     CUDA_TRY(c, cudaMemcpyAsync(c->st, &s0, sizeof s0, cudaMemcpyHostToDevice, c->stream));
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
-    if (d.simulation_method == SPH_DFSPH) {
+    if (c->desc.simulation_method == SPH_DFSPH) {
         /* DFSPHSolver::init: densities and alpha at the initial positions */
         launch_density(P, arrays(c), true, false, c->stream);
     }
@@ -642,6 +759,39 @@ int sph_sync(sph_ctx* c, sph_step_stats* out)
     int rc = read_state(c, &now);
     if (rc != SPH_OK) return rc;
     fill_stats(c, c->last, now, out);
+    if (c->nscenes) {
+        /* batch: time/dt of the slowest scene, iterations summed over scenes */
+        std::vector<SceneState> sst(c->nscenes);
+        CUDA_TRY(c, cudaMemcpy(sst.data(), c->d_sst, c->nscenes * sizeof(SceneState), cudaMemcpyDeviceToHost));
+        if (out) {
+            if (c->last_sst.size() != sst.size()) c->last_sst.assign(sst.size(), SceneState{});
+            double tmin = 1e300;
+            float dtmin = 3e38f;
+            unsigned long long its = 0, itsv = 0;
+            unsigned mx = 0, mxv = 0;
+            double avg = 0.0, avgv = 0.0;
+            for (unsigned s = 0; s < c->nscenes; ++s) {
+                tmin = std::min(tmin, sst[s].time);
+                dtmin = std::min(dtmin, sst[s].dt);
+                its += sst[s].sum_its - c->last_sst[s].sum_its;
+                itsv += sst[s].sum_its_v - c->last_sst[s].sum_its_v;
+                mx = std::max(mx, sst[s].its);
+                mxv = std::max(mxv, sst[s].its_v);
+                avg = std::max(avg, sst[s].avg_dens);
+                avgv = std::max(avgv, sst[s].avg_div);
+            }
+            out->time = tmin;
+            out->dt = dtmin;
+            out->iterations = mx;
+            out->iterations_v = mxv;
+            out->total_iterations = its;
+            out->total_iterations_v = itsv;
+            out->avg_density_error = avg;
+            out->avg_divergence_error = avgv;
+            out->steps = sst[0].steps - c->last_sst[0].steps;
+        }
+        c->last_sst = sst;
+    }
     if (c->batch_open) {
         float ms = 0.0f;
         if (out && cudaEventElapsedTime(&ms, c->ev_begin, c->ev_end) == cudaSuccess) out->device_ms = ms;
@@ -839,6 +989,94 @@ int sph_compute_phase(sph_ctx* c, int phase, float* out)
     cudaFreeAsync(tmp, c->stream);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return check_launch(c, "compute_phase");
+}
+
+int sph_batch_create(const sph_scene_desc* descs, unsigned nscenes, sph_ctx** out)
+{
+    if (!descs || !out || nscenes == 0) return fail(nullptr, SPH_ERR_ARG, "descs, nscenes > 0 and out are required");
+    const sph_scene_desc& d0 = descs[0];
+    if (d0.simulation_method != SPH_WCSPH && d0.simulation_method != SPH_DFSPH)
+        return fail(nullptr, SPH_ERR_ARG, "batches run WCSPH or DFSPH scenes");
+    for (unsigned s = 1; s < nscenes; ++s) {
+        const sph_scene_desc& d = descs[s];
+        const bool same = d.simulation_method == d0.simulation_method && d.boundary_method == d0.boundary_method &&
+                          d.viscosity_method == d0.viscosity_method &&
+                          d.surface_tension_method == d0.surface_tension_method &&
+                          d.adhesion_method == d0.adhesion_method && d.particle_radius == d0.particle_radius &&
+                          d.density0 == d0.density0 && d.gravity[0] == d0.gravity[0] &&
+                          d.gravity[1] == d0.gravity[1] && d.gravity[2] == d0.gravity[2] &&
+                          d.stiffness == d0.stiffness && d.gamma == d0.gamma && d.eta == d0.eta &&
+                          d.eta_v == d0.eta_v && d.cfl_factor == d0.cfl_factor &&
+                          d.min_iterations == d0.min_iterations && d.max_iterations == d0.max_iterations &&
+                          d.min_iterations_v == d0.min_iterations_v && d.max_iterations_v == d0.max_iterations_v &&
+                          d.surface_tension == d0.surface_tension && d.adhesion == d0.adhesion &&
+                          d.min_time_step == d0.min_time_step && d.max_time_step == d0.max_time_step &&
+                          d.fps == d0.fps;
+        if (!same)
+            return fail(nullptr, SPH_ERR_ARG, "scene " + std::to_string(s) + " differs from scene 0 in a shared "
+                                              "parameter (only viscosity, boundary viscosity and time step may differ)");
+    }
+    sph_scene_desc shared = d0;
+    /* the viscosity force exists for the batch if its method is set; scenes
+       with a zero coefficient add exact zeros */
+    int rc = sph_create(&shared, out);
+    if (rc != SPH_OK) return rc;
+    sph_ctx* c = *out;
+    if (c->P.visc_method < 0 && d0.viscosity_method > -1 && d0.viscosity_method <= 2)
+        c->P.visc_method = d0.viscosity_method;
+    c->nscenes = nscenes;
+    c->descs.assign(descs, descs + nscenes);
+    c->sc_fluid.resize(nscenes);
+    c->sc_vel.resize(nscenes);
+    c->sc_bound.resize(nscenes);
+    return SPH_OK;
+}
+
+int sph_batch_set_scene(sph_ctx* c, unsigned scene, unsigned nf, const float* xyz, const float* v, unsigned nb,
+                        const float* bxyz)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->nscenes) return fail(c, SPH_ERR_STATE, "not a batch context");
+    if (c->initialized) return fail(c, SPH_ERR_STATE, "sph_batch_set_scene after sph_init");
+    if (scene >= c->nscenes) return fail(c, SPH_ERR_ARG, "scene index out of range");
+    if ((nf && !xyz) || (nb && !bxyz)) return fail(c, SPH_ERR_ARG, "null positions");
+    c->sc_fluid[scene].assign(xyz, xyz + 3ull * nf);
+    if (v) c->sc_vel[scene].assign(v, v + 3ull * nf);
+    else c->sc_vel[scene].assign(3ull * nf, 0.0f);
+    c->sc_bound[scene].assign(bxyz, bxyz + 3ull * nb);
+    return SPH_OK;
+}
+
+unsigned sph_batch_num_scenes(const sph_ctx* c) { return c ? c->nscenes : 0u; }
+
+int sph_batch_scene_range(const sph_ctx* c, unsigned scene, unsigned* begin, unsigned* end)
+{
+    if (!c || !c->nscenes || scene >= c->nscenes || !c->initialized) return SPH_ERR_ARG;
+    if (begin) *begin = c->fsplit[scene];
+    if (end) *end = c->fsplit[scene + 1];
+    return SPH_OK;
+}
+
+int sph_batch_scene_stats(sph_ctx* c, unsigned scene, sph_step_stats* out)
+{
+    if (!c || !out) return SPH_ERR_ARG;
+    if (!c->nscenes || !c->initialized) return fail(c, SPH_ERR_STATE, "not an initialised batch");
+    if (scene >= c->nscenes) return fail(c, SPH_ERR_ARG, "scene index out of range");
+    SceneState s{};
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    CUDA_TRY(c, cudaMemcpy(&s, c->d_sst + scene, sizeof s, cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof *out);
+    out->time = s.time;
+    out->dt = s.dt;
+    out->iterations = s.its;
+    out->iterations_v = s.its_v;
+    out->total_iterations = s.sum_its;
+    out->total_iterations_v = s.sum_its_v;
+    out->avg_density_error = s.avg_dens;
+    out->avg_divergence_error = s.avg_div;
+    out->max_velocity = s.last_vmax;
+    out->steps = s.steps;
+    return SPH_OK;
 }
 
 int sph_debug_barrier_timeout(sph_ctx* c)

@@ -226,20 +226,91 @@ __device__ __forceinline__ int cell_coord(float x, float h, int cmin, int dim)
     return min(max(c, 0), dim - 1);
 }
 
-__device__ __forceinline__ unsigned brick_morton(int cx, int cy, int cz, const SimParams& P)
+/* One scene's cell grid: origin key, extent (x, y, z multiples of 4) and
+   the offset of its cells in the global cell table (0 for a single scene;
+   batched scenes own disjoint ranges of one table). */
+struct Grid {
+    int cminx, cminy, cminz;
+    int dimx, dimy, dimz;
+    int nbx, nby;
+    unsigned base;
+};
+
+/* Per-scene constants of a batch. Slots [fbegin, fend) of the sorted fluid
+   arrays and [bbegin, bend) of the boundary arrays belong to the scene; the
+   sort is scene-major, so these ranges never change. */
+struct SceneInfo {
+    Grid grid;
+    float visc, bvisc;
+    unsigned fbegin, fend, bbegin, bend;
+};
+
+/* Per-scene solver state of a batch (the per-scene part of DevState). */
+struct SceneState {
+    double time, avg_dens, avg_div;
+    float dt, dt_next, last_vmax;
+    unsigned vmax_bits, its, its_v, steps, active;
+    unsigned long long sum_its, sum_its_v;
+};
+
+__device__ __forceinline__ Grid grid_single(const SimParams& P)
+{
+    Grid g;
+    g.cminx = P.cminx; g.cminy = P.cminy; g.cminz = P.cminz;
+    g.dimx = P.dimx; g.dimy = P.dimy; g.dimz = P.dimz;
+    g.nbx = P.nbx; g.nby = P.nby;
+    g.base = 0u;
+    return g;
+}
+
+__device__ __forceinline__ unsigned brick_morton(int cx, int cy, int cz, const Grid& g)
 {
     const unsigned lx = (unsigned)cx & 3u, ly = (unsigned)cy & 3u, lz = (unsigned)cz & 3u;
     const unsigned m = (lx & 1u) | ((ly & 1u) << 1) | ((lz & 1u) << 2) | ((lx & 2u) << 2) |
                        ((ly & 2u) << 3) | ((lz & 2u) << 4);
-    const unsigned b = ((unsigned)(cz >> 2) * (unsigned)P.nby + (unsigned)(cy >> 2)) * (unsigned)P.nbx +
+    const unsigned b = ((unsigned)(cz >> 2) * (unsigned)g.nby + (unsigned)(cy >> 2)) * (unsigned)g.nbx +
                        (unsigned)(cx >> 2);
-    return (b << 6) | m;
+    return g.base + ((b << 6) | m);
 }
 
-__device__ __forceinline__ unsigned cell_index(float4 x, const SimParams& P)
+__device__ __forceinline__ unsigned cell_index(float4 x, float h, const Grid& g)
 {
-    return brick_morton(cell_coord(x.x, P.h, P.cminx, P.dimx), cell_coord(x.y, P.h, P.cminy, P.dimy),
-                        cell_coord(x.z, P.h, P.cminz, P.dimz), P);
+    return brick_morton(cell_coord(x.x, h, g.cminx, g.dimx), cell_coord(x.y, h, g.cminy, g.dimy),
+                        cell_coord(x.z, h, g.cminz, g.dimz), g);
+}
+
+/* Calls f(c) for the existing cells among the 27 around x's cell, in the
+   reference's offset order (x outermost, z innermost; HashTable.cpp:59-65). */
+template <typename F>
+__device__ __forceinline__ void for_cells27(float4 x, float h, const Grid& g, F&& f)
+{
+    const int cx = cell_coord(x.x, h, g.cminx, g.dimx);
+    const int cy = cell_coord(x.y, h, g.cminy, g.dimy);
+    const int cz = cell_coord(x.z, h, g.cminz, g.dimz);
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int xx = cx + dx;
+        if (xx < 0 || xx >= g.dimx) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int yy = cy + dy;
+            if (yy < 0 || yy >= g.dimy) continue;
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int zz = cz + dz;
+                if (zz < 0 || zz >= g.dimz) continue;
+                f(brick_morton(xx, yy, zz, g));
+            }
+        }
+    }
+}
+
+/* Scene table of a batch (both NULL for a single scene). */
+struct SceneRef {
+    const SceneInfo* scenes;
+    const unsigned* scene_of;   /* scene of each sorted slot */
+};
+
+__device__ __forceinline__ Grid grid_for(const SimParams& P, const SceneRef& S, unsigned slot)
+{
+    return S.scenes ? S.scenes[S.scene_of[slot]].grid : grid_single(P);
 }
 
 /* exact |xi - xj| <= h test of the reference (glm::length: sqrt((dx dx + dy dy) + dz dz)) */

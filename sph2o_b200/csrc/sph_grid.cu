@@ -25,13 +25,13 @@
 
 namespace sph {
 
-__global__ void __launch_bounds__(256) k_ns_count(SimParams P, int n, const float4* __restrict__ pos,
+__global__ void __launch_bounds__(256) k_ns_count(SimParams P, SceneRef S, int n, const float4* __restrict__ pos,
                                                   unsigned* __restrict__ cell_count, unsigned* __restrict__ cell_of,
                                                   unsigned* __restrict__ slot)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const unsigned c = cell_index(pos[i], P);
+    const unsigned c = cell_index(pos[i], P.h, grid_for(P, S, (unsigned)i));
     cell_of[i] = c;
     slot[i] = atomicAdd(&cell_count[c], 1u);
 }
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(256) k_ns_rank_gather(int n, const unsigned* _
 }
 
 /* Neighbour lists in the reference's candidate order, filtered at |r| <= h. */
-__global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, const float4* __restrict__ pos,
+__global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S, const float4* __restrict__ pos,
                                                         const unsigned* __restrict__ cell_start,
                                                         const float4* __restrict__ bpos,
                                                         const unsigned* __restrict__ bcell_start,
@@ -165,46 +165,32 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, const float
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.nf) return;
     const float4 xi = pos[i];
-    const int cx = cell_coord(xi.x, P.h, P.cminx, P.dimx);
-    const int cy = cell_coord(xi.y, P.h, P.cminy, P.dimy);
-    const int cz = cell_coord(xi.z, P.h, P.cminz, P.dimz);
     const size_t nf = (size_t)P.nf;
     /* a cheap float test settles clear cases; candidates within a relative
        1e-5 band of h take the exact IEEE test that defines the set */
     const float lo2 = P.h2 * (1.0f - 1.0e-5f), hi2 = P.h2 * (1.0f + 1.0e-5f);
     unsigned nF = 0, nB = 0;
-    for (int dx = -1; dx <= 1; ++dx) {
-        const int x = cx + dx;
-        if (x < 0 || x >= P.dimx) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int y = cy + dy;
-            if (y < 0 || y >= P.dimy) continue;
-            for (int dz = -1; dz <= 1; ++dz) {
-                const int z = cz + dz;
-                if (z < 0 || z >= P.dimz) continue;
-                const unsigned c = brick_morton(x, y, z, P);
-                const unsigned s = cell_start[c], e = cell_start[c + 1];
-                for (unsigned q = s; q < e; ++q) {
-                    const float4 xq = pos[q];
-                    const float dx = xi.x - xq.x, dy = xi.y - xq.y, dz = xi.z - xq.z;
-                    const float d2 = dx * dx + dy * dy + dz * dz;
-                    if (d2 < lo2 || (d2 <= hi2 && within_h_exact(xi, xq, P.h))) {
-                        if (nF < P.capF) nbr_f[(size_t)nF * nf + i] = q;
-                        ++nF;
-                    }
-                }
-                if (P.nb > 0) {
-                    const unsigned bs = bcell_start[c], be = bcell_start[c + 1];
-                    for (unsigned q = bs; q < be; ++q) {
-                        if (within_h_exact(xi, bpos[q], P.h)) {
-                            if (nB < P.capB) nbr_b[(size_t)nB * nf + i] = q;
-                            ++nB;
-                        }
-                    }
+    for_cells27(xi, P.h, grid_for(P, S, (unsigned)i), [&](unsigned c) {
+        const unsigned s = cell_start[c], e = cell_start[c + 1];
+        for (unsigned q = s; q < e; ++q) {
+            const float4 xq = pos[q];
+            const float dx = xi.x - xq.x, dy = xi.y - xq.y, dz = xi.z - xq.z;
+            const float d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 < lo2 || (d2 <= hi2 && within_h_exact(xi, xq, P.h))) {
+                if (nF < P.capF) nbr_f[(size_t)nF * nf + i] = q;
+                ++nF;
+            }
+        }
+        if (P.nb > 0) {
+            const unsigned bs = bcell_start[c], be = bcell_start[c + 1];
+            for (unsigned q = bs; q < be; ++q) {
+                if (within_h_exact(xi, bpos[q], P.h)) {
+                    if (nB < P.capB) nbr_b[(size_t)nB * nf + i] = q;
+                    ++nB;
                 }
             }
         }
-    }
+    });
     cnt_f[i] = min(nF, P.capF);
     cnt_b[i] = min(nB, P.capB);
     if (nF > P.capF || nB > P.capB) {
@@ -216,34 +202,20 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, const float
 /* Akinci boundary volume V_b = 1 / sum_b' W(x_b - x_b') over the 27 cells
    (AkinciBoundaryObject.cpp:10-34); k_boundary_psi then stores
    psi = rho0 V_b in bpos.w for the fluid kernels. */
-__global__ void __launch_bounds__(128) k_boundary_volume(SimParams P, const float4* __restrict__ bpos,
+__global__ void __launch_bounds__(128) k_boundary_volume(SimParams P, SceneRef S, const float4* __restrict__ bpos,
                                                          const unsigned* __restrict__ bcell_start,
                                                          float* __restrict__ bvol)
 {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= P.nb) return;
     const float4 xb = bpos[b];
-    const int cx = cell_coord(xb.x, P.h, P.cminx, P.dimx);
-    const int cy = cell_coord(xb.y, P.h, P.cminy, P.dimy);
-    const int cz = cell_coord(xb.z, P.h, P.cminz, P.dimz);
     float delta = 0.0f;
-    for (int dx = -1; dx <= 1; ++dx) {
-        const int x = cx + dx;
-        if (x < 0 || x >= P.dimx) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int y = cy + dy;
-            if (y < 0 || y >= P.dimy) continue;
-            for (int dz = -1; dz <= 1; ++dz) {
-                const int z = cz + dz;
-                if (z < 0 || z >= P.dimz) continue;
-                const unsigned c = brick_morton(x, y, z, P);
-                for (unsigned q = bcell_start[c]; q < bcell_start[c + 1]; ++q) {
-                    const float s2 = dist2_exact(xb, bpos[q]);
-                    if (s2 <= P.h2_guard) delta = __fadd_rn(delta, cs_W_exact(s2, P));
-                }
-            }
+    for_cells27(xb, P.h, grid_for(P, S, (unsigned)b), [&](unsigned c) {
+        for (unsigned q = bcell_start[c]; q < bcell_start[c + 1]; ++q) {
+            const float s2 = dist2_exact(xb, bpos[q]);
+            if (s2 <= P.h2_guard) delta = __fadd_rn(delta, cs_W_exact(s2, P));
         }
-    }
+    });
     bvol[b] = __fdiv_rn(1.0f, delta);
 }
 
@@ -300,7 +272,8 @@ __global__ void k_iota(int n, unsigned* __restrict__ out)
 
 static inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
-void launch_sort(const SimParams& P, int n, const float4* pos_for_keys, unsigned* cell_count, unsigned* cell_start,
+void launch_sort(const SimParams& P, const SceneRef& S, int n, const float4* pos_for_keys, unsigned* cell_count,
+                 unsigned* cell_start,
                  unsigned* block_sums, unsigned* cell_of, unsigned* slot, unsigned* tmp_key, unsigned* tmp_src,
                  const unsigned* orig_in, const GatherSet& g, cudaStream_t s)
 {
@@ -309,7 +282,7 @@ void launch_sort(const SimParams& P, int n, const float4* pos_for_keys, unsigned
         cudaMemsetAsync(cell_start, 0, ((size_t)P.ncells + 1) * sizeof(unsigned), s);
         return;
     }
-    k_ns_count<<<blocks_for(n, 256), 256, 0, s>>>(P, n, pos_for_keys, cell_count, cell_of, slot);
+    k_ns_count<<<blocks_for(n, 256), 256, 0, s>>>(P, S, n, pos_for_keys, cell_count, cell_of, slot);
     const int nblk = (int)(P.ncells / 4096);
     k_scan_local<<<nblk, 1024, 0, s>>>(cell_count, cell_start, block_sums);
     k_scan_blocks<<<1, 1024, 0, s>>>(block_sums, nblk, cell_start + P.ncells);
@@ -318,20 +291,21 @@ void launch_sort(const SimParams& P, int n, const float4* pos_for_keys, unsigned
     k_ns_rank_gather<<<blocks_for(n, 256), 256, 0, s>>>(n, cell_of, cell_start, tmp_key, tmp_src, g);
 }
 
-void launch_build_lists(const SimParams& P, const float4* pos, const unsigned* cell_start, const float4* bpos,
+void launch_build_lists(const SimParams& P, const SceneRef& S, const float4* pos, const unsigned* cell_start,
+                        const float4* bpos,
                         const unsigned* bcell_start, unsigned* nbr_f, unsigned* cnt_f, unsigned* nbr_b,
                         unsigned* cnt_b, DevState* st, cudaStream_t s)
 {
     if (P.nf <= 0) return;
-    k_ns_build_lists<<<blocks_for(P.nf, 128), 128, 0, s>>>(P, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f,
+    k_ns_build_lists<<<blocks_for(P.nf, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f,
                                                             nbr_b, cnt_b, st);
 }
 
-void launch_boundary_volume(const SimParams& P, float4* bpos, const unsigned* bcell_start, float* bvol,
-                            cudaStream_t s)
+void launch_boundary_volume(const SimParams& P, const SceneRef& S, float4* bpos, const unsigned* bcell_start,
+                            float* bvol, cudaStream_t s)
 {
     if (P.nb <= 0) return;
-    k_boundary_volume<<<blocks_for(P.nb, 128), 128, 0, s>>>(P, bpos, bcell_start, bvol);
+    k_boundary_volume<<<blocks_for(P.nb, 128), 128, 0, s>>>(P, S, bpos, bcell_start, bvol);
     k_boundary_psi<<<blocks_for(P.nb, 256), 256, 0, s>>>(P, bpos, bvol);
 }
 

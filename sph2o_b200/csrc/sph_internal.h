@@ -48,17 +48,24 @@ struct DeviceArrays {
     const unsigned* cnt_b;
     double* accum;        /* per-iteration residual accumulators, zeroed per solve */
     DevState* st;
+    SceneRef sref;        /* batch scene table (empty for a single scene) */
+    SceneState* sst;      /* per-scene state of a batch (NULL for a single scene) */
+    unsigned* any_active; /* batch: per-iteration "some scene still iterates" flags */
+    int nscenes;
+    unsigned accum_stride;/* batch: doubles per scene in accum */
 };
 
 /* sph_grid.cu */
-void launch_sort(const SimParams& P, int n, const float4* pos_for_keys, unsigned* cell_count, unsigned* cell_start,
+void launch_sort(const SimParams& P, const SceneRef& S, int n, const float4* pos_for_keys, unsigned* cell_count,
+                 unsigned* cell_start,
                  unsigned* block_sums, unsigned* cell_of, unsigned* slot, unsigned* tmp_key, unsigned* tmp_src,
                  const unsigned* orig_in, const GatherSet& g, cudaStream_t s);
-void launch_build_lists(const SimParams& P, const float4* pos, const unsigned* cell_start, const float4* bpos,
+void launch_build_lists(const SimParams& P, const SceneRef& S, const float4* pos, const unsigned* cell_start,
+                        const float4* bpos,
                         const unsigned* bcell_start, unsigned* nbr_f, unsigned* cnt_f, unsigned* nbr_b,
                         unsigned* cnt_b, DevState* st, cudaStream_t s);
-void launch_boundary_volume(const SimParams& P, float4* bpos, const unsigned* bcell_start, float* bvol,
-                            cudaStream_t s);
+void launch_boundary_volume(const SimParams& P, const SceneRef& S, float4* bpos, const unsigned* bcell_start,
+                            float* bvol, cudaStream_t s);
 void launch_unsort_v4(int n, const unsigned* orig, const float4* in, float* out3, cudaStream_t s);
 void launch_unsort_f(int n, const unsigned* orig, const float* in, float* out, cudaStream_t s);
 void launch_sort_v3(int n, const unsigned* orig, const float* in3, float4* out, cudaStream_t s);
@@ -78,9 +85,10 @@ void launch_normals(const SimParams& P, const DeviceArrays& A, cudaStream_t s);
 void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, cudaStream_t s);
 int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s);
 int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s);
+int launch_dfsph_solve_batch(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s);
 int launch_barrier_timeout_probe(DevState* st, cudaStream_t s);
 /* co-resident grid size of the persistent solver kernels (0 on error) */
-int persistent_grid(bool pcisph, bool divergence);
+int persistent_grid(bool pcisph, bool divergence, bool batch = false);
 constexpr int kSolverBlock = 256;
 
 } // namespace sph

@@ -105,38 +105,22 @@ __global__ void __launch_bounds__(128) k_na_density(SimParams P, const float4* _
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.nf) return;
     const float4 xi = pos[i];
-    const int cx = cell_coord(xi.x, P.h, P.cminx, P.dimx);
-    const int cy = cell_coord(xi.y, P.h, P.cminy, P.dimy);
-    const int cz = cell_coord(xi.z, P.h, P.cminz, P.dimz);
+    const Grid g = grid_single(P);
     float rho = 0.0f;
-    for (int pass = 0; pass < 2; ++pass) {
-        if (pass == 1 && P.nb == 0) break;
-        const unsigned* cs = pass == 0 ? cell_start : bcell_start;
-        for (int dx = -1; dx <= 1; ++dx) {
-            const int x = cx + dx;
-            if (x < 0 || x >= P.dimx) continue;
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int y = cy + dy;
-                if (y < 0 || y >= P.dimy) continue;
-                for (int dz = -1; dz <= 1; ++dz) {
-                    const int z = cz + dz;
-                    if (z < 0 || z >= P.dimz) continue;
-                    const unsigned c = brick_morton(x, y, z, P);
-                    const unsigned e = cs[c + 1];
-                    for (unsigned q = cs[c]; q < e; ++q) {
-                        if (pass == 0) {
-                            const float s2 = dist2_exact(xi, pos[q]);
-                            if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(s2, P)));
-                        } else {
-                            const float4 xb = bpos[q];
-                            const float s2 = dist2_exact(xi, xb);
-                            if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(s2, P)));
-                        }
-                    }
-                }
-            }
+    for_cells27(xi, P.h, g, [&](unsigned c) {
+        for (unsigned q = cell_start[c]; q < cell_start[c + 1]; ++q) {
+            const float s2 = dist2_exact(xi, pos[q]);
+            if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(s2, P)));
         }
-    }
+    });
+    if (P.nb > 0)
+        for_cells27(xi, P.h, g, [&](unsigned c) {
+            for (unsigned q = bcell_start[c]; q < bcell_start[c + 1]; ++q) {
+                const float4 xb = bpos[q];
+                const float s2 = dist2_exact(xi, xb);
+                if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(s2, P)));
+            }
+        });
     rho_out[orig[i]] = rho;
 }
 
@@ -248,7 +232,7 @@ extern "C" int sph_density_noalloc(float particle_radius, float density0, const 
         gb.orig_out = borig;
         gb.v4_in[0] = braw;
         gb.v4_out[0] = bpos;
-        launch_sort(P, (int)nb, braw, cell_count, bcell_start, block_sums, cell_of, slot, key, src, ids, gb, s);
+        launch_sort(P, SceneRef{}, (int)nb, braw, cell_count, bcell_start, block_sums, cell_of, slot, key, src, ids, gb, s);
     } else {
         e = cudaMemsetAsync(bcell_start, 0, ((size_t)P.ncells + 1) * sizeof(unsigned), s);
         if (e != cudaSuccess) return na_fail(SPH_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
@@ -258,7 +242,7 @@ extern "C" int sph_density_noalloc(float particle_radius, float density0, const 
     gf.orig_out = orig;
     gf.v4_in[0] = pos_raw;
     gf.v4_out[0] = pos;
-    launch_sort(P, (int)nf, pos_raw, cell_count, cell_start, block_sums, cell_of, slot, key, src, ids, gf, s);
+    launch_sort(P, SceneRef{}, (int)nf, pos_raw, cell_count, cell_start, block_sums, cell_of, slot, key, src, ids, gf, s);
     k_na_density<<<(nf + 127) / 128, 128, 0, s>>>(P, pos, cell_start, orig, bpos, bcell_start, rho_out);
     e = cudaGetLastError();
     if (e != cudaSuccess) return na_fail(SPH_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));

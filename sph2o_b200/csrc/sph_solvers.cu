@@ -119,7 +119,11 @@ __global__ void __launch_bounds__(128, 12) k_forces(SimParams P, DeviceArrays A)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < P.nf;
     const size_t nf = (size_t)P.nf;
-    const float dt = A.st->dt;
+    /* per-scene coefficients and time step of a batch */
+    const unsigned scene = (A.sst && active) ? A.sref.scene_of[i] : 0u;
+    const float dt = A.sst ? (active ? A.sst[scene].dt : 0.0f) : A.st->dt;
+    const float visc_c = A.sst ? (active ? A.sref.scenes[scene].visc : 0.0f) : P.visc;
+    const float bvisc_c = A.sst ? (active ? A.sref.scenes[scene].bvisc : 0.0f) : P.bvisc;
     float ax = 0.0f, ay = 0.0f, az = 0.0f;
     float4 xi = make_float4(0, 0, 0, 0), vi = xi;
     if (active) {
@@ -152,13 +156,13 @@ __global__ void __launch_bounds__(128, 12) k_forces(SimParams P, DeviceArrays A)
                 const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
                 if (vm == 1) {
                     const float dot = (dvx * p.rx + dvy * p.ry) + dvz * p.rz;
-                    const float c = P.visc * (P.mass / rho_j) * dot / (p.s + eps_h2) * f;
+                    const float c = visc_c * (P.mass / rho_j) * dot / (p.s + eps_h2) * f;
                     ax += c * p.rx; ay += c * p.ry; az += c * p.rz;
                 } else if (vm == 0) {
                     const float c = P.mass / rho_j * visco_lapl(p.rl, P);
                     svx -= c * dvx; svy -= c * dvy; svz -= c * dvz;
                 } else {
-                    const float c = P.visc * (P.mass / rho_j) * cs_W(p.rl * P.inv_h, P) / dt;
+                    const float c = visc_c * (P.mass / rho_j) * cs_W(p.rl * P.inv_h, P) / dt;
                     ax -= c * dvx; ay -= c * dvy; az -= c * dvz;
                 }
             }
@@ -172,10 +176,10 @@ __global__ void __launch_bounds__(128, 12) k_forces(SimParams P, DeviceArrays A)
             }
         }
         if (vm == 0) {
-            const float c = P.visc / rho_i;
+            const float c = visc_c / rho_i;
             ax += svx * c; ay += svy * c; az += svz * c;
         }
-        const bool bvisc = vm >= 0 && P.bvisc != 0.0f;
+        const bool bvisc = vm >= 0 && bvisc_c != 0.0f;
         if (pressure || bvisc || (np && P.adh_on)) {
             float bvx = 0.0f, bvy = 0.0f, bvz = 0.0f;
             for (unsigned kk = 0; kk < nB; ++kk) {
@@ -190,13 +194,13 @@ __global__ void __launch_bounds__(128, 12) k_forces(SimParams P, DeviceArrays A)
                 if (bvisc) {
                     if (vm == 1) {
                         const float dot = (vi.x * p.rx + vi.y * p.ry) + vi.z * p.rz;
-                        const float c = P.bvisc * (psi / rho_i) * dot / (p.s + eps_h2) * f;
+                        const float c = bvisc_c * (psi / rho_i) * dot / (p.s + eps_h2) * f;
                         ax += c * p.rx; ay += c * p.ry; az += c * p.rz;
                     } else if (vm == 0) {
                         const float c = psi / rho_i * visco_lapl(p.rl, P);
                         bvx -= c * vi.x; bvy -= c * vi.y; bvz -= c * vi.z;
                     } else {
-                        const float c = P.bvisc * (psi / rho_i) * cs_W(p.rl * P.inv_h, P) / dt;
+                        const float c = bvisc_c * (psi / rho_i) * cs_W(p.rl * P.inv_h, P) / dt;
                         ax -= c * vi.x; ay -= c * vi.y; az -= c * vi.z;
                     }
                 }
@@ -206,7 +210,7 @@ __global__ void __launch_bounds__(128, 12) k_forces(SimParams P, DeviceArrays A)
                 }
             }
             if (bvisc && vm == 0) {
-                const float c = P.bvisc / rho_i;
+                const float c = bvisc_c / rho_i;
                 ax += bvx * c; ay += bvy * c; az += bvz * c;
             }
         }
@@ -224,7 +228,12 @@ __global__ void __launch_bounds__(128, 12) k_forces(SimParams P, DeviceArrays A)
             A.pos_alt[i] = make_float4(px, py, pz, 0.0f);
             if (!isfinite(px) || !isfinite(py) || !isfinite(pz)) atomicOr(&A.st->err, ERRBIT_NAN);
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (A.sst) {
+            if (active && (unsigned)i == A.sref.scenes[scene].fbegin) {
+                A.sst[scene].time += (double)dt;
+                A.sst[scene].steps += 1u;
+            }
+        } else if (blockIdx.x == 0 && threadIdx.x == 0) {
             A.st->time += (double)dt;
             A.st->steps += 1u;
         }
@@ -240,8 +249,19 @@ __global__ void __launch_bounds__(128, 12) k_forces(SimParams P, DeviceArrays A)
             speed = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(cx, cx), __fmul_rn(cy, cy)), __fmul_rn(cz, cz)));
             if (!(speed == speed)) speed = 3.0e38f;
         }
-        const float m = block_max(speed, s_red);
-        if (threadIdx.x == 0) atomicMax(&A.st->vmax_bits, __float_as_uint(m));
+        if (A.sst) {
+            /* per-scene maximum: one atomic per warp when the warp holds one scene */
+            const unsigned s0 = __shfl_sync(0xffffffffu, scene, 0);
+            if (__all_sync(0xffffffffu, !active || scene == s0)) {
+                const float m = warp_max(speed);
+                if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(&A.sst[s0].vmax_bits, __float_as_uint(m));
+            } else if (active) {
+                atomicMax(&A.sst[scene].vmax_bits, __float_as_uint(speed));
+            }
+        } else {
+            const float m = block_max(speed, s_red);
+            if (threadIdx.x == 0) atomicMax(&A.st->vmax_bits, __float_as_uint(m));
+        }
     }
 }
 
@@ -437,6 +457,182 @@ __global__ void __launch_bounds__(kSolverBlock, 8) k_dfsph_solve(SimParams P, De
 }
 
 /* ---------------------------------------------------------------------- */
+/* DFSPH over a batch of independent scenes: the same passes, each scene with
+   its own dt (CFL + iteration rule), residual and convergence test. A scene
+   that has converged stops contributing; the loop runs until no scene is
+   active (masked convergence). Residuals are reduced per scene in FP64 with
+   one atomic per warp when the warp holds a single scene.                  */
+
+__device__ __forceinline__ void scene_accumulate(double* accum, unsigned stride, unsigned it, unsigned scene,
+                                                 bool valid, double v)
+{
+    const unsigned s0 = __shfl_sync(0xffffffffu, scene, 0);
+    if (__all_sync(0xffffffffu, !valid || scene == s0)) {
+        v = warp_sum(valid ? v : 0.0);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&accum[(size_t)s0 * stride + it], v);
+    } else if (valid) {
+        atomicAdd(&accum[(size_t)scene * stride + it], v);
+    }
+}
+
+template <bool DIV>
+__global__ void __launch_bounds__(kSolverBlock, 8) k_dfsph_solve_batch(SimParams P, DeviceArrays A)
+{
+    DevState* st = A.st;
+    SceneState* sst = A.sst;
+    const SceneInfo* sc = A.sref.scenes;
+    const unsigned* so = A.sref.scene_of;
+    const int nfi = P.nf, ns = A.nscenes;
+    const size_t nf = (size_t)nfi;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthr = gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const unsigned stride = A.accum_stride;
+    const unsigned min_it = DIV ? P.min_it_v : P.min_it;
+    const unsigned max_it = P.max_it;
+
+    /* per-scene time step (DFSPHSolver::updateTimeStep) and first activity */
+    for (int s = tid; s < ns; s += nthr) {
+        float dt;
+        if (!DIV) {
+            float vmax = __uint_as_float(sst[s].vmax_bits);
+            if (vmax < 1.0e-9f) vmax = 1.0e-9f;
+            const float cfl_ts = P.cfl * 0.4f * (2.0f * P.r) / vmax;
+            const unsigned its = max(sst[s].its, sst[s].its_v);
+            float hs = sst[s].dt;
+            if (its > 6u) hs *= 0.9f;
+            else if (its < 4u) hs *= 1.05f;
+            hs = fminf(hs, cfl_ts);
+            hs = fmaxf(hs, P.min_ts);
+            dt = fminf(hs, P.max_ts);
+            sst[s].last_vmax = vmax;
+        } else {
+            dt = sst[s].dt;
+        }
+        sst[s].dt_next = dt;
+        sst[s].active = (min_it > 0u && max_it > 0u) ? 1u : 0u;  /* parity 0: iteration 0 */
+    }
+    if (!grid_barrier(st)) return;
+    if (!DIV) {
+        for (int i = tid; i < nfi; i += nthr) {
+            const float dt = sst[so[i]].dt_next;
+            const float4 a = A.acc[i];
+            float4 v = A.vel[i];
+            v.x = __fadd_rn(v.x, __fmul_rn(__fadd_rn(a.x, P.gx), dt));
+            v.y = __fadd_rn(v.y, __fmul_rn(__fadd_rn(a.y, P.gy), dt));
+            v.z = __fadd_rn(v.z, __fmul_rn(__fadd_rn(a.z, P.gz), dt));
+            A.vel[i] = v;
+            A.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        if (!grid_barrier(st)) return;
+    }
+    float* kws = DIV ? A.kvws : A.kws;
+    for (int i = tid; i < nfi; i += nthr) {
+        const float dt = sst[so[i]].dt_next;
+        const float r = dfsph_residual<DIV>(P, A, i, nf, dt);
+        if (DIV) kws[i] = r > 0.0f ? kws[i] / dt : 0.0f;
+        else kws[i] = r > P.rho0 ? kws[i] / (dt * dt) : 0.0f;
+    }
+    if (!grid_barrier(st)) return;
+    for (int i = tid; i < nfi; i += nthr) dfsph_correct(P, A, kws, i, nf, sst[so[i]].dt_next);
+    if (!grid_barrier(st)) return;
+    for (int i = tid; i < nfi; i += nthr) kws[i] = 0.0f;
+
+    /* activity for iteration it lives in bit (it & 1) of SceneState::active;
+       the convergence test of iteration it keeps that bit (the correction
+       pass of the same iteration still reads it) and sets the other one,
+       dropping whatever the iteration before left there */
+    bool any = min_it > 0u && max_it > 0u && ns > 0;
+    unsigned it = 0;
+    while (any) {
+        const unsigned bit = 1u << (it & 1u);
+        for (int i0 = tid - lane; i0 < nfi; i0 += nthr) {
+            const int i = i0 + lane;
+            const bool valid_i = i < nfi;
+            const unsigned s = valid_i ? so[i] : 0u;
+            const bool on = valid_i && (sst[s].active & bit);
+            double err = 0.0;
+            if (on) {
+                const float dt = sst[s].dt_next;
+                const float r = dfsph_residual<DIV>(P, A, i, nf, dt);
+                float k;
+                if (DIV) {
+                    k = r * A.alpha[i] / (dt * A.rho[i]);
+                    err = (double)(r / P.rho0);
+                } else {
+                    k = __fdiv_rn(__fmul_rn(__fsub_rn(r, P.rho0), A.alpha[i]), __fmul_rn(dt * dt, A.rho[i]));
+                    err = (double)((r - P.rho0) / P.rho0);
+                }
+                A.k[i] = k;
+                kws[i] += k;
+            } else if (valid_i) {
+                A.k[i] = 0.0f;
+            }
+            scene_accumulate(A.accum, stride, it, s, on, err);
+        }
+        if (!grid_barrier(st)) return;
+        /* convergence test per scene for the next iteration */
+        const unsigned nbit = 1u << ((it + 1u) & 1u);
+        for (int s = tid; s < ns; s += nthr) {
+            const unsigned cur = sst[s].active;
+            unsigned nxt = 0u;
+            if (cur & bit) {
+                const double avg = *(volatile double*)&A.accum[(size_t)s * stride + it] / (double)(sc[s].fend - sc[s].fbegin);
+                const float dt = sst[s].dt_next;
+                const double limit = DIV ? (double)(P.eta_v / dt) : (double)P.eta;
+                if (DIV) sst[s].avg_div = avg;
+                else sst[s].avg_dens = avg;
+                nxt = ((avg > limit || it + 1u < min_it) && it + 1u < max_it) ? 1u : 0u;
+                if (DIV) sst[s].its_v = it + 1u;
+                else sst[s].its = it + 1u;
+                if (nxt) atomicOr(&A.any_active[it + 1u], 1u);
+            }
+            sst[s].active = (cur & bit) | (nxt ? nbit : 0u);
+        }
+        for (int i = tid; i < nfi; i += nthr) {
+            const unsigned s = so[i];
+            if (sst[s].active & bit) dfsph_correct(P, A, A.k, i, nf, sst[s].dt_next);
+        }
+        if (!grid_barrier(st)) return;
+        any = *(volatile unsigned*)&A.any_active[it + 1u] != 0u;
+        ++it;
+    }
+
+    for (int i = tid; i < nfi; i += nthr) {
+        const float dt = sst[so[i]].dt_next;
+        kws[i] *= DIV ? dt : dt * dt;
+    }
+    if (!DIV) {
+        bool bad = false;
+        for (int i = tid; i < nfi; i += nthr) {
+            const float dt = sst[so[i]].dt_next;
+            const float4 v = A.vel[i];
+            float4 x = A.pos[i];
+            x.x = __fadd_rn(x.x, __fmul_rn(v.x, dt));
+            x.y = __fadd_rn(x.y, __fmul_rn(v.y, dt));
+            x.z = __fadd_rn(x.z, __fmul_rn(v.z, dt));
+            A.pos[i] = x;
+            bad |= !isfinite(x.x) || !isfinite(x.y) || !isfinite(x.z);
+        }
+        if (bad) atomicOr(&st->err, ERRBIT_NAN);
+    }
+    for (int s = tid; s < ns; s += nthr) {
+        if (!DIV) {
+            if (min_it == 0u || max_it == 0u) sst[s].its = 0u;
+            sst[s].dt = sst[s].dt_next;
+            sst[s].sum_its += sst[s].its;
+        } else {
+            if (min_it == 0u || max_it == 0u) sst[s].its_v = 0u;
+            sst[s].sum_its_v += sst[s].its_v;
+            sst[s].time += (double)sst[s].dt;
+            sst[s].steps += 1u;
+            sst[s].vmax_bits = 0u;
+        }
+        sst[s].active = 0u;
+    }
+}
+
+/* ---------------------------------------------------------------------- */
 /* PCISPH                                                                   */
 
 __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, DeviceArrays A)
@@ -475,42 +671,26 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
         for (int i = tid; i < nfi; i += nthr) {
             const float4 xi = A.pos[i];
             const float4 pi = A.predr[i];
-            const int cx = cell_coord(xi.x, P.h, P.cminx, P.dimx);
-            const int cy = cell_coord(xi.y, P.h, P.cminy, P.dimy);
-            const int cz = cell_coord(xi.z, P.h, P.cminz, P.dimz);
             /* all fluid candidates of the 27 cells first, then all boundary
                candidates: the reference's summation order (PCISPHSolver.cpp:180-206) */
+            const Grid g = grid_for(P, A.sref, (unsigned)i);
             float rho = 0.0f;
-            for (int pass = 0; pass < 2; ++pass) {
-                if (pass == 1 && P.nb == 0) break;
-                const unsigned* __restrict__ cs = pass == 0 ? A.cell_start : A.bcell_start;
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int x = cx + dx;
-                    if (x < 0 || x >= P.dimx) continue;
-                    for (int dy = -1; dy <= 1; ++dy) {
-                        const int y = cy + dy;
-                        if (y < 0 || y >= P.dimy) continue;
-                        for (int dz = -1; dz <= 1; ++dz) {
-                            const int z = cz + dz;
-                            if (z < 0 || z >= P.dimz) continue;
-                            const unsigned c = brick_morton(x, y, z, P);
-                            const unsigned e = cs[c + 1];
-                            if (pass == 0) {
-                                for (unsigned q = cs[c]; q < e; ++q) {
-                                    const float s2 = dist2_exact(pi, A.predr[q]);
-                                    if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(s2, P)));
-                                }
-                            } else {
-                                for (unsigned q = cs[c]; q < e; ++q) {
-                                    const float4 xb = A.bpos[q];
-                                    const float s2 = dist2_exact(pi, xb);
-                                    if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(s2, P)));
-                                }
-                            }
-                        }
-                    }
+            for_cells27(xi, P.h, g, [&](unsigned c) {
+                const unsigned e = A.cell_start[c + 1];
+                for (unsigned q = A.cell_start[c]; q < e; ++q) {
+                    const float s2 = dist2_exact(pi, A.predr[q]);
+                    if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(s2, P)));
                 }
-            }
+            });
+            if (P.nb > 0)
+                for_cells27(xi, P.h, g, [&](unsigned c) {
+                    const unsigned e = A.bcell_start[c + 1];
+                    for (unsigned q = A.bcell_start[c]; q < e; ++q) {
+                        const float4 xb = A.bpos[q];
+                        const float s2 = dist2_exact(pi, xb);
+                        if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(s2, P)));
+                    }
+                });
             A.rho[i] = rho;
             const float err = fmaxf(0.0f, __fsub_rn(rho, P.rho0));
             A.press[i] = __fadd_rn(A.press[i], __fmul_rn(P.pcisph_delta, err));
@@ -627,13 +807,15 @@ void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, cudaStre
     }
 }
 
-int persistent_grid(bool pcisph, bool divergence)
+int persistent_grid(bool pcisph, bool divergence, bool batch)
 {
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
     const void* fn = pcisph ? (const void*)k_pcisph_solve
-                            : divergence ? (const void*)k_dfsph_solve<true> : (const void*)k_dfsph_solve<false>;
+                     : batch ? (divergence ? (const void*)k_dfsph_solve_batch<true>
+                                           : (const void*)k_dfsph_solve_batch<false>)
+                             : (divergence ? (const void*)k_dfsph_solve<true> : (const void*)k_dfsph_solve<false>);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolverBlock, 0) != cudaSuccess) return 0;
     return per_sm * sms;
 }
@@ -652,6 +834,14 @@ int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergenc
     const int g = grid < need ? grid : need;
     return coop_launch(divergence ? (const void*)k_dfsph_solve<true> : (const void*)k_dfsph_solve<false>, P, A,
                        g > 0 ? g : 1, s);
+}
+
+int launch_dfsph_solve_batch(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s)
+{
+    const int need = blocks_for(P.nf > 0 ? P.nf : 1, kSolverBlock);
+    const int g = grid < need ? grid : need;
+    return coop_launch(divergence ? (const void*)k_dfsph_solve_batch<true> : (const void*)k_dfsph_solve_batch<false>,
+                       P, A, g > 0 ? g : 1, s);
 }
 
 int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s)
