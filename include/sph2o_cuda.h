@@ -155,6 +155,25 @@ int sph_profile_enable(sph_ctx* ctx, int enable);
    (arrays of SPH_PROF_COUNT; either may be NULL). Waits for queued work. */
 int sph_profile_read(sph_ctx* ctx, double* ms, unsigned long long* launches);
 
+/* ---- launch options and autotuning (no reference counterpart) -------- */
+enum sph_option {
+    SPH_OPT_CUDA_GRAPHS = 0,      /* 1 (default): steps taken in pairs replay a captured CUDA graph */
+    SPH_OPT_CELL_ORDER = 1,       /* 0 (default): 4x4x4 cell bricks, Morton inside; 1: linear, x fastest */
+    SPH_OPT_SOLVER_OCCUPANCY = 2, /* DFSPH persistent solver blocks per SM: 8 (default) or 4 */
+    SPH_OPT_PASS_BLOCK = 3        /* threads per block of the particle-pass kernels: 256 (default) or 128 */
+};
+int sph_set_option(sph_ctx* ctx, int option, int value);
+int sph_get_option(const sph_ctx* ctx, int option, int* value);
+
+/* Chooses SPH_OPT_CELL_ORDER, SPH_OPT_SOLVER_OCCUPANCY and SPH_OPT_PASS_BLOCK
+   by timing trial_steps steps (CUDA events) of every combination, each from
+   a snapshot of the current state that is restored afterwards: the
+   simulation is left exactly where it was. cache_path (may be NULL) names a
+   JSON file keyed by GPU name, method and particle counts; a hit skips the
+   trials and a miss appends the result. config (may be NULL) receives the
+   three chosen values in option order 1..3. */
+int sph_autotune(sph_ctx* ctx, int trial_steps, const char* cache_path, int* config);
+
 /* Fluid state in the caller's particle order. Any pointer may be NULL.
    rho is FluidObject::density as SPH2O leaves it after a step. */
 int sph_get_state(sph_ctx* ctx, float* xyz, float* v, float* rho);

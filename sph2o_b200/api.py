@@ -27,6 +27,7 @@ STATUS = {
     -7: "SPH_ERR_NO_DEVICE", -8: "SPH_ERR_IO", -9: "SPH_ERR_CAPACITY",
 }
 PHASE_DENSITY, PHASE_ALPHA, PHASE_NONPRESSURE_ACC, PHASE_PRESSURE, PHASE_PRESSURE_ACC = range(5)
+OPT_CUDA_GRAPHS, OPT_CELL_ORDER, OPT_SOLVER_OCCUPANCY, OPT_PASS_BLOCK = range(4)
 PROF_NAMES = ["sort", "lists", "density", "normals", "forces", "density_solve", "divergence_solve",
               "pressure_solve"]
 PROF_COUNT = len(PROF_NAMES)
@@ -103,6 +104,9 @@ def lib():
         "sph_debug_neighbors": (I, [P, C.POINTER(U), C.POINTER(U), C.c_size_t, C.POINTER(U), C.POINTER(U),
                                     C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
         "sph_debug_barrier_timeout": (I, [P]),
+        "sph_set_option": (I, [P, I, I]),
+        "sph_get_option": (I, [P, I, C.POINTER(I)]),
+        "sph_autotune": (I, [P, I, C.c_char_p, C.POINTER(I)]),
         "sph_profile_enable": (I, [P, I]),
         "sph_profile_read": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_ulonglong)]),
         "sph_batch_create": (I, [C.POINTER(SceneDesc), U, C.POINTER(P)]),
@@ -267,6 +271,20 @@ class Simulation:
         out = np.zeros((self.nf, 3) if vec else self.nf, np.float32)
         self._check(lib().sph_compute_phase(self._h, int(phase), _fptr(out)))
         return out
+
+    def set_option(self, option, value):
+        self._check(lib().sph_set_option(self._h, int(option), int(value)))
+
+    def get_option(self, option):
+        v = C.c_int()
+        self._check(lib().sph_get_option(self._h, int(option), C.byref(v)))
+        return v.value
+
+    def autotune(self, trial_steps=3, cache_path=None):
+        cfg = (C.c_int * 3)()
+        path = os.fsencode(cache_path) if cache_path else None
+        self._check(lib().sph_autotune(self._h, int(trial_steps), path, cfg))
+        return {"cell_order": cfg[0], "solver_occupancy": cfg[1], "pass_block": cfg[2]}
 
     def profile(self, enable=True):
         self._check(lib().sph_profile_enable(self._h, 1 if enable else 0))

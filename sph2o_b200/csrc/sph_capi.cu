@@ -16,13 +16,16 @@
  * No step makes a host round trip; sph_step waits once at the end.
  */
 #include "../../include/sph2o_cuda.h"
+#include "../host/json_lite.h"
 #include "sph_internal.h"
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <new>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -91,9 +94,31 @@ struct sph_ctx {
     unsigned accum_stride = 0;
     int grid_batch_density = 0, grid_batch_div = 0;
     std::vector<SceneState> last_sst;
+    /* CUDA graphs of two steps, keyed by the buffer assignment they start
+       from (the sort swaps buffers, two steps may return to the start) */
+    bool use_graphs = true;
+    /* tunables (sph_set_option / sph_autotune) */
+    int pass_block = 256;
+    int solver_occ = 8;
+    int grid_density4 = 0, grid_div4 = 0;
+    float4* braw = nullptr;      /* boundary in caller order (re-sorted when the cell order changes) */
+    unsigned* bid = nullptr;
+    /* autotune snapshot */
+    float4 *snap_pos = nullptr, *snap_vel = nullptr;
+    unsigned* snap_orig = nullptr;
+    float *snap_kws = nullptr, *snap_kvws = nullptr, *snap_rho = nullptr;
+    SceneState* snap_sst = nullptr;
+    DevState* snap_st = nullptr;
+    struct Graph { unsigned key; cudaGraphExec_t exec; unsigned long long launches; };
+    std::vector<Graph> graphs;
+    float4* pos_base = nullptr;
+    unsigned* orig_base = nullptr;
+    float* kws_base = nullptr;
 };
 
 namespace {
+
+void drop_graphs(sph_ctx* c);
 
 int fail(sph_ctx* c, int code, const std::string& msg)
 {
@@ -345,9 +370,9 @@ int step_wcsph(sph_ctx* c)
     int rc;
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     DeviceArrays A = arrays(c);
-    { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, false, true, c->stream); }
-    if (c->P.st_on) { Phase ph(c, SPH_PROF_NORMALS, 1); launch_normals(c->P, A, c->stream); }
-    { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_WCSPH, c->stream); }
+    { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, false, true, c->pass_block, c->stream); }
+    if (c->P.st_on) { Phase ph(c, SPH_PROF_NORMALS, 1); launch_normals(c->P, A, c->pass_block, c->stream); }
+    { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_WCSPH, c->pass_block, c->stream); }
     std::swap(c->pos, c->pos2);
     std::swap(c->vel, c->vel2);
     c->lists_valid = false;
@@ -359,9 +384,9 @@ int step_pcisph(sph_ctx* c)
     int rc;
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     DeviceArrays A = arrays(c);
-    { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, false, false, c->stream); }
-    if (c->P.st_on) { Phase ph(c, SPH_PROF_NORMALS, 1); launch_normals(c->P, A, c->stream); }
-    { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_NP, c->stream); }
+    { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, false, false, c->pass_block, c->stream); }
+    if (c->P.st_on) { Phase ph(c, SPH_PROF_NORMALS, 1); launch_normals(c->P, A, c->pass_block, c->stream); }
+    { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_NP, c->pass_block, c->stream); }
     if ((rc = zero_accum(c)) != SPH_OK) return rc;
     int e;
     { Phase ph(c, SPH_PROF_PRESSURE_SOLVE, 1); e = launch_pcisph_solve(c->P, A, c->grid_pcisph, c->stream); }
@@ -374,25 +399,25 @@ int step_dfsph(sph_ctx* c)
 {
     int rc;
     DeviceArrays A = arrays(c);
-    if (c->P.st_on) { Phase ph(c, SPH_PROF_NORMALS, 1); launch_normals(c->P, A, c->stream); }
-    { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_NP_CFL, c->stream); }
+    if (c->P.st_on) { Phase ph(c, SPH_PROF_NORMALS, 1); launch_normals(c->P, A, c->pass_block, c->stream); }
+    { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_NP_CFL, c->pass_block, c->stream); }
     if ((rc = zero_accum(c)) != SPH_OK) return rc;
     int e;
     {
         Phase ph(c, SPH_PROF_DENSITY_SOLVE, 1);
         e = c->nscenes ? launch_dfsph_solve_batch(c->P, A, false, c->grid_batch_density, c->stream)
-                       : launch_dfsph_solve(c->P, A, false, c->grid_density, c->stream);
+                       : launch_dfsph_solve(c->P, A, false, c->solver_occ == 4 ? c->grid_density4 : c->grid_density, c->solver_occ, c->stream);
     }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph density solver launch: ") + cudaGetErrorString((cudaError_t)e));
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     A = arrays(c);
-    { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, true, false, c->stream); }
+    { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, true, false, c->pass_block, c->stream); }
     A.accum = c->accum + c->accum_len / 2;
     if (c->d_any) A.any_active = c->d_any + ((size_t)c->P.max_it + 2);
     {
         Phase ph(c, SPH_PROF_DIVERGENCE_SOLVE, 1);
         e = c->nscenes ? launch_dfsph_solve_batch(c->P, A, true, c->grid_batch_div, c->stream)
-                       : launch_dfsph_solve(c->P, A, true, c->grid_div, c->stream);
+                       : launch_dfsph_solve(c->P, A, true, c->solver_occ == 4 ? c->grid_div4 : c->grid_div, c->solver_occ, c->stream);
     }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph divergence solver launch: ") + cudaGetErrorString((cudaError_t)e));
     return check_launch(c, "dfsph step");
@@ -426,6 +451,7 @@ int recover_overflow(sph_ctx* c)
         auto it = std::find(c->allocations.begin(), c->allocations.end(), (void*)p);
         if (it != c->allocations.end()) { cudaFree(p); c->allocations.erase(it); }
     };
+    drop_graphs(c);
     drop(c->nbr_f);
     drop(c->nbr_b);
     c->P.capF = c->P.capF + c->P.capF / 2;
@@ -451,6 +477,84 @@ int fill_stats(sph_ctx* c, const DevState& before, const DevState& now, sph_step
     out->neighbor_overflows = now.overflow;
     (void)c;
     return SPH_OK;
+}
+
+unsigned buffer_key(const sph_ctx* c)
+{
+    return (c->pos == c->pos_base ? 1u : 0u) | (c->orig == c->orig_base ? 2u : 0u) | (c->kws == c->kws_base ? 4u : 0u);
+}
+
+void drop_graphs(sph_ctx* c)
+{
+    for (auto& g : c->graphs) cudaGraphExecDestroy(g.exec);
+    c->graphs.clear();
+}
+
+int eager_step(sph_ctx* c)
+{
+    switch (c->desc.simulation_method) {
+    case SPH_WCSPH: return step_wcsph(c);
+    case SPH_PCISPH: return step_pcisph(c);
+    default: return step_dfsph(c);
+    }
+}
+
+/* Two steps as one CUDA graph: captured on first use for the current buffer
+   assignment, replayed afterwards. Returns false when capture is not
+   possible (the caller then steps eagerly and stops trying). */
+bool graph_two_steps(sph_ctx* c, int* rc)
+{
+    const unsigned key = buffer_key(c);
+    for (auto& g : c->graphs)
+        if (g.key == key) {
+            const cudaError_t e = cudaGraphLaunch(g.exec, c->stream);
+            if (e != cudaSuccess) { *rc = fail(c, SPH_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); return true; }
+            c->launches += g.launches;
+            *rc = SPH_OK;
+            return true;
+        }
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    /* host-side buffer assignment before capture, restored if capture fails
+       (captured work never ran, so swaps made while capturing must be undone) */
+    float4 *p0 = c->pos, *p1 = c->pos2, *v0 = c->vel, *v1 = c->vel2;
+    unsigned *o0 = c->orig, *o1 = c->orig2;
+    float *k0 = c->kws, *k1 = c->kws2, *q0 = c->kvws, *q1 = c->kvws2;
+    const bool lv = c->lists_valid;
+    auto restore = [&]() {
+        c->pos = p0; c->pos2 = p1; c->vel = v0; c->vel2 = v1; c->orig = o0; c->orig2 = o1;
+        c->kws = k0; c->kws2 = k1; c->kvws = q0; c->kvws2 = q1; c->lists_valid = lv;
+    };
+    const unsigned long long l0 = c->launches;
+    int r = eager_step(c);
+    if (r == SPH_OK) r = eager_step(c);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
+    const unsigned long long nl = c->launches - l0;
+    c->launches = l0;
+    if (r != SPH_OK || ec != cudaSuccess || !graph || buffer_key(c) != key) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        restore();
+        c->err.clear();
+        return false;
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+        cudaGetLastError();
+        restore();
+        return false;
+    }
+    c->graphs.push_back({key, exec, nl});
+    const cudaError_t e = cudaGraphLaunch(exec, c->stream);
+    if (e != cudaSuccess) { *rc = fail(c, SPH_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); return true; }
+    c->launches += nl;
+    *rc = SPH_OK;
+    return true;
 }
 
 } // namespace
@@ -571,6 +675,7 @@ int sph_init(sph_ctx* c)
             si.grid.dimx = dim[0]; si.grid.dimy = dim[1]; si.grid.dimz = dim[2];
             si.grid.nbx = dim[0] / 4; si.grid.nby = dim[1] / 4;
             si.grid.base = (unsigned)base;
+            si.grid.order = P.cell_order;
             base += (unsigned long long)dim[0] * dim[1] * dim[2];
             if (base > (1ull << 28)) return fail(c, SPH_ERR_CAPACITY, "batch too large: more than 2^28 grid cells");
             const sph_scene_desc& ds = c->descs[s];
@@ -639,6 +744,9 @@ int sph_init(sph_ctx* c)
     ALLOC(cnt_f, nf); ALLOC(cnt_b, nf);
     ALLOC(st, 1);
 #undef ALLOC
+    c->pos_base = c->pos;
+    c->orig_base = c->orig;
+    c->kws_base = c->kws;
     if ((rc = alloc_lists(c)) != SPH_OK) return rc;
     c->accum_len = 2 * ((size_t)P.max_it + 2) * std::max(1u, c->nscenes);
     if ((rc = dalloc(c, &c->accum, c->accum_len)) != SPH_OK) return rc;
@@ -672,8 +780,10 @@ int sph_init(sph_ctx* c)
     CUDA_TRY(c, cudaEventCreate(&c->ev_begin));
     CUDA_TRY(c, cudaEventCreate(&c->ev_end));
 
-    c->grid_density = persistent_grid(false, false);
-    c->grid_div = persistent_grid(false, true);
+    c->grid_density = persistent_grid(false, false, false, 8);
+    c->grid_div = persistent_grid(false, true, false, 8);
+    c->grid_density4 = persistent_grid(false, false, false, 4);
+    c->grid_div4 = persistent_grid(false, true, false, 4);
     c->grid_pcisph = persistent_grid(true, false);
     if (c->grid_density <= 0 || c->grid_div <= 0 || c->grid_pcisph <= 0)
         return fail(c, SPH_ERR_CUDA, "cannot size the persistent solver grid");
@@ -691,10 +801,10 @@ int sph_init(sph_ctx* c)
 
     /* boundary: sort once, volumes (SPHSolver::init, SPHSolver.cpp:21-38) */
     if (nb > 0) {
-        float4* braw = nullptr;
-        unsigned* bid = nullptr;
-        if ((rc = dalloc(c, &braw, nb)) != SPH_OK) return rc;
-        if ((rc = dalloc(c, &bid, nb)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->braw, nb)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->bid, nb)) != SPH_OK) return rc;
+        float4* braw = c->braw;
+        unsigned* bid = c->bid;
         CUDA_TRY(c, cudaMemcpyAsync(stage, c->h_bound.data(), 3 * nb * sizeof(float), cudaMemcpyHostToDevice, c->stream));
         launch_pack_v3((int)nb, stage, braw, 0.0f, c->stream);
         launch_iota((int)nb, bid, c->stream);
@@ -717,7 +827,7 @@ int sph_init(sph_ctx* c)
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     if (c->desc.simulation_method == SPH_DFSPH) {
         /* DFSPHSolver::init: densities and alpha at the initial positions */
-        launch_density(P, arrays(c), true, false, c->stream);
+        launch_density(P, arrays(c), true, false, c->pass_block, c->stream);
     }
     if ((rc = check_launch(c, "init")) != SPH_OK) return rc;
     DevState now{};
@@ -738,14 +848,21 @@ int sph_step_async(sph_ctx* c, int nsteps)
         c->batch_open = true;
         c->launches_at_open = c->launches;
     }
-    for (int s = 0; s < nsteps; ++s) {
-        int rc;
-        switch (c->desc.simulation_method) {
-        case SPH_WCSPH: rc = step_wcsph(c); break;
-        case SPH_PCISPH: rc = step_pcisph(c); break;
-        default: rc = step_dfsph(c); break;
+    int left = nsteps;
+    while (left > 0) {
+        int rc = SPH_OK;
+        if (left >= 2 && c->use_graphs && !c->prof) {
+            if (graph_two_steps(c, &rc)) {
+                if (rc != SPH_OK) return rc;
+                left -= 2;
+                continue;
+            }
+            c->use_graphs = false;  /* capture unsupported: stay eager */
+            drop_graphs(c);
         }
+        rc = eager_step(c);
         if (rc != SPH_OK) return rc;
+        --left;
     }
     CUDA_TRY(c, cudaEventRecord(c->ev_end, c->stream));
     return SPH_OK;
@@ -861,7 +978,7 @@ int sph_set_state(sph_ctx* c, const float* xyz, const float* v)
         /* DFSPH keeps densities/alpha of the current positions between steps */
         int rc = neighbor_search(c);
         if (rc != SPH_OK) return rc;
-        launch_density(c->P, arrays(c), true, false, c->stream);
+        launch_density(c->P, arrays(c), true, false, c->pass_block, c->stream);
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     }
     return check_launch(c, "set_state");
@@ -942,6 +1059,7 @@ int sph_destroy(sph_ctx* c)
     if (!c) return SPH_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     drain_profile(c);
+    drop_graphs(c);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev_begin) cudaEventDestroy(c->ev_begin);
     if (c->ev_end) cudaEventDestroy(c->ev_end);
@@ -962,7 +1080,7 @@ int sph_compute_phase(sph_ctx* c, int phase, float* out)
     if (rc != SPH_OK) return rc;
     DeviceArrays A = arrays(c);
     const bool eos = phase == SPH_PHASE_PRESSURE || phase == SPH_PHASE_PRESSURE_ACC;
-    launch_density(c->P, A, phase == SPH_PHASE_ALPHA || c->desc.simulation_method == SPH_DFSPH, eos, c->stream);
+    launch_density(c->P, A, phase == SPH_PHASE_ALPHA || c->desc.simulation_method == SPH_DFSPH, eos, c->pass_block, c->stream);
     const size_t nf = c->nf;
     float* tmp = nullptr;
     CUDA_TRY(c, cudaMallocAsync((void**)&tmp, 3 * nf * sizeof(float), c->stream));
@@ -972,13 +1090,13 @@ int sph_compute_phase(sph_ctx* c, int phase, float* out)
     case SPH_PHASE_ALPHA: launch_unsort_f((int)nf, c->orig, c->alpha, tmp, c->stream); break;
     case SPH_PHASE_PRESSURE: launch_unsort_f((int)nf, c->orig, c->press, tmp, c->stream); break;
     case SPH_PHASE_NONPRESSURE_ACC:
-        if (c->P.st_on) launch_normals(c->P, A, c->stream);
-        launch_forces(c->P, A, FORCE_NP, c->stream);
+        if (c->P.st_on) launch_normals(c->P, A, c->pass_block, c->stream);
+        launch_forces(c->P, A, FORCE_NP, c->pass_block, c->stream);
         launch_unsort_v4((int)nf, c->orig, c->acc, tmp, c->stream);
         count = 3 * nf;
         break;
     default:
-        launch_forces(c->P, A, FORCE_PRESSURE, c->stream);
+        launch_forces(c->P, A, FORCE_PRESSURE, c->pass_block, c->stream);
         launch_unsort_v4((int)nf, c->orig, c->acc, tmp, c->stream);
         count = 3 * nf;
         break;
@@ -989,6 +1107,260 @@ int sph_compute_phase(sph_ctx* c, int phase, float* out)
     cudaFreeAsync(tmp, c->stream);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return check_launch(c, "compute_phase");
+}
+
+} // extern "C"
+
+namespace {
+
+/* Re-sort the static boundary and recompute its volumes (cell order change). */
+int resort_boundary(sph_ctx* c)
+{
+    if (c->nb == 0) return SPH_OK;
+    GatherSet g{};
+    g.orig_out = c->borig;
+    g.v4_in[0] = c->braw;
+    g.v4_out[0] = c->bpos;
+    const SceneRef bref{c->d_scenes, c->d_bscene_of};
+    launch_sort(c->P, bref, (int)c->nb, c->braw, c->cell_count, c->bcell_start, c->block_sums, c->cell_of, c->slot,
+                c->tmp_key, c->tmp_src, c->bid, g, c->stream);
+    launch_boundary_volume(c->P, bref, c->bpos, c->bcell_start, c->bvol, c->stream);
+    return check_launch(c, "boundary re-sort");
+}
+
+/* Make the between-steps data consistent with the current cell order. WCSPH
+   and PCISPH search at the start of every step and need nothing; DFSPH
+   carries lists, densities and alpha from the end of a step, so it searches
+   again (at unchanged positions the sort is the identity up to the cell
+   order) and recomputes them, which reproduces them bit for bit. */
+int refresh(sph_ctx* c)
+{
+    if (c->desc.simulation_method != SPH_DFSPH) {
+        c->lists_valid = false;
+        return SPH_OK;
+    }
+    int rc = neighbor_search(c);
+    if (rc != SPH_OK) return rc;
+    launch_density(c->P, arrays(c), true, false, c->pass_block, c->stream);
+    return check_launch(c, "refresh");
+}
+
+int apply_cell_order(sph_ctx* c, int order)
+{
+    c->P.cell_order = order;
+    if (c->nscenes) {
+        for (auto& si : c->h_scenes) si.grid.order = order;
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_scenes, c->h_scenes.data(), c->nscenes * sizeof(SceneInfo),
+                                    cudaMemcpyHostToDevice, c->stream));
+    }
+    drop_graphs(c);
+    int rc = resort_boundary(c);
+    if (rc != SPH_OK) return rc;
+    return refresh(c);
+}
+
+int snapshot(sph_ctx* c, bool save)
+{
+    const size_t nf = c->nf;
+    int rc;
+    if (!c->snap_pos) {
+        if ((rc = dalloc(c, &c->snap_pos, nf)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->snap_vel, nf)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->snap_orig, nf)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->snap_kws, nf)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->snap_kvws, nf)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->snap_rho, nf)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->snap_st, 1)) != SPH_OK) return rc;
+        if (c->nscenes && (rc = dalloc(c, &c->snap_sst, c->nscenes)) != SPH_OK) return rc;
+    }
+    auto cp = [&](void* a, void* b, size_t bytes) -> int {
+        CUDA_TRY(c, cudaMemcpyAsync(save ? b : a, save ? a : b, bytes, cudaMemcpyDeviceToDevice, c->stream));
+        return SPH_OK;
+    };
+    if ((rc = cp(c->pos, c->snap_pos, nf * sizeof(float4))) != SPH_OK) return rc;
+    if ((rc = cp(c->vel, c->snap_vel, nf * sizeof(float4))) != SPH_OK) return rc;
+    if ((rc = cp(c->orig, c->snap_orig, nf * sizeof(unsigned))) != SPH_OK) return rc;
+    if ((rc = cp(c->kws, c->snap_kws, nf * sizeof(float))) != SPH_OK) return rc;
+    if ((rc = cp(c->kvws, c->snap_kvws, nf * sizeof(float))) != SPH_OK) return rc;
+    if ((rc = cp(c->rho, c->snap_rho, nf * sizeof(float))) != SPH_OK) return rc;
+    if ((rc = cp(c->st, c->snap_st, sizeof(DevState))) != SPH_OK) return rc;
+    if (c->nscenes && (rc = cp(c->d_sst, c->snap_sst, c->nscenes * sizeof(SceneState))) != SPH_OK) return rc;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SPH_OK;
+}
+
+std::string tune_key(sph_ctx* c)
+{
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, c->device);
+    std::ostringstream k;
+    k << prop.name << "|m" << c->desc.simulation_method << "|n" << c->nf << "|b" << c->nb << "|s" << c->nscenes;
+    return k.str();
+}
+
+bool tune_lookup(const char* path, const std::string& key, int* cfg)
+{
+    if (!path) return false;
+    std::ifstream f(path);
+    if (!f) return false;
+    std::stringstream ss;
+    ss << f.rdbuf();
+    try {
+        const sphjson::Value root = sphjson::parse(ss.str());
+        const sphjson::Value* v = root.find(key);
+        if (!v || v->size() != 3) return false;
+        for (int i = 0; i < 3; ++i) cfg[i] = (int)v->at(i).as_number();
+        return true;
+    } catch (const std::exception&) {
+        return false;
+    }
+}
+
+void tune_store(const char* path, const std::string& key, const int* cfg)
+{
+    if (!path) return;
+    std::vector<std::pair<std::string, std::vector<int>>> entries;
+    {
+        std::ifstream f(path);
+        if (f) {
+            std::stringstream ss;
+            ss << f.rdbuf();
+            try {
+                const sphjson::Value root = sphjson::parse(ss.str());
+                for (const auto& kv : root.items()) {
+                    if (kv.first == key || kv.second.size() != 3) continue;
+                    entries.push_back({kv.first, {(int)kv.second.at(0).as_number(), (int)kv.second.at(1).as_number(),
+                                                  (int)kv.second.at(2).as_number()}});
+                }
+            } catch (const std::exception&) {
+            }
+        }
+    }
+    entries.push_back({key, {cfg[0], cfg[1], cfg[2]}});
+    std::ofstream o(path);
+    o << "{\n";
+    for (size_t i = 0; i < entries.size(); ++i) {
+        std::string k;
+        for (char ch : entries[i].first) k += (ch == '"' || ch == '\\') ? std::string("\\") + ch : std::string(1, ch);
+        o << "  \"" << k << "\": [" << entries[i].second[0] << ", " << entries[i].second[1] << ", "
+          << entries[i].second[2] << "]" << (i + 1 < entries.size() ? "," : "") << "\n";
+    }
+    o << "}\n";
+}
+
+int apply_config(sph_ctx* c, const int* cfg)
+{
+    c->solver_occ = cfg[1] == 4 ? 4 : 8;
+    c->pass_block = cfg[2] == 128 ? 128 : 256;
+    drop_graphs(c);
+    if (cfg[0] != c->P.cell_order) return apply_cell_order(c, cfg[0] == 1 ? 1 : 0);
+    return SPH_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int sph_set_option(sph_ctx* c, int option, int value)
+{
+    if (!c) return SPH_ERR_ARG;
+    switch (option) {
+    case SPH_OPT_CUDA_GRAPHS:
+        c->use_graphs = value != 0;
+        if (!c->use_graphs) drop_graphs(c);
+        return SPH_OK;
+    case SPH_OPT_CELL_ORDER:
+        if (value != 0 && value != 1) return fail(c, SPH_ERR_ARG, "cell order is 0 or 1");
+        if (!c->initialized) { c->P.cell_order = value; return SPH_OK; }
+        if (value == c->P.cell_order) return SPH_OK;
+        return apply_cell_order(c, value);
+    case SPH_OPT_SOLVER_OCCUPANCY:
+        if (value != 4 && value != 8) return fail(c, SPH_ERR_ARG, "solver occupancy is 4 or 8");
+        c->solver_occ = value;
+        drop_graphs(c);
+        return SPH_OK;
+    case SPH_OPT_PASS_BLOCK:
+        if (value != 128 && value != 256) return fail(c, SPH_ERR_ARG, "pass block is 128 or 256");
+        c->pass_block = value;
+        drop_graphs(c);
+        return SPH_OK;
+    default:
+        return fail(c, SPH_ERR_ARG, "unknown option");
+    }
+}
+
+int sph_get_option(const sph_ctx* c, int option, int* value)
+{
+    if (!c || !value) return SPH_ERR_ARG;
+    switch (option) {
+    case SPH_OPT_CUDA_GRAPHS: *value = c->use_graphs ? 1 : 0; return SPH_OK;
+    case SPH_OPT_CELL_ORDER: *value = c->P.cell_order; return SPH_OK;
+    case SPH_OPT_SOLVER_OCCUPANCY: *value = c->solver_occ; return SPH_OK;
+    case SPH_OPT_PASS_BLOCK: *value = c->pass_block; return SPH_OK;
+    default: return SPH_ERR_ARG;
+    }
+}
+
+int sph_autotune(sph_ctx* c, int trial_steps, const char* cache_path, int* config)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_autotune before sph_init");
+    if (trial_steps < 1) return fail(c, SPH_ERR_ARG, "trial_steps must be positive");
+    const std::string key = tune_key(c);
+    int best[3] = {c->P.cell_order, c->solver_occ, c->pass_block};
+    int rc;
+    if (tune_lookup(cache_path, key, best)) {
+        if ((rc = apply_config(c, best)) != SPH_OK) return rc;
+        if (config) for (int i = 0; i < 3; ++i) config[i] = best[i];
+        return SPH_OK;
+    }
+    if ((rc = snapshot(c, true)) != SPH_OK) return rc;
+    const DevState last = c->last;
+    const std::vector<SceneState> last_sst = c->last_sst;
+    const bool graphs = c->use_graphs;
+    c->use_graphs = false;
+    double best_ms = 1e300;
+    const bool dfsph = c->desc.simulation_method == SPH_DFSPH;
+    for (int order = 0; order < 2; ++order)
+        for (int occ : {8, 4}) {
+            if ((!dfsph || c->nscenes) && occ == 4) continue;  /* only the single-scene DFSPH solver has it */
+            for (int blk : {256, 128}) {
+                const int cfg[3] = {order, occ, blk};
+                if ((rc = snapshot(c, false)) != SPH_OK) return rc;
+                c->solver_occ = occ;
+                c->pass_block = blk;
+                rc = order != c->P.cell_order ? apply_cell_order(c, order) : refresh(c);
+                if (rc != SPH_OK) return rc;
+                if ((rc = sph_step_async(c, 1)) != SPH_OK) return rc;  /* warm-up */
+                CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+                c->batch_open = false;
+                CUDA_TRY(c, cudaEventRecord(c->ev_begin, c->stream));
+                for (int s = 0; s < trial_steps; ++s)
+                    if ((rc = eager_step(c)) != SPH_OK) return rc;
+                CUDA_TRY(c, cudaEventRecord(c->ev_end, c->stream));
+                CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, c->ev_begin, c->ev_end);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    for (int i = 0; i < 3; ++i) best[i] = cfg[i];
+                }
+            }
+        }
+    /* back to the snapshot with the chosen configuration */
+    if ((rc = snapshot(c, false)) != SPH_OK) return rc;
+    c->solver_occ = best[1];
+    c->pass_block = best[2];
+    rc = best[0] != c->P.cell_order ? apply_cell_order(c, best[0]) : refresh(c);
+    if (rc != SPH_OK) return rc;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->last = last;
+    c->last_sst = last_sst;
+    c->use_graphs = graphs;
+    c->batch_open = false;
+    tune_store(cache_path, key, best);
+    if (config) for (int i = 0; i < 3; ++i) config[i] = best[i];
+    return SPH_OK;
 }
 
 int sph_batch_create(const sph_scene_desc* descs, unsigned nscenes, sph_ctx** out)

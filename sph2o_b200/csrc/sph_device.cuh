@@ -59,6 +59,7 @@ struct SimParams {
     int nbx, nby;              /* 4^3 bricks per axis (x, y)             */
     unsigned ncells;
     unsigned capF, capB;       /* neighbour-list capacity per particle   */
+    int cell_order;            /* 0: 4^3 bricks, Morton inside; 1: linear, x fastest */
 };
 
 /* Device-resident solver state; read by the host after a step. */
@@ -234,6 +235,7 @@ struct Grid {
     int dimx, dimy, dimz;
     int nbx, nby;
     unsigned base;
+    int order;                 /* SimParams::cell_order */
 };
 
 /* Per-scene constants of a batch. Slots [fbegin, fend) of the sorted fluid
@@ -260,11 +262,16 @@ __device__ __forceinline__ Grid grid_single(const SimParams& P)
     g.dimx = P.dimx; g.dimy = P.dimy; g.dimz = P.dimz;
     g.nbx = P.nbx; g.nby = P.nby;
     g.base = 0u;
+    g.order = P.cell_order;
     return g;
 }
 
+/* Cell index of (cx, cy, cz): 4 x 4 x 4 bricks in x-fastest order with
+   Morton order inside a brick (order 0), or plain x-fastest (order 1). */
 __device__ __forceinline__ unsigned brick_morton(int cx, int cy, int cz, const Grid& g)
 {
+    if (g.order == 1)
+        return g.base + ((unsigned)cz * (unsigned)g.dimy + (unsigned)cy) * (unsigned)g.dimx + (unsigned)cx;
     const unsigned lx = (unsigned)cx & 3u, ly = (unsigned)cy & 3u, lz = (unsigned)cz & 3u;
     const unsigned m = (lx & 1u) | ((ly & 1u) << 1) | ((lz & 1u) << 2) | ((lx & 2u) << 2) |
                        ((ly & 2u) << 3) | ((lz & 2u) << 4);

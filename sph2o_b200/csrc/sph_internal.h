@@ -80,15 +80,17 @@ enum ForceMode : int {
     FORCE_PRESSURE = 3     /* pressure acceleration only -> acc (phase access) */
 };
 
-void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool eos, cudaStream_t s);
-void launch_normals(const SimParams& P, const DeviceArrays& A, cudaStream_t s);
-void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, cudaStream_t s);
-int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s);
+/* block: threads per block of the pass kernels (128 or 256, autotuned) */
+void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool eos, int block, cudaStream_t s);
+void launch_normals(const SimParams& P, const DeviceArrays& A, int block, cudaStream_t s);
+void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, int block, cudaStream_t s);
+/* occ: blocks per SM of the persistent DFSPH solver variant (4 or 8) */
+int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, int occ, cudaStream_t s);
 int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s);
 int launch_dfsph_solve_batch(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s);
 int launch_barrier_timeout_probe(DevState* st, cudaStream_t s);
 /* co-resident grid size of the persistent solver kernels (0 on error) */
-int persistent_grid(bool pcisph, bool divergence, bool batch = false);
+int persistent_grid(bool pcisph, bool divergence, bool batch = false, int occ = 8);
 constexpr int kSolverBlock = 256;
 
 } // namespace sph

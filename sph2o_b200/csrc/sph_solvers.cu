@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(256, 8) k_normals(SimParams P, DeviceArrays A)
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(128, 12) k_forces(SimParams P, DeviceArrays A)
+__global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
 {
     __shared__ float s_red[32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -334,10 +334,12 @@ __device__ __forceinline__ void dfsph_correct(const SimParams& P, const DeviceAr
     A.vel[i] = v;
 }
 
-/* 8 blocks of 256 per SM (32 registers): the passes are bound by the latency
-   of dependent neighbour gathers, and full occupancy hides most of it */
-template <bool DIV>
-__global__ void __launch_bounds__(kSolverBlock, 8) k_dfsph_solve(SimParams P, DeviceArrays A)
+/* OCC blocks of 256 per SM: 8 (32 registers) by default -- the passes are
+   bound by the latency of dependent neighbour gathers and full occupancy
+   hides most of it; 4 (64 registers, no spills) is the autotuner's other
+   candidate */
+template <bool DIV, int OCC>
+__global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, DeviceArrays A)
 {
     __shared__ double s_red[32];
     DevState* st = A.st;
@@ -780,34 +782,34 @@ int launch_barrier_timeout_probe(DevState* st, cudaStream_t s)
 
 static inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
-void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool eos, cudaStream_t s)
+void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool eos, int block, cudaStream_t s)
 {
     if (P.nf <= 0) return;
-    const int g = blocks_for(P.nf, 256);
-    if (alpha && eos) k_density<true, true><<<g, 256, 0, s>>>(P, A);
-    else if (alpha) k_density<true, false><<<g, 256, 0, s>>>(P, A);
-    else if (eos) k_density<false, true><<<g, 256, 0, s>>>(P, A);
-    else k_density<false, false><<<g, 256, 0, s>>>(P, A);
+    const int g = blocks_for(P.nf, block);
+    if (alpha && eos) k_density<true, true><<<g, block, 0, s>>>(P, A);
+    else if (alpha) k_density<true, false><<<g, block, 0, s>>>(P, A);
+    else if (eos) k_density<false, true><<<g, block, 0, s>>>(P, A);
+    else k_density<false, false><<<g, block, 0, s>>>(P, A);
 }
 
-void launch_normals(const SimParams& P, const DeviceArrays& A, cudaStream_t s)
+void launch_normals(const SimParams& P, const DeviceArrays& A, int block, cudaStream_t s)
 {
     if (P.nf <= 0) return;
-    k_normals<<<blocks_for(P.nf, 256), 256, 0, s>>>(P, A);
+    k_normals<<<blocks_for(P.nf, block), block, 0, s>>>(P, A);
 }
 
-void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, cudaStream_t s)
+void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, int block, cudaStream_t s)
 {
-    const int g = P.nf > 0 ? blocks_for(P.nf, 128) : 1;
+    const int g = P.nf > 0 ? blocks_for(P.nf, block) : 1;
     switch (mode) {
-    case FORCE_NP: k_forces<FORCE_NP><<<g, 128, 0, s>>>(P, A); break;
-    case FORCE_NP_CFL: k_forces<FORCE_NP_CFL><<<g, 128, 0, s>>>(P, A); break;
-    case FORCE_WCSPH: k_forces<FORCE_WCSPH><<<g, 128, 0, s>>>(P, A); break;
-    default: k_forces<FORCE_PRESSURE><<<g, 128, 0, s>>>(P, A); break;
+    case FORCE_NP: k_forces<FORCE_NP><<<g, block, 0, s>>>(P, A); break;
+    case FORCE_NP_CFL: k_forces<FORCE_NP_CFL><<<g, block, 0, s>>>(P, A); break;
+    case FORCE_WCSPH: k_forces<FORCE_WCSPH><<<g, block, 0, s>>>(P, A); break;
+    default: k_forces<FORCE_PRESSURE><<<g, block, 0, s>>>(P, A); break;
     }
 }
 
-int persistent_grid(bool pcisph, bool divergence, bool batch)
+int persistent_grid(bool pcisph, bool divergence, bool batch, int occ)
 {
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
@@ -815,7 +817,8 @@ int persistent_grid(bool pcisph, bool divergence, bool batch)
     const void* fn = pcisph ? (const void*)k_pcisph_solve
                      : batch ? (divergence ? (const void*)k_dfsph_solve_batch<true>
                                            : (const void*)k_dfsph_solve_batch<false>)
-                             : (divergence ? (const void*)k_dfsph_solve<true> : (const void*)k_dfsph_solve<false>);
+                             : occ == 4 ? (divergence ? (const void*)k_dfsph_solve<true, 4> : (const void*)k_dfsph_solve<false, 4>)
+                                        : (divergence ? (const void*)k_dfsph_solve<true, 8> : (const void*)k_dfsph_solve<false, 8>);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolverBlock, 0) != cudaSuccess) return 0;
     return per_sm * sms;
 }
@@ -828,12 +831,13 @@ static int coop_launch(const void* fn, const SimParams& P, const DeviceArrays& A
     return (int)cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kSolverBlock), args, 0, s);
 }
 
-int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s)
+int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, int occ, cudaStream_t s)
 {
     const int need = blocks_for(P.nf > 0 ? P.nf : 1, kSolverBlock);
     const int g = grid < need ? grid : need;
-    return coop_launch(divergence ? (const void*)k_dfsph_solve<true> : (const void*)k_dfsph_solve<false>, P, A,
-                       g > 0 ? g : 1, s);
+    const void* fn = occ == 4 ? (divergence ? (const void*)k_dfsph_solve<true, 4> : (const void*)k_dfsph_solve<false, 4>)
+                              : (divergence ? (const void*)k_dfsph_solve<true, 8> : (const void*)k_dfsph_solve<false, 8>);
+    return coop_launch(fn, P, A, g > 0 ? g : 1, s);
 }
 
 int launch_dfsph_solve_batch(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s)
