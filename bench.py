@@ -9,8 +9,12 @@ sphere obstacle R = 0.2 m), seeded synthetic lattice. One "step" is one
 DFSPH time step of the whole scene. `value` is fluid particle-steps/s with
 the state resident in HBM, timed with CUDA events recorded by the library on
 the stream its kernels run on; `e2e` is the same metric through the public C
-ABI with host buffers (state uploaded from pinned host memory at the start,
-stats read back every step, state read back at the end).
+ABI with host buffers over the same window (the state entering it uploaded
+from pinned host memory, statistics read back by every step, the final
+state read back). The line also carries, under "secondary", the
+differentiable WCSPH workload (32,768 particles, 500 steps, forward +
+backward) and the 256-scene batches (WCSPH and DFSPH) against the plain
+per-scene GPU loop.
 
 With N > 1 (torchrun) every rank runs an independent replica of the scene
 (the single-scene path does not shard): weak scaling, value = all ranks'
@@ -23,6 +27,7 @@ the same scene; under torchrun only rank 0 runs it.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import shutil
@@ -115,6 +120,48 @@ def batched_run(steps, warmup, method=0, count=256, loop_steps=None):
             "value_wall": batched_wall, "per_scene_loop": loop, "speedup_vs_loop": batched_wall / loop,
             "ms_per_step": dev_ms / steps, "mean_iterations": st["total_iterations"] / max(1, steps) / count,
             "method": "WCSPH" if method == 0 else "DFSPH"}
+
+
+def adjoint_run(steps=500, every=50, repeats=3):
+    """Differentiable WCSPH workload: 32,768 particles, 500 steps, checkpoint
+    every 50; one forward + backward pair per repeat from the same initial
+    state, device time from the library's events. Rate = particles x steps
+    / (forward + backward) time."""
+    import numpy as np
+
+    from sph2o_b200 import scenes as S
+    from sph2o_b200.api import Scene, Simulation
+
+    sc = Scene.from_dict(S.adjoint_wcsph_32k())
+    x0, _ = sc.fluid()
+    v0, t = S.adjoint_problem(x0)
+    sim = Simulation(sc.desc(), x0, sc.boundary(), vel=v0)
+    t_0, dt_0 = sim.time()
+    nf = sim.nf
+    best = None
+    for r in range(repeats + 1):
+        sim.set_state(x0, v0)
+        sim.set_time(t_0, dt_0)
+        loss = sim.wcsph_forward(steps, t, ckpt_every=every)
+        g = sim.wcsph_backward()
+        f_ms, b_ms = sim.wcsph_timing()
+        if r > 0 and (best is None or f_ms + b_ms < best[0] + best[1]):  # r == 0 warms up (graph capture)
+            best = (f_ms, b_ms, loss, g)
+    sim.close()
+    sc.close()
+    f_ms, b_ms, loss, g = best
+    algo = 480.0 * nf * steps  # forward 120 B + backward ~3 x forward per particle-step
+    peak, kind = hbm_peak()
+    return {"workload": "differentiable WCSPH, 32,768 fluid particles (32^3, r=0.02), 500 steps at dt=2e-4, "
+                        "checkpoint every 50, gradient w.r.t. v0 (32,768 x 3), viscosity and stiffness",
+            "value": nf * steps / ((f_ms + b_ms) / 1e3), "unit": "particle-steps/s (forward + backward)",
+            "forward_ms": f_ms, "backward_ms": b_ms, "forward_rate": nf * steps / (f_ms / 1e3),
+            "loss": loss, "grad_v0_norm": float(np.linalg.norm(g["v0"].astype(np.float64))),
+            "dL_dviscosity": g["viscosity"], "dL_dstiffness": g["stiffness"],
+            "roofline": {"bound": "hbm", "algorithmic_bytes_per_particle_step": 480,
+                         "achieved": algo / ((f_ms + b_ms) / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": algo / ((f_ms + b_ms) / 1e3) / 1e9 / peak, "peak_kind": f"of {kind}"},
+            "timing": f"best of {repeats} pairs after one warm-up pair, CUDA events on the library stream"}
 
 
 def hbm_peak():
@@ -267,6 +314,8 @@ def main():
     ap.add_argument("--batch-only", action="store_true", help="time only the batched-scenes workload")
     ap.add_argument("--batch-method", type=int, default=0)
     ap.add_argument("--batch-scenes", type=int, default=256)
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the adjoint and batched-scenes measurements added to the JSON line")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     name = args.workload
@@ -297,7 +346,17 @@ def main():
     scene = Scene.from_dict(scene_dict)
     sim = Simulation.from_scene(scene)
     nf, nb = sim.nf, sim.nb
-    warm_stats = sim.step(args.warmup) if args.warmup > 0 else None
+    if args.warmup > 0:
+        sim.step(args.warmup)
+    # the state entering the timed window, kept in pinned host memory so the
+    # end-to-end run below replays the same window through the public API
+    px = torch.empty((nf, 3), dtype=torch.float32, pin_memory=True).numpy()
+    pv = torch.empty((nf, 3), dtype=torch.float32, pin_memory=True).numpy()
+    pr = torch.empty(nf, dtype=torch.float32, pin_memory=True).numpy()
+    x_w, v_w, _ = sim.state()
+    px[:] = x_w
+    pv[:] = v_w
+    t_w, dt_w = sim.time()
 
     gpu_uuid = torch.cuda.get_device_properties(local).uuid
     sampler = ClockSampler(f"GPU-{gpu_uuid}" if gpu_uuid else local)
@@ -339,32 +398,39 @@ def main():
                 "traffic": None, "kernel": dom, "peak_kind": f"of {peak_kind}",
                 "algorithmic_bytes_per_launch": algo, "avg_launch_ms": avg_ms}
 
-    # end to end through the C ABI with host buffers
-    e2e = None
-    ke = min(args.steps, 50)
-    x, v, _ = sim.state()
-    px = torch.empty((nf, 3), dtype=torch.float32, pin_memory=True).numpy()
-    pv = torch.empty((nf, 3), dtype=torch.float32, pin_memory=True).numpy()
-    pr = torch.empty(nf, dtype=torch.float32, pin_memory=True).numpy()
-    px[:] = x
-    pv[:] = v
+    # End to end through the C ABI with host buffers, over the same window:
+    # the state entering it is uploaded from pinned host memory, every step
+    # is one sph_step call that returns its statistics (density error,
+    # iterations) to the host, and the final state is read back.
+    from sph2o_b200.api import StepStats, _fptr, lib
+    L = lib()
+    ke = args.steps
     if world > 1:
         dist.barrier()
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    sim.set_state(px, pv)
+    rc = L.sph_set_state(sim._h, _fptr(px), _fptr(pv))
+    rc = rc or L.sph_set_time(sim._h, t_w, dt_w)
+    e2e_its = 0
+    st1 = StepStats()
     for _ in range(ke):
-        sim.step(1)
-    from sph2o_b200.api import _fptr, lib
-    rc = lib().sph_get_state(sim._h, _fptr(px), _fptr(pv), _fptr(pr))
+        if rc:
+            break
+        rc = L.sph_step(sim._h, 1, st1)
+        e2e_its += st1.total_iterations
+    rc = rc or L.sph_get_state(sim._h, _fptr(px), _fptr(pv), _fptr(pr))
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e = None
     if rc == 0:
         e2e = {"value": world * nf * ke / float(te.item()), "unit": UNIT,
                "h2d_bytes_per_step": (nf * 24) // ke,
-               "d2h_bytes_per_step": 112 + (nf * 28) // ke,
-               "steps": ke}
+               "d2h_bytes_per_step": ctypes.sizeof(StepStats) + (nf * 28) // ke,
+               "steps": ke, "mean_iterations": e2e_its / ke,
+               "note": "state uploaded once from pinned host memory, per-step statistics read back by every "
+                       "sph_step call, final state (x, v, rho) read back; same window as value"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -376,6 +442,12 @@ def main():
                              f" + {res['mean_iterations_v']:.2f}"}
         else:
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference", "sample": err}
+
+    secondary = None
+    if not args.no_secondary:
+        secondary = {"adjoint_wcsph_32k": adjoint_run()}
+        for m, name in ((0, "batched_wcsph_256"), (2, "batched_dfsph_256")):
+            secondary[name] = batched_run(50, 3, method=m, count=args.batch_scenes)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -395,6 +467,7 @@ def main():
         "gpu_launches": stats["kernel_launches"],
         "clocks": clocks,
         "phases_ms_per_step": {k: prof[k]["ms"] / args.steps for k in prof if prof[k]["launches"]},
+        "secondary": secondary,
     }
     if rank == 0:
         print(json.dumps(line))

@@ -157,7 +157,8 @@ int sph_profile_read(sph_ctx* ctx, double* ms, unsigned long long* launches);
 
 /* ---- launch options and autotuning (no reference counterpart) -------- */
 enum sph_option {
-    SPH_OPT_CUDA_GRAPHS = 0,      /* 1 (default): steps taken in pairs replay a captured CUDA graph */
+    SPH_OPT_CUDA_GRAPHS = 0,      /* 1 (default): steps replay captured CUDA graphs of two steps (one
+                                     for an odd remainder), keyed by the buffer assignment */
     SPH_OPT_CELL_ORDER = 1,       /* 0 (default): 4x4x4 cell bricks, Morton inside; 1: linear, x fastest */
     SPH_OPT_SOLVER_OCCUPANCY = 2, /* DFSPH persistent solver blocks per SM: 8 (default) or 4 */
     SPH_OPT_PASS_BLOCK = 3        /* threads per block of the particle-pass kernels: 256 (default) or 128 */
@@ -223,6 +224,39 @@ unsigned sph_batch_num_scenes(const sph_ctx* ctx);
 int sph_batch_scene_range(const sph_ctx* ctx, unsigned scene, unsigned* begin, unsigned* end);
 /* Per-scene time, dt, iterations and residuals (cumulative iteration totals). */
 int sph_batch_scene_stats(sph_ctx* ctx, unsigned scene, sph_step_stats* out);
+
+/* ---- differentiable WCSPH (no reference counterpart) -------------------
+   SPH2O has no adjoint; these entry points differentiate its WCSPH step
+   (WCSPHSolver::step, WCSPHSolver.cpp:14-78: densities, Tait EOS, pressure
+   force, artificial viscosity, symplectic Euler; Akinci boundaries) with the
+   neighbour lists of each step held fixed. Loss:
+       L = (1/N) sum_i |x_i(T) - target_i|^2
+   over the N fluid particles after nsteps steps. Single-scene WCSPH
+   contexts with artificial viscosity (or none) and neither surface tension
+   nor adhesion; anything else returns SPH_ERR_ARG. */
+
+/* Steps the context nsteps WCSPH steps from its current state (which
+   becomes x(0), v(0)), keeping a checkpoint of the state entering every
+   ckpt_every-th step, and returns the loss against `target` (n*3 floats,
+   caller order). The context is left in the final state, as sph_step
+   leaves it. Device memory: (nsteps / ckpt_every + ckpt_every) states of
+   36 bytes per particle. */
+int sph_wcsph_forward(sph_ctx* ctx, int nsteps, int ckpt_every, const float* target, double* loss);
+
+/* Gradients of the last sph_wcsph_forward's loss with respect to the
+   initial velocities (dL_dv0: n*3 floats, caller order), the artificial
+   viscosity coefficient and the EOS stiffness (any pointer may be NULL).
+   Segments are recomputed from their checkpoints (bit-identical to the
+   forward run); the context is returned to the state the forward run left. */
+int sph_wcsph_backward(sph_ctx* ctx, float* dL_dv0, float* dL_dvisc, float* dL_dk);
+
+/* Gradient with respect to the initial positions from the last
+   sph_wcsph_backward (n*3 floats, caller order). */
+int sph_wcsph_grad_x0(sph_ctx* ctx, float* dL_dx0);
+
+/* Device milliseconds of the last sph_wcsph_forward / sph_wcsph_backward
+   (CUDA events on the context stream). */
+int sph_wcsph_timing(const sph_ctx* ctx, double* forward_ms, double* backward_ms);
 
 /* ---- phase access for parity checks ------------------------------------- */
 

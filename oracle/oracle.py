@@ -30,6 +30,8 @@ def lib():
         L.sph_oracle_neighbors.argtypes = [P, U, U, C.c_size_t, U, U, C.c_size_t, C.POINTER(C.c_size_t),
                                            C.POINTER(C.c_size_t)]
         L.sph_oracle_destroy.argtypes = [P]
+        L.sph_oracle_wcsph_adjoint.argtypes = [P, C.c_double, C.c_double, C.c_uint, D, D, C.c_uint, D, C.c_int, D,
+                                               D, D, D, D, D, D]
         _lib = L
     return _lib
 
@@ -104,3 +106,31 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+
+def wcsph_adjoint(desc, x0, v0, boundary, nsteps, target, nu=None, k=None, grad=True):
+    """FP64 WCSPH run + adjoint (oracle/wcsph_adjoint.cpp). nu / k default to
+    the description's viscosity / stiffness. Returns a dict with the loss,
+    the final positions and, when grad, dL/dx0, dL/dv0, dL/dnu, dL/dk."""
+    L = lib()
+    x0 = np.ascontiguousarray(x0, np.float64).reshape(-1, 3)
+    v0 = np.ascontiguousarray(v0, np.float64).reshape(-1, 3)
+    b = np.ascontiguousarray(boundary, np.float64).reshape(-1, 3)
+    t = np.ascontiguousarray(target, np.float64).reshape(-1, 3)
+    n = x0.shape[0]
+    loss = C.c_double()
+    xo = np.zeros((n, 3))
+    gx = np.zeros((n, 3)) if grad else None
+    gv = np.zeros((n, 3)) if grad else None
+    gnu, gk = C.c_double(), C.c_double()
+    nu = float(desc.viscosity) if nu is None else float(nu)
+    k = float(desc.stiffness) if k is None else float(k)
+    rc = L.sph_oracle_wcsph_adjoint(C.addressof(desc), nu, k, n, _d(x0), _d(v0), b.shape[0], _d(b), int(nsteps),
+                                    _d(t), C.byref(loss), _d(xo), _d(gx) if grad else None,
+                                    _d(gv) if grad else None, C.byref(gnu), C.byref(gk))
+    if rc != 0:
+        raise RuntimeError(f"sph_oracle_wcsph_adjoint failed: {rc}")
+    out = {"loss": loss.value, "x": xo}
+    if grad:
+        out.update(x0=gx, v0=gv, viscosity=gnu.value, stiffness=gk.value)
+    return out

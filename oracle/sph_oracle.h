@@ -38,6 +38,13 @@ int sph_oracle_neighbors(sph_oracle* o, unsigned* f_off, unsigned* f_idx, size_t
                          unsigned* b_idx, size_t b_cap, size_t* nf_total, size_t* nb_total);
 void sph_oracle_destroy(sph_oracle* o);
 
+/* wcsph_adjoint.cpp: FP64 WCSPH run from (x0, v0) for nsteps steps with
+   viscosity nu and stiffness k, loss (1/N) sum |x_i(T) - target_i|^2, and
+   (when dv0 is not NULL) its gradients dL/dx0, dL/dv0, dL/dnu, dL/dk. */
+int sph_oracle_wcsph_adjoint(const sph_scene_desc* d, double nu, double k, unsigned nf, const double* x0,
+                             const double* v0, unsigned nb, const double* bxyz, int nsteps, const double* target,
+                             double* loss, double* x_out, double* dx0, double* dv0, double* dnu, double* dk);
+
 #ifdef __cplusplus
 }
 #endif

@@ -124,6 +124,10 @@ def lib():
         "sph_scene_error": (C.c_char_p, []),
         "sph_scene_free": (None, [P]),
         "sph_create_from_scene": (I, [P, C.POINTER(P)]),
+        "sph_wcsph_forward": (I, [P, I, I, F, C.POINTER(C.c_double)]),
+        "sph_wcsph_backward": (I, [P, F, F, F]),
+        "sph_wcsph_grad_x0": (I, [P, F]),
+        "sph_wcsph_timing": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
@@ -294,6 +298,33 @@ class Simulation:
         n = (C.c_ulonglong * PROF_COUNT)()
         self._check(lib().sph_profile_read(self._h, ms, n))
         return {PROF_NAMES[i]: {"ms": ms[i], "launches": n[i]} for i in range(PROF_COUNT)}
+
+    def wcsph_forward(self, nsteps, target, ckpt_every=50):
+        """Differentiable WCSPH run from the current state; returns the loss
+        (1/N) sum |x_i(T) - target_i|^2."""
+        t = np.ascontiguousarray(target, np.float32).reshape(-1, 3)
+        loss = C.c_double()
+        self._check(lib().sph_wcsph_forward(self._h, int(nsteps), int(ckpt_every), _fptr(t), C.byref(loss)))
+        return loss.value
+
+    def wcsph_backward(self, want_x0=False):
+        """Gradients of the last wcsph_forward's loss: dL/dv0 (n x 3), dL/dviscosity,
+        dL/dstiffness (and dL/dx0 when want_x0)."""
+        gv = np.zeros((self.nf, 3), np.float32)
+        dvisc = C.c_float()
+        dk = C.c_float()
+        self._check(lib().sph_wcsph_backward(self._h, _fptr(gv), C.byref(dvisc), C.byref(dk)))
+        out = {"v0": gv, "viscosity": dvisc.value, "stiffness": dk.value}
+        if want_x0:
+            gx = np.zeros((self.nf, 3), np.float32)
+            self._check(lib().sph_wcsph_grad_x0(self._h, _fptr(gx)))
+            out["x0"] = gx
+        return out
+
+    def wcsph_timing(self):
+        f, b = C.c_double(), C.c_double()
+        self._check(lib().sph_wcsph_timing(self._h, C.byref(f), C.byref(b)))
+        return f.value, b.value
 
     def neighbors(self):
         """CSR neighbour sets (caller order): (f_off, f_idx, b_off, b_idx)."""

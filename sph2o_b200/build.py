@@ -21,7 +21,8 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libsph2o_cuda.so")
 DRIVER = os.path.join(HERE, "bin", "sph2o")
 
-CUDA_SOURCES = ["csrc/sph_grid.cu", "csrc/sph_solvers.cu", "csrc/sph_capi.cu", "csrc/sph_noalloc.cu"]
+CUDA_SOURCES = ["csrc/sph_grid.cu", "csrc/sph_solvers.cu", "csrc/sph_capi.cu", "csrc/sph_noalloc.cu",
+                "csrc/sph_adjoint.cu"]
 HOST_SOURCES = ["host/scene.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

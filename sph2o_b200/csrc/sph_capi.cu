@@ -35,9 +35,12 @@ namespace {
 
 thread_local std::string g_global_error;
 
-struct DeviceBuffer {
-    void* p = nullptr;
-    size_t bytes = 0;
+/* The host-side buffer assignment (which of each swapped pair is current). */
+struct Buffers {
+    float4 *pos, *pos2, *vel, *vel2;
+    unsigned *orig, *orig2;
+    float *kws, *kws2, *kvws, *kvws2;
+    bool lists_valid;
 };
 
 } // namespace
@@ -109,11 +112,33 @@ struct sph_ctx {
     float *snap_kws = nullptr, *snap_kvws = nullptr, *snap_rho = nullptr;
     SceneState* snap_sst = nullptr;
     DevState* snap_st = nullptr;
-    struct Graph { unsigned key; cudaGraphExec_t exec; unsigned long long launches; };
+    struct Graph { unsigned key; cudaGraphExec_t exec; unsigned long long launches; Buffers end; };
     std::vector<Graph> graphs;
     float4* pos_base = nullptr;
     unsigned* orig_base = nullptr;
     float* kws_base = nullptr;
+    /* WCSPH adjoint (sph_wcsph_forward / sph_wcsph_backward) */
+    struct Adjoint {
+        int nsteps = 0, every = 0, nseg = 0;
+        int cap_seg = 0, cap_every = 0;
+        float4 *ck_pos = nullptr, *ck_vel = nullptr;   /* checkpoints: state entering each segment */
+        unsigned* ck_orig = nullptr;
+        float4 *sl_pos = nullptr, *sl_vel = nullptr;   /* state entering each step of one segment */
+        unsigned* sl_orig = nullptr;
+        float4 *fin_pos = nullptr, *fin_vel = nullptr; /* state after the forward run */
+        unsigned* fin_orig = nullptr;
+        DevState *st0 = nullptr, *st1 = nullptr;       /* solver state at the start / end of the run */
+        float* target = nullptr;
+        float4 *xbar = nullptr, *vbar = nullptr, *abar = nullptr, *xacc = nullptr, *vacc = nullptr;
+        float *Ap = nullptr, *rhobar = nullptr;
+        double *part = nullptr, *red = nullptr;  /* per-block partial sums, their totals */
+        bool ready = false, have_grad = false;
+        cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+        double fwd_ms = 0.0, bwd_ms = 0.0;
+        struct Graph { int len; cudaGraphExec_t exec; unsigned long long launches; Buffers end; };
+        std::vector<Graph> graphs;
+        bool use_graphs = true;
+    } adj;
 };
 
 namespace {
@@ -488,6 +513,8 @@ void drop_graphs(sph_ctx* c)
 {
     for (auto& g : c->graphs) cudaGraphExecDestroy(g.exec);
     c->graphs.clear();
+    for (auto& g : c->adj.graphs) cudaGraphExecDestroy(g.exec);
+    c->adj.graphs.clear();
 }
 
 int eager_step(sph_ctx* c)
@@ -499,16 +526,30 @@ int eager_step(sph_ctx* c)
     }
 }
 
-/* Two steps as one CUDA graph: captured on first use for the current buffer
-   assignment, replayed afterwards. Returns false when capture is not
-   possible (the caller then steps eagerly and stops trying). */
-bool graph_two_steps(sph_ctx* c, int* rc)
+Buffers get_buffers(const sph_ctx* c)
 {
-    const unsigned key = buffer_key(c);
+    return {c->pos, c->pos2, c->vel, c->vel2, c->orig, c->orig2, c->kws, c->kws2, c->kvws, c->kvws2, c->lists_valid};
+}
+
+void set_buffers(sph_ctx* c, const Buffers& b)
+{
+    c->pos = b.pos; c->pos2 = b.pos2; c->vel = b.vel; c->vel2 = b.vel2; c->orig = b.orig; c->orig2 = b.orig2;
+    c->kws = b.kws; c->kws2 = b.kws2; c->kvws = b.kvws; c->kvws2 = b.kvws2; c->lists_valid = b.lists_valid;
+}
+
+/* nsteps (1 or 2) steps as one CUDA graph, captured on first use for the
+   current buffer assignment (which the key determines) and replayed
+   afterwards; a replay leaves the host-side assignment where the captured
+   steps left it. Returns false when capture is not possible (the caller
+   then steps eagerly and stops trying). */
+bool graph_steps(sph_ctx* c, int nsteps, int* rc)
+{
+    const unsigned key = buffer_key(c) | ((unsigned)nsteps << 8);
     for (auto& g : c->graphs)
         if (g.key == key) {
             const cudaError_t e = cudaGraphLaunch(g.exec, c->stream);
             if (e != cudaSuccess) { *rc = fail(c, SPH_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); return true; }
+            set_buffers(c, g.end);
             c->launches += g.launches;
             *rc = SPH_OK;
             return true;
@@ -517,44 +558,52 @@ bool graph_two_steps(sph_ctx* c, int* rc)
         cudaGetLastError();
         return false;
     }
-    /* host-side buffer assignment before capture, restored if capture fails
-       (captured work never ran, so swaps made while capturing must be undone) */
-    float4 *p0 = c->pos, *p1 = c->pos2, *v0 = c->vel, *v1 = c->vel2;
-    unsigned *o0 = c->orig, *o1 = c->orig2;
-    float *k0 = c->kws, *k1 = c->kws2, *q0 = c->kvws, *q1 = c->kvws2;
-    const bool lv = c->lists_valid;
-    auto restore = [&]() {
-        c->pos = p0; c->pos2 = p1; c->vel = v0; c->vel2 = v1; c->orig = o0; c->orig2 = o1;
-        c->kws = k0; c->kws2 = k1; c->kvws = q0; c->kvws2 = q1; c->lists_valid = lv;
-    };
+    /* captured work never runs during capture: the swaps it makes on the host
+       are undone afterwards and applied by the replay */
+    const Buffers start = get_buffers(c);
     const unsigned long long l0 = c->launches;
-    int r = eager_step(c);
-    if (r == SPH_OK) r = eager_step(c);
+    int r = SPH_OK;
+    for (int n = 0; n < nsteps && r == SPH_OK; ++n) r = eager_step(c);
     cudaGraph_t graph = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
     const unsigned long long nl = c->launches - l0;
     c->launches = l0;
-    if (r != SPH_OK || ec != cudaSuccess || !graph || buffer_key(c) != key) {
-        if (graph) cudaGraphDestroy(graph);
+    const Buffers end = get_buffers(c);
+    set_buffers(c, start);
+    cudaGraphExec_t exec = nullptr;
+    const bool ok = r == SPH_OK && ec == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
         cudaGetLastError();
-        restore();
         c->err.clear();
         return false;
     }
-    cudaGraphExec_t exec = nullptr;
-    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ei != cudaSuccess) {
-        cudaGetLastError();
-        restore();
-        return false;
+    c->graphs.push_back({key, exec, nl, end});
+    return graph_steps(c, nsteps, rc);
+}
+
+/* Queue nsteps steps: pairs (and a remaining single step) replay captured
+   graphs; while profiling every step runs eagerly. */
+int run_steps(sph_ctx* c, int nsteps)
+{
+    int left = nsteps;
+    while (left > 0) {
+        int rc = SPH_OK;
+        if (c->use_graphs && !c->prof) {
+            const int n = left >= 2 ? 2 : 1;
+            if (graph_steps(c, n, &rc)) {
+                if (rc != SPH_OK) return rc;
+                left -= n;
+                continue;
+            }
+            c->use_graphs = false;  /* capture unsupported: stay eager */
+            drop_graphs(c);
+        }
+        rc = eager_step(c);
+        if (rc != SPH_OK) return rc;
+        --left;
     }
-    c->graphs.push_back({key, exec, nl});
-    const cudaError_t e = cudaGraphLaunch(exec, c->stream);
-    if (e != cudaSuccess) { *rc = fail(c, SPH_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); return true; }
-    c->launches += nl;
-    *rc = SPH_OK;
-    return true;
+    return SPH_OK;
 }
 
 } // namespace
@@ -848,22 +897,8 @@ int sph_step_async(sph_ctx* c, int nsteps)
         c->batch_open = true;
         c->launches_at_open = c->launches;
     }
-    int left = nsteps;
-    while (left > 0) {
-        int rc = SPH_OK;
-        if (left >= 2 && c->use_graphs && !c->prof) {
-            if (graph_two_steps(c, &rc)) {
-                if (rc != SPH_OK) return rc;
-                left -= 2;
-                continue;
-            }
-            c->use_graphs = false;  /* capture unsupported: stay eager */
-            drop_graphs(c);
-        }
-        rc = eager_step(c);
-        if (rc != SPH_OK) return rc;
-        --left;
-    }
+    const int rc = run_steps(c, nsteps);
+    if (rc != SPH_OK) return rc;
     CUDA_TRY(c, cudaEventRecord(c->ev_end, c->stream));
     return SPH_OK;
 }
@@ -1063,6 +1098,8 @@ int sph_destroy(sph_ctx* c)
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev_begin) cudaEventDestroy(c->ev_begin);
     if (c->ev_end) cudaEventDestroy(c->ev_end);
+    for (cudaEvent_t e : c->adj.ev)
+        if (e) cudaEventDestroy(e);
     free_all(c);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1508,6 +1545,298 @@ int sph_debug_neighbors(sph_ctx* c, unsigned* f_offsets, unsigned* f_index, size
     if (nf_total) *nf_total = tf;
     if (nb_total) *nb_total = tb;
     if ((f_index && tf > f_cap) || (b_index && tb > b_cap)) return fail(c, SPH_ERR_ARG, "index arrays too small");
+    return SPH_OK;
+}
+
+} // extern "C"
+
+/* ---- WCSPH adjoint ----------------------------------------------------
+   Forward: nsteps ordinary WCSPH steps from the current state, the state
+   entering every ckpt_every-th step kept as a checkpoint (positions,
+   velocities and the sorted-slot ids, 36 B per particle). Backward: per
+   segment, last first, the segment is recomputed from its checkpoint with
+   the state entering each step kept (the recomputation is bit-identical:
+   the sort ranks particles inside a cell by id and every pass is a
+   gather), then each step's neighbour search and densities are redone and
+   its adjoint kernels run, newest step first. Memory: (nsteps / K + K)
+   states of 36 B per particle for K = ckpt_every. */
+namespace {
+
+void dfree(sph_ctx* c, void* p)
+{
+    if (!p) return;
+    auto it = std::find(c->allocations.begin(), c->allocations.end(), p);
+    if (it != c->allocations.end()) {
+        cudaFree(p);
+        c->allocations.erase(it);
+    }
+}
+
+int adj_supported(sph_ctx* c)
+{
+    if (c->nscenes) return fail(c, SPH_ERR_ARG, "the WCSPH adjoint applies to a single scene, not to a batch");
+    if (c->desc.simulation_method != SPH_WCSPH) return fail(c, SPH_ERR_ARG, "the adjoint differentiates the WCSPH step only");
+    if (c->P.st_on || c->P.adh_on)
+        return fail(c, SPH_ERR_ARG, "the WCSPH adjoint covers neither surface tension nor adhesion");
+    if (c->P.visc_method != -1 && c->P.visc_method != SPH_VISCOSITY_ARTIFICIAL)
+        return fail(c, SPH_ERR_ARG, "the WCSPH adjoint covers artificial viscosity (or none) only");
+    return SPH_OK;
+}
+
+int adj_reserve(sph_ctx* c, int nseg, int every)
+{
+    auto& a = c->adj;
+    const size_t nf = c->nf;
+    int rc;
+#define AALLOC(ptr, count) if ((rc = dalloc(c, &a.ptr, (count))) != SPH_OK) return rc
+    if (!a.xbar) {
+        AALLOC(fin_pos, nf); AALLOC(fin_vel, nf); AALLOC(fin_orig, nf);
+        AALLOC(st0, 1); AALLOC(st1, 1); AALLOC(target, 3 * nf);
+        AALLOC(xbar, nf); AALLOC(vbar, nf); AALLOC(abar, nf); AALLOC(xacc, nf); AALLOC(vacc, nf);
+        AALLOC(Ap, nf); AALLOC(rhobar, nf); AALLOC(red, 4);
+        AALLOC(part, 3 * (size_t)adjoint_blocks((int)nf));
+        for (auto& e : a.ev) CUDA_TRY(c, cudaEventCreate(&e));
+    }
+    if (nseg > a.cap_seg) {
+        dfree(c, a.ck_pos); dfree(c, a.ck_vel); dfree(c, a.ck_orig);
+        a.ck_pos = a.ck_vel = nullptr; a.ck_orig = nullptr; a.cap_seg = 0;
+        AALLOC(ck_pos, (size_t)nseg * nf); AALLOC(ck_vel, (size_t)nseg * nf); AALLOC(ck_orig, (size_t)nseg * nf);
+        a.cap_seg = nseg;
+    }
+    if (every > a.cap_every) {
+        drop_graphs(c);
+        dfree(c, a.sl_pos); dfree(c, a.sl_vel); dfree(c, a.sl_orig);
+        a.sl_pos = a.sl_vel = nullptr; a.sl_orig = nullptr; a.cap_every = 0;
+        AALLOC(sl_pos, (size_t)every * nf); AALLOC(sl_vel, (size_t)every * nf); AALLOC(sl_orig, (size_t)every * nf);
+        a.cap_every = every;
+    }
+#undef AALLOC
+    return SPH_OK;
+}
+
+int copy_state(sph_ctx* c, float4* dp, float4* dv, unsigned* dorig, const float4* sp, const float4* sv,
+               const unsigned* sorig)
+{
+    const size_t nf = c->nf;
+    CUDA_TRY(c, cudaMemcpyAsync(dp, sp, nf * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(dv, sv, nf * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(dorig, sorig, nf * sizeof(unsigned), cudaMemcpyDeviceToDevice, c->stream));
+    return SPH_OK;
+}
+
+/* Name the first-allocated buffers "current" (contents are about to be
+   overwritten by a restore), so that a segment always starts from the same
+   buffer assignment and its captured graph can be replayed. */
+void canonical_buffers(sph_ctx* c)
+{
+    if (c->pos != c->pos_base) { std::swap(c->pos, c->pos2); std::swap(c->vel, c->vel2); }
+    if (c->orig != c->orig_base) std::swap(c->orig, c->orig2);
+}
+
+AdjointArrays adj_arrays(sph_ctx* c)
+{
+    auto& a = c->adj;
+    AdjointArrays J{};
+    J.pos = c->pos; J.vel = c->vel; J.rho = c->rho; J.press = c->press; J.orig = c->orig;
+    J.bpos = c->bpos; J.nbr_f = c->nbr_f; J.cnt_f = c->cnt_f; J.nbr_b = c->nbr_b; J.cnt_b = c->cnt_b;
+    J.st = c->st;
+    J.xbar = a.xbar; J.vbar = a.vbar; J.abar = a.abar; J.xacc = a.xacc; J.vacc = a.vacc;
+    J.Ap = a.Ap; J.rhobar = a.rhobar; J.part = a.part;
+    return J;
+}
+
+/* Recompute a segment of len steps from the state in the current buffers,
+   keeping each step's input, then run the adjoint of its steps, last first. */
+int adj_segment_body(sph_ctx* c, int len)
+{
+    auto& a = c->adj;
+    const size_t nf = c->nf;
+    int rc;
+    for (int n = 0; n < len; ++n) {
+        if ((rc = copy_state(c, a.sl_pos + n * nf, a.sl_vel + n * nf, a.sl_orig + n * nf, c->pos, c->vel, c->orig)) != SPH_OK)
+            return rc;
+        if ((rc = step_wcsph(c)) != SPH_OK) return rc;
+    }
+    for (int n = len - 1; n >= 0; --n) {
+        if ((rc = copy_state(c, c->pos, c->vel, c->orig, a.sl_pos + n * nf, a.sl_vel + n * nf, a.sl_orig + n * nf)) != SPH_OK)
+            return rc;
+        if ((rc = neighbor_search(c)) != SPH_OK) return rc;
+        { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, arrays(c), false, true, c->pass_block, c->stream); }
+        launch_adjoint_step(c->P, adj_arrays(c), c->stream);
+        c->launches += 3;
+    }
+    c->lists_valid = false;
+    return check_launch(c, "adjoint segment");
+}
+
+/* One segment, from a graph captured on the first segment of this length
+   (segments start from the canonical buffer assignment, so the captured
+   launch sequence is the same for every segment of that length). */
+int adj_segment(sph_ctx* c, int len)
+{
+    auto& a = c->adj;
+    if (a.use_graphs && !c->prof) {
+        for (auto& g : a.graphs)
+            if (g.len == len) {
+                const cudaError_t e = cudaGraphLaunch(g.exec, c->stream);
+                if (e != cudaSuccess) return fail(c, SPH_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+                set_buffers(c, g.end);
+                c->launches += g.launches;
+                return SPH_OK;
+            }
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const Buffers start = get_buffers(c);
+            const unsigned long long l0 = c->launches;
+            const int r = adj_segment_body(c, len);
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
+            const unsigned long long nl = c->launches - l0;
+            c->launches = l0;
+            cudaGraphExec_t exec = nullptr;
+            const bool ok = r == SPH_OK && ec == cudaSuccess && graph &&
+                            cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+            if (graph) cudaGraphDestroy(graph);
+            const Buffers end = get_buffers(c);
+            set_buffers(c, start);
+            if (ok) {
+                a.graphs.push_back({len, exec, nl, end});
+                return adj_segment(c, len);
+            }
+            cudaGetLastError();
+            c->err.clear();
+        } else {
+            cudaGetLastError();
+        }
+        a.use_graphs = false;  /* capture unsupported: stay eager */
+        drop_graphs(c);
+    }
+    return adj_segment_body(c, len);
+}
+
+} // namespace
+
+extern "C" {
+
+int sph_wcsph_forward(sph_ctx* c, int nsteps, int ckpt_every, const float* target, double* loss)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_wcsph_forward before sph_init");
+    if (nsteps <= 0 || ckpt_every <= 0) return fail(c, SPH_ERR_ARG, "nsteps and ckpt_every must be positive");
+    if (!target || !loss) return fail(c, SPH_ERR_ARG, "target and loss must not be NULL");
+    int rc = adj_supported(c);
+    if (rc != SPH_OK) return rc;
+    auto& a = c->adj;
+    a.ready = false;
+    a.have_grad = false;
+    const int every = std::min(ckpt_every, nsteps);
+    const int nseg = (nsteps + every - 1) / every;
+    if ((rc = adj_reserve(c, nseg, every)) != SPH_OK) return rc;
+    const size_t nf = c->nf;
+    CUDA_TRY(c, cudaMemcpyAsync(a.target, target, 3 * nf * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaEventRecord(a.ev[0], c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(a.st0, c->st, sizeof(DevState), cudaMemcpyDeviceToDevice, c->stream));
+    for (int s = 0; s < nseg; ++s) {
+        if ((rc = copy_state(c, a.ck_pos + s * nf, a.ck_vel + s * nf, a.ck_orig + s * nf, c->pos, c->vel, c->orig)) != SPH_OK)
+            return rc;
+        if ((rc = run_steps(c, std::min(every, nsteps - s * every))) != SPH_OK) return rc;
+    }
+    if ((rc = copy_state(c, a.fin_pos, a.fin_vel, a.fin_orig, c->pos, c->vel, c->orig)) != SPH_OK) return rc;
+    CUDA_TRY(c, cudaMemcpyAsync(a.st1, c->st, sizeof(DevState), cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(a.part, 0, 3 * (size_t)adjoint_blocks((int)nf) * sizeof(double), c->stream));
+    launch_adjoint_seed((int)nf, a.fin_pos, a.fin_orig, a.target, a.xbar, a.vbar, a.part, c->stream);
+    launch_adjoint_finish((int)nf, a.part, a.red, c->stream);
+    c->launches += 2;
+    CUDA_TRY(c, cudaEventRecord(a.ev[1], c->stream));
+    double red[4] = {0, 0, 0, 0};
+    CUDA_TRY(c, cudaMemcpyAsync(red, a.red, sizeof red, cudaMemcpyDeviceToHost, c->stream));
+    DevState now{};
+    if ((rc = read_state(c, &now)) != SPH_OK) return rc;
+    if ((rc = check_launch(c, "wcsph forward")) != SPH_OK) return rc;
+    float ms = 0.0f;
+    a.fwd_ms = cudaEventElapsedTime(&ms, a.ev[0], a.ev[1]) == cudaSuccess ? ms : 0.0;
+    c->last = now;
+    if ((rc = status_from_state(c, now)) != SPH_OK) {
+        if (rc == SPH_ERR_NEIGHBOR_OVERFLOW) {
+            const int r2 = recover_overflow(c);
+            if (r2 != SPH_OK) return r2;
+            c->err = "neighbour list capacity exceeded during the forward run; capacity grown, run it again";
+        }
+        return rc;
+    }
+    *loss = red[2] / (double)nf;
+    a.nsteps = nsteps;
+    a.every = every;
+    a.nseg = nseg;
+    a.ready = true;
+    return SPH_OK;
+}
+
+int sph_wcsph_backward(sph_ctx* c, float* dL_dv0, float* dL_dvisc, float* dL_dk)
+{
+    if (!c) return SPH_ERR_ARG;
+    auto& a = c->adj;
+    if (!c->initialized || !a.ready) return fail(c, SPH_ERR_STATE, "sph_wcsph_backward before sph_wcsph_forward");
+    int rc = adj_supported(c);
+    if (rc != SPH_OK) return rc;
+    const size_t nf = c->nf;
+    CUDA_TRY(c, cudaEventRecord(a.ev[2], c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(a.part, 0, 3 * (size_t)adjoint_blocks((int)nf) * sizeof(double), c->stream));
+    launch_adjoint_seed((int)nf, a.fin_pos, a.fin_orig, a.target, a.xbar, a.vbar, a.part, c->stream);
+    c->launches += 1;
+    CUDA_TRY(c, cudaMemcpyAsync(c->st, a.st0, sizeof(DevState), cudaMemcpyDeviceToDevice, c->stream));
+    for (int s = a.nseg - 1; s >= 0; --s) {
+        canonical_buffers(c);
+        if ((rc = copy_state(c, c->pos, c->vel, c->orig, a.ck_pos + s * nf, a.ck_vel + s * nf, a.ck_orig + s * nf)) != SPH_OK)
+            return rc;
+        if ((rc = adj_segment(c, std::min(a.every, a.nsteps - s * a.every))) != SPH_OK) return rc;
+    }
+    launch_adjoint_finish((int)nf, a.part, a.red, c->stream);
+    c->launches += 1;
+    CUDA_TRY(c, cudaEventRecord(a.ev[3], c->stream));
+    if (dL_dv0) {
+        float* tmp = reinterpret_cast<float*>(a.xacc); /* 4 nf floats of scratch */
+        launch_adjoint_unpack((int)nf, a.vbar, tmp, c->stream);
+        CUDA_TRY(c, cudaMemcpyAsync(dL_dv0, tmp, 3 * nf * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    }
+    double red[4] = {0, 0, 0, 0};
+    CUDA_TRY(c, cudaMemcpyAsync(red, a.red, sizeof red, cudaMemcpyDeviceToHost, c->stream));
+    DevState seen{};
+    if ((rc = read_state(c, &seen)) != SPH_OK) return rc;
+    if ((rc = check_launch(c, "wcsph backward")) != SPH_OK) return rc;
+    float ms = 0.0f;
+    a.bwd_ms = cudaEventElapsedTime(&ms, a.ev[2], a.ev[3]) == cudaSuccess ? ms : 0.0;
+    /* back to the state the forward run ended in */
+    canonical_buffers(c);
+    if ((rc = copy_state(c, c->pos, c->vel, c->orig, a.fin_pos, a.fin_vel, a.fin_orig)) != SPH_OK) return rc;
+    CUDA_TRY(c, cudaMemcpyAsync(c->st, a.st1, sizeof(DevState), cudaMemcpyDeviceToDevice, c->stream));
+    c->lists_valid = false;
+    DevState now{};
+    if ((rc = read_state(c, &now)) != SPH_OK) return rc;
+    c->last = now;
+    if ((rc = status_from_state(c, seen)) != SPH_OK) return rc;
+    if (dL_dvisc) *dL_dvisc = (float)red[1];
+    if (dL_dk) *dL_dk = (float)red[0];
+    a.have_grad = true;
+    return SPH_OK;
+}
+
+int sph_wcsph_grad_x0(sph_ctx* c, float* dL_dx0)
+{
+    if (!c || !dL_dx0) return SPH_ERR_ARG;
+    auto& a = c->adj;
+    if (!a.have_grad) return fail(c, SPH_ERR_STATE, "sph_wcsph_grad_x0 before sph_wcsph_backward");
+    float* tmp = reinterpret_cast<float*>(a.xacc);
+    launch_adjoint_unpack((int)c->nf, a.xbar, tmp, c->stream);
+    CUDA_TRY(c, cudaMemcpyAsync(dL_dx0, tmp, 3 * (size_t)c->nf * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_launch(c, "grad_x0");
+}
+
+int sph_wcsph_timing(const sph_ctx* c, double* forward_ms, double* backward_ms)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (forward_ms) *forward_ms = c->adj.fwd_ms;
+    if (backward_ms) *backward_ms = c->adj.bwd_ms;
     return SPH_OK;
 }
 

@@ -1,7 +1,8 @@
 /*
  * Host-side declarations of the kernel launchers (one CUDA stream each).
- * Kernels live in sph_grid.cu (neighbour search, sort, boundary volumes) and
- * sph_solvers.cu (density, forces, WCSPH / PCISPH / DFSPH steps).
+ * Kernels live in sph_grid.cu (neighbour search, sort, boundary volumes),
+ * sph_solvers.cu (density, forces, WCSPH / PCISPH / DFSPH steps) and
+ * sph_adjoint.cu (reverse-mode WCSPH step).
  */
 #ifndef SPH2O_INTERNAL_H
 #define SPH2O_INTERNAL_H
@@ -89,6 +90,41 @@ int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergenc
 int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s);
 int launch_dfsph_solve_batch(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s);
 int launch_barrier_timeout_probe(DevState* st, cudaStream_t s);
+
+/* sph_adjoint.cu: reverse-mode WCSPH step. Sorted-order arrays of the
+   recomputed step (pos .. cnt_b), caller-order adjoint state (xbar, vbar),
+   sorted-order work arrays (abar .. rhobar) and per-block FP64 partial sums
+   part[3 b + q] (q = 0: dL/dk, 1: dL/dnu, 2: loss * N), adjoint_blocks(n)
+   blocks, which launch_adjoint_finish reduces into red[0..2]. */
+struct AdjointArrays {
+    const float4* pos;
+    const float4* vel;
+    const float* rho;
+    const float* press;
+    const unsigned* orig;
+    const float4* bpos;
+    const unsigned* nbr_f;
+    const unsigned* cnt_f;
+    const unsigned* nbr_b;
+    const unsigned* cnt_b;
+    const DevState* st;
+    float4* xbar;
+    float4* vbar;
+    float4* abar;
+    float4* xacc;
+    float4* vacc;
+    float* Ap;
+    float* rhobar;
+    double* part;
+};
+int adjoint_blocks(int n);
+void launch_adjoint_seed(int n, const float4* pos, const unsigned* orig, const float* target, float4* xbar,
+                         float4* vbar, double* part, cudaStream_t s);
+void launch_adjoint_finish(int n, const double* part, double* red, cudaStream_t s);
+/* load + forces + density adjoint kernels of one step (3 launches) */
+void launch_adjoint_step(const SimParams& P, const AdjointArrays& J, cudaStream_t s);
+void launch_adjoint_unpack(int n, const float4* in, float* out3, cudaStream_t s);
+
 /* co-resident grid size of the persistent solver kernels (0 on error) */
 int persistent_grid(bool pcisph, bool divergence, bool batch = false, int occ = 8);
 constexpr int kSolverBlock = 256;

@@ -19,7 +19,8 @@ fluid would otherwise touch or cross the walls, fluid placed 4r from walls):
   dam_break_dfsph_125k   DFSPH + Akinci surface tension 0.05, 50^3, r=0.01
   double_dam_break_1m    DFSPH or PCISPH, 2 x 100x100x50 blocks, r=0.005,
                          4x2x2 m tank with a sphere obstacle R=0.2
-  adjoint_wcsph_32k      WCSPH, 32^3, r=0.02
+  adjoint_wcsph_32k      WCSPH, 32^3, r=0.02 (with adjoint_problem: seeded
+                         initial velocities and target block)
 """
 from __future__ import annotations
 
@@ -178,6 +179,18 @@ def adjoint_wcsph_32k(seed=5):
         tank=((0, 0, 0), (2.5, 1.28 + 8 * r, 1.28 + 8 * r)), time_step=2e-4,
         stiffness=400.0, gamma=7.0, viscosity=0.01, seed=seed,
     )
+
+
+def adjoint_problem(x0, seed_v=5, seed_t=6, sigma=0.1):
+    """Initial velocities and target of the differentiable WCSPH workload:
+    v0 ~ N(0, sigma^2) per component (seed_v) and the target = the initial
+    block shifted by a seeded offset (seed_t) of 0.05-0.15 m in x and
+    -0.05-0.05 m in y, z unchanged. Returns float32 arrays (n, 3)."""
+    x0 = np.asarray(x0, np.float32)
+    v0 = np.random.default_rng(seed_v).normal(0.0, sigma, x0.shape).astype(np.float32)
+    rng = np.random.default_rng(seed_t)
+    shift = np.array([rng.uniform(0.05, 0.15), rng.uniform(-0.05, 0.05), 0.0], np.float32)
+    return v0, (x0 + shift).astype(np.float32)
 
 
 def small(method=DFSPH, n=(10, 10, 10), radius=0.025, surface_tension=0.0,

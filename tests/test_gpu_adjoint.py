@@ -1,0 +1,187 @@
+"""GPU WCSPH adjoint (sph_wcsph_forward / sph_wcsph_backward) against the
+FP64 CPU adjoint of the oracle (pinned by test_oracle_adjoint.py) and FP64
+central differences, plus size-independent properties at the full
+32,768-particle, 500-step workload.
+
+Tolerances: the GPU runs in FP32, the oracle in FP64; gradients agree within
+1e-3 relative (norm-wise for vectors), the bar the adjoint is built to."""
+import numpy as np
+import pytest
+
+from oracle.oracle import wcsph_adjoint
+from sph2o_b200 import scenes as S
+from sph2o_b200.api import Scene, Simulation, SphError
+
+pytestmark = pytest.mark.gpu
+
+NSTEPS = 40
+TOL = 1e-3
+
+
+def rel_norm(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module", params=["visc", "visc_bvisc", "inviscid"])
+def case(request):
+    kw = {"visc": dict(viscosity=0.01), "visc_bvisc": dict(viscosity=0.02, boundary_viscosity=0.01),
+          "inviscid": dict(viscosity_method=-1, viscosity=0.0)}[request.param]
+    d = S.small(method=S.WCSPH, n=(10, 9, 8), radius=0.02, time_step=2e-4, seed=5, **kw)
+    sc = Scene.from_dict(d)
+    desc = sc.desc()
+    x0, _ = sc.fluid()
+    b = sc.boundary()
+    v0, t = S.adjoint_problem(x0)
+    sim = Simulation(desc, x0, b, vel=v0)
+    loss = sim.wcsph_forward(NSTEPS, t, ckpt_every=8)
+    g = sim.wcsph_backward(want_x0=True)
+    ref = wcsph_adjoint(desc, x0, v0, b, NSTEPS, t)
+    yield request.param, desc, x0, v0, b, t, sim, loss, g, ref
+    sim.close()
+
+
+def test_loss_matches_fp64(case):
+    name, desc, x0, v0, b, t, sim, loss, g, ref = case
+    assert abs(loss - ref["loss"]) <= 1e-4 * ref["loss"], (loss, ref["loss"])
+
+
+def test_v0_gradient_matches_fp64_adjoint(case):
+    name, desc, x0, v0, b, t, sim, loss, g, ref = case
+    assert np.all(np.isfinite(g["v0"]))
+    assert rel_norm(g["v0"], ref["v0"]) <= TOL
+
+
+def test_x0_gradient_matches_fp64_adjoint(case):
+    name, desc, x0, v0, b, t, sim, loss, g, ref = case
+    assert rel_norm(g["x0"], ref["x0"]) <= TOL
+
+
+def test_parameter_gradients_match_fp64_adjoint(case):
+    name, desc, x0, v0, b, t, sim, loss, g, ref = case
+    assert abs(g["stiffness"] - ref["stiffness"]) <= TOL * abs(ref["stiffness"])
+    if name == "inviscid":
+        assert g["viscosity"] == 0.0
+    else:
+        assert abs(g["viscosity"] - ref["viscosity"]) <= TOL * abs(ref["viscosity"])
+
+
+def test_v0_gradient_matches_fp64_central_differences(case):
+    """Directional derivative along a seeded direction vs FP64 central
+    differences of the oracle's forward run (eps = 1e-4)."""
+    name, desc, x0, v0, b, t, sim, loss, g, ref = case
+    d = np.random.default_rng(42).normal(size=x0.shape)
+    eps = 1e-4
+    lp = wcsph_adjoint(desc, x0, v0.astype(np.float64) + eps * d, b, NSTEPS, t, grad=False)["loss"]
+    lm = wcsph_adjoint(desc, x0, v0.astype(np.float64) - eps * d, b, NSTEPS, t, grad=False)["loss"]
+    fd = (lp - lm) / (2 * eps)
+    ad = float(np.sum(g["v0"].astype(np.float64) * d))
+    assert abs(ad - fd) <= TOL * abs(fd), (ad, fd)
+
+
+def test_forward_is_the_ordinary_step(case):
+    """sph_wcsph_forward takes exactly the steps sph_step takes, and the
+    backward pass leaves the context in the forward run's final state."""
+    name, desc, x0, v0, b, t, sim, loss, g, ref = case
+    plain = Simulation(desc, x0, b, vel=v0)
+    plain.step(NSTEPS)
+    px, pv, _ = plain.state()
+    plain.close()
+    ax, av, _ = sim.state()
+    assert np.array_equal(px, ax) and np.array_equal(pv, av)
+    assert loss == pytest.approx(float(np.mean(np.sum((px.astype(np.float64) - t) ** 2, axis=1))), rel=1e-12)
+
+
+@pytest.mark.parametrize("every", [1, 5, NSTEPS])
+def test_checkpoint_interval_does_not_change_gradients(every):
+    """Recomputation from checkpoints is bit-identical to the forward run, so
+    the gradients do not depend on the checkpoint interval."""
+    d = S.small(method=S.WCSPH, n=(8, 8, 8), radius=0.02, time_step=2e-4, seed=9)
+    sc = Scene.from_dict(d)
+    x0, _ = sc.fluid()
+    v0, t = S.adjoint_problem(x0)
+    out = []
+    for k in (every, 7):
+        sim = Simulation(sc.desc(), x0, sc.boundary(), vel=v0)
+        loss = sim.wcsph_forward(NSTEPS, t, ckpt_every=k)
+        out.append((loss, sim.wcsph_backward()))
+        sim.close()
+    (l0, g0), (l1, g1) = out
+    assert l0 == l1
+    assert np.array_equal(g0["v0"], g1["v0"])
+    assert g0["viscosity"] == g1["viscosity"] and g0["stiffness"] == g1["stiffness"]
+
+
+def test_backward_twice_and_continue_stepping():
+    d = S.small(method=S.WCSPH, n=(8, 8, 8), radius=0.02, time_step=2e-4, seed=10)
+    sc = Scene.from_dict(d)
+    x0, _ = sc.fluid()
+    v0, t = S.adjoint_problem(x0)
+    sim = Simulation(sc.desc(), x0, sc.boundary(), vel=v0)
+    sim.wcsph_forward(10, t, ckpt_every=4)
+    g1 = sim.wcsph_backward()
+    g2 = sim.wcsph_backward()
+    assert np.array_equal(g1["v0"], g2["v0"])
+    x10, v10, _ = sim.state()
+    sim.step(5)
+    ref = Simulation(sc.desc(), x0, sc.boundary(), vel=v0)
+    ref.step(15)
+    assert np.array_equal(sim.state()[0], ref.state()[0])
+    ref.close()
+    sim.close()
+
+
+def test_unsupported_configurations_rejected():
+    d = S.small(method=S.DFSPH, n=(6, 6, 6), seed=3)
+    sc = Scene.from_dict(d)
+    x0, _ = sc.fluid()
+    sim = Simulation(sc.desc(), x0, sc.boundary())
+    with pytest.raises(SphError) as e:
+        sim.wcsph_forward(2, x0)
+    assert e.value.code == -1
+    sim.close()
+    d = S.small(method=S.WCSPH, n=(6, 6, 6), seed=3, surface_tension=0.05)
+    sc = Scene.from_dict(d)
+    sim = Simulation(sc.desc(), x0, sc.boundary())
+    with pytest.raises(SphError) as e:
+        sim.wcsph_forward(2, x0)
+    assert e.value.code == -1
+    sim.close()
+    d = S.small(method=S.WCSPH, n=(6, 6, 6), seed=3)
+    sc = Scene.from_dict(d)
+    sim = Simulation(sc.desc(), x0, sc.boundary())
+    with pytest.raises(SphError) as e:
+        sim.wcsph_backward()
+    assert e.value.code == -6
+    sim.close()
+
+
+def test_full_size_32k_500_steps():
+    """The differentiable workload at full size: 32,768 particles, 500 steps,
+    checkpoint every 50. Properties: finite gradients; checkpoint interval
+    50 and 100 give bit-identical gradients; a small step against the
+    gradient lowers the loss by about the first-order prediction."""
+    sc = Scene.from_dict(S.adjoint_wcsph_32k())
+    x0, _ = sc.fluid()
+    b = sc.boundary()
+    v0, t = S.adjoint_problem(x0)
+    sim = Simulation(sc.desc(), x0, b, vel=v0)
+    loss = sim.wcsph_forward(500, t, ckpt_every=50)
+    g = sim.wcsph_backward()
+    sim.close()
+    assert np.all(np.isfinite(g["v0"])) and np.isfinite(g["viscosity"]) and np.isfinite(g["stiffness"])
+    sim = Simulation(sc.desc(), x0, b, vel=v0)
+    loss2 = sim.wcsph_forward(500, t, ckpt_every=100)
+    g2 = sim.wcsph_backward()
+    sim.close()
+    assert loss == loss2 and np.array_equal(g["v0"], g2["v0"])
+    gv = g["v0"].astype(np.float64)
+    gn = float(np.linalg.norm(gv))
+    alpha = 0.01 / gn  # move v0 by 0.01 m/s (norm) against the gradient
+    sim = Simulation(sc.desc(), x0, b, vel=(v0 - alpha * gv).astype(np.float32))
+    lower = sim.wcsph_forward(500, t, ckpt_every=500)
+    sim.close()
+    predicted = alpha * gn * gn
+    assert lower < loss
+    assert abs((loss - lower) - predicted) <= 0.1 * predicted, (loss - lower, predicted)

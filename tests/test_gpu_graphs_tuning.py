@@ -51,8 +51,8 @@ def test_graph_replay_matches_eager_bitwise(method):
 
 @pytest.mark.parametrize("method", METHODS)
 def test_graph_replay_odd_chunks(method):
-    """Odd step counts mix one eager step with graph pairs; the buffer
-    assignment alternates, so both graph keys are exercised."""
+    """Odd step counts mix a single-step graph with graph pairs; the buffer
+    assignment alternates, so every graph key is exercised."""
     a, ta, _ = run(method, 9, chunk=3)
     b, tb, _ = run(method, 9, [(api.OPT_CUDA_GRAPHS, 0)])
     for u, w in zip(a, b):
