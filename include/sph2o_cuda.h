@@ -161,18 +161,22 @@ enum sph_option {
                                      for an odd remainder), keyed by the buffer assignment */
     SPH_OPT_CELL_ORDER = 1,       /* 0 (default): 4x4x4 cell bricks, Morton inside; 1: linear, x fastest */
     SPH_OPT_SOLVER_OCCUPANCY = 2, /* DFSPH persistent solver blocks per SM: 8 (default) or 4 */
-    SPH_OPT_PASS_BLOCK = 3        /* threads per block of the particle-pass kernels: 256 (default) or 128 */
+    SPH_OPT_PASS_BLOCK = 3,       /* threads per block of the particle-pass kernels: 256 (default) or 128 */
+    SPH_OPT_SOLVER_LANES = 4      /* lanes sharing one particle's neighbour list in the persistent DFSPH
+                                     solver: 1, 2 (default) or 4 */
 };
+/* Number of values sph_autotune chooses (options 1..4 in order). */
+#define SPH_TUNE_COUNT 4
 int sph_set_option(sph_ctx* ctx, int option, int value);
 int sph_get_option(const sph_ctx* ctx, int option, int* value);
 
-/* Chooses SPH_OPT_CELL_ORDER, SPH_OPT_SOLVER_OCCUPANCY and SPH_OPT_PASS_BLOCK
-   by timing trial_steps steps (CUDA events) of every combination, each from
-   a snapshot of the current state that is restored afterwards: the
-   simulation is left exactly where it was. cache_path (may be NULL) names a
-   JSON file keyed by GPU name, method and particle counts; a hit skips the
-   trials and a miss appends the result. config (may be NULL) receives the
-   three chosen values in option order 1..3. */
+/* Chooses SPH_OPT_CELL_ORDER, SPH_OPT_SOLVER_OCCUPANCY, SPH_OPT_PASS_BLOCK and
+   SPH_OPT_SOLVER_LANES by timing trial_steps steps (CUDA events) of every
+   combination, each from a snapshot of the current state that is restored
+   afterwards: the simulation is left exactly where it was. cache_path (may
+   be NULL) names a JSON file keyed by GPU name, method and particle counts;
+   a hit skips the trials and a miss appends the result. config (may be NULL)
+   receives the SPH_TUNE_COUNT chosen values in option order 1..4. */
 int sph_autotune(sph_ctx* ctx, int trial_steps, const char* cache_path, int* config);
 
 /* Fluid state in the caller's particle order. Any pointer may be NULL.

@@ -27,7 +27,8 @@ STATUS = {
     -7: "SPH_ERR_NO_DEVICE", -8: "SPH_ERR_IO", -9: "SPH_ERR_CAPACITY",
 }
 PHASE_DENSITY, PHASE_ALPHA, PHASE_NONPRESSURE_ACC, PHASE_PRESSURE, PHASE_PRESSURE_ACC = range(5)
-OPT_CUDA_GRAPHS, OPT_CELL_ORDER, OPT_SOLVER_OCCUPANCY, OPT_PASS_BLOCK = range(4)
+OPT_CUDA_GRAPHS, OPT_CELL_ORDER, OPT_SOLVER_OCCUPANCY, OPT_PASS_BLOCK, OPT_SOLVER_LANES = range(5)
+TUNE_COUNT = 4
 PROF_NAMES = ["sort", "lists", "density", "normals", "forces", "density_solve", "divergence_solve",
               "pressure_solve"]
 PROF_COUNT = len(PROF_NAMES)
@@ -285,10 +286,10 @@ class Simulation:
         return v.value
 
     def autotune(self, trial_steps=3, cache_path=None):
-        cfg = (C.c_int * 3)()
+        cfg = (C.c_int * TUNE_COUNT)()
         path = os.fsencode(cache_path) if cache_path else None
         self._check(lib().sph_autotune(self._h, int(trial_steps), path, cfg))
-        return {"cell_order": cfg[0], "solver_occupancy": cfg[1], "pass_block": cfg[2]}
+        return {"cell_order": cfg[0], "solver_occupancy": cfg[1], "pass_block": cfg[2], "solver_lanes": cfg[3]}
 
     def profile(self, enable=True):
         self._check(lib().sph_profile_enable(self._h, 1 if enable else 0))

@@ -72,7 +72,8 @@ struct sph_ctx {
     DevState* st_host = nullptr; /* pinned mirror */
     double* accum = nullptr;
     size_t accum_len = 0;
-    int grid_density = 0, grid_div = 0, grid_pcisph = 0;
+    int grid_pcisph = 0;
+    int grid_solve[2][2][3] = {};  /* DFSPH solver grid by [divergence][occupancy 8, 4][lanes 1, 2, 4] */
     DevState last{};
     bool lists_valid = false;
     /* timing: batch events + per-phase profiling */
@@ -103,7 +104,7 @@ struct sph_ctx {
     /* tunables (sph_set_option / sph_autotune) */
     int pass_block = 256;
     int solver_occ = 8;
-    int grid_density4 = 0, grid_div4 = 0;
+    int solver_tpp = 2;  /* measured best on B200 for the 1M-particle scene (1, 2, 4: 1.03, 0.84, 0.92 ms) */
     float4* braw = nullptr;      /* boundary in caller order (re-sorted when the cell order changes) */
     unsigned* bid = nullptr;
     /* autotune snapshot */
@@ -420,6 +421,13 @@ int step_pcisph(sph_ctx* c)
     return check_launch(c, "pcisph step");
 }
 
+int tpp_index(int tpp) { return tpp == 4 ? 2 : tpp == 2 ? 1 : 0; }
+
+int solve_grid(const sph_ctx* c, bool divergence)
+{
+    return c->grid_solve[divergence ? 1 : 0][c->solver_occ == 4 ? 1 : 0][tpp_index(c->solver_tpp)];
+}
+
 int step_dfsph(sph_ctx* c)
 {
     int rc;
@@ -431,7 +439,7 @@ int step_dfsph(sph_ctx* c)
     {
         Phase ph(c, SPH_PROF_DENSITY_SOLVE, 1);
         e = c->nscenes ? launch_dfsph_solve_batch(c->P, A, false, c->grid_batch_density, c->stream)
-                       : launch_dfsph_solve(c->P, A, false, c->solver_occ == 4 ? c->grid_density4 : c->grid_density, c->solver_occ, c->stream);
+                       : launch_dfsph_solve(c->P, A, false, solve_grid(c, false), c->solver_occ, c->solver_tpp, c->stream);
     }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph density solver launch: ") + cudaGetErrorString((cudaError_t)e));
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
@@ -442,7 +450,7 @@ int step_dfsph(sph_ctx* c)
     {
         Phase ph(c, SPH_PROF_DIVERGENCE_SOLVE, 1);
         e = c->nscenes ? launch_dfsph_solve_batch(c->P, A, true, c->grid_batch_div, c->stream)
-                       : launch_dfsph_solve(c->P, A, true, c->solver_occ == 4 ? c->grid_div4 : c->grid_div, c->solver_occ, c->stream);
+                       : launch_dfsph_solve(c->P, A, true, solve_grid(c, true), c->solver_occ, c->solver_tpp, c->stream);
     }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph divergence solver launch: ") + cudaGetErrorString((cudaError_t)e));
     return check_launch(c, "dfsph step");
@@ -829,13 +837,14 @@ int sph_init(sph_ctx* c)
     CUDA_TRY(c, cudaEventCreate(&c->ev_begin));
     CUDA_TRY(c, cudaEventCreate(&c->ev_end));
 
-    c->grid_density = persistent_grid(false, false, false, 8);
-    c->grid_div = persistent_grid(false, true, false, 8);
-    c->grid_density4 = persistent_grid(false, false, false, 4);
-    c->grid_div4 = persistent_grid(false, true, false, 4);
     c->grid_pcisph = persistent_grid(true, false);
-    if (c->grid_density <= 0 || c->grid_div <= 0 || c->grid_pcisph <= 0)
-        return fail(c, SPH_ERR_CUDA, "cannot size the persistent solver grid");
+    if (c->grid_pcisph <= 0) return fail(c, SPH_ERR_CUDA, "cannot size the persistent solver grid");
+    for (int dv = 0; dv < 2; ++dv)
+        for (int o = 0; o < 2; ++o)
+            for (int t = 0; t < 3; ++t) {
+                c->grid_solve[dv][o][t] = persistent_grid(false, dv == 1, false, o ? 4 : 8, 1 << t);
+                if (c->grid_solve[dv][o][t] <= 0) return fail(c, SPH_ERR_CUDA, "cannot size the persistent solver grid");
+            }
 
     /* upload: fluid in caller order becomes the first "unsorted" state */
     float* stage = nullptr;
@@ -1245,8 +1254,8 @@ bool tune_lookup(const char* path, const std::string& key, int* cfg)
     try {
         const sphjson::Value root = sphjson::parse(ss.str());
         const sphjson::Value* v = root.find(key);
-        if (!v || v->size() != 3) return false;
-        for (int i = 0; i < 3; ++i) cfg[i] = (int)v->at(i).as_number();
+        if (!v || v->size() != SPH_TUNE_COUNT) return false;
+        for (int i = 0; i < SPH_TUNE_COUNT; ++i) cfg[i] = (int)v->at(i).as_number();
         return true;
     } catch (const std::exception&) {
         return false;
@@ -1265,22 +1274,24 @@ void tune_store(const char* path, const std::string& key, const int* cfg)
             try {
                 const sphjson::Value root = sphjson::parse(ss.str());
                 for (const auto& kv : root.items()) {
-                    if (kv.first == key || kv.second.size() != 3) continue;
-                    entries.push_back({kv.first, {(int)kv.second.at(0).as_number(), (int)kv.second.at(1).as_number(),
-                                                  (int)kv.second.at(2).as_number()}});
+                    if (kv.first == key || kv.second.size() != SPH_TUNE_COUNT) continue;
+                    std::vector<int> v;
+                    for (int i = 0; i < SPH_TUNE_COUNT; ++i) v.push_back((int)kv.second.at(i).as_number());
+                    entries.push_back({kv.first, v});
                 }
             } catch (const std::exception&) {
             }
         }
     }
-    entries.push_back({key, {cfg[0], cfg[1], cfg[2]}});
+    entries.push_back({key, std::vector<int>(cfg, cfg + SPH_TUNE_COUNT)});
     std::ofstream o(path);
     o << "{\n";
     for (size_t i = 0; i < entries.size(); ++i) {
         std::string k;
         for (char ch : entries[i].first) k += (ch == '"' || ch == '\\') ? std::string("\\") + ch : std::string(1, ch);
-        o << "  \"" << k << "\": [" << entries[i].second[0] << ", " << entries[i].second[1] << ", "
-          << entries[i].second[2] << "]" << (i + 1 < entries.size() ? "," : "") << "\n";
+        o << "  \"" << k << "\": [";
+        for (int q = 0; q < SPH_TUNE_COUNT; ++q) o << (q ? ", " : "") << entries[i].second[q];
+        o << "]" << (i + 1 < entries.size() ? "," : "") << "\n";
     }
     o << "}\n";
 }
@@ -1289,6 +1300,7 @@ int apply_config(sph_ctx* c, const int* cfg)
 {
     c->solver_occ = cfg[1] == 4 ? 4 : 8;
     c->pass_block = cfg[2] == 128 ? 128 : 256;
+    c->solver_tpp = (cfg[3] == 2 || cfg[3] == 4) ? cfg[3] : 1;
     drop_graphs(c);
     if (cfg[0] != c->P.cell_order) return apply_cell_order(c, cfg[0] == 1 ? 1 : 0);
     return SPH_OK;
@@ -1321,6 +1333,11 @@ int sph_set_option(sph_ctx* c, int option, int value)
         c->pass_block = value;
         drop_graphs(c);
         return SPH_OK;
+    case SPH_OPT_SOLVER_LANES:
+        if (value != 1 && value != 2 && value != 4) return fail(c, SPH_ERR_ARG, "solver lanes per particle is 1, 2 or 4");
+        c->solver_tpp = value;
+        drop_graphs(c);
+        return SPH_OK;
     default:
         return fail(c, SPH_ERR_ARG, "unknown option");
     }
@@ -1334,6 +1351,7 @@ int sph_get_option(const sph_ctx* c, int option, int* value)
     case SPH_OPT_CELL_ORDER: *value = c->P.cell_order; return SPH_OK;
     case SPH_OPT_SOLVER_OCCUPANCY: *value = c->solver_occ; return SPH_OK;
     case SPH_OPT_PASS_BLOCK: *value = c->pass_block; return SPH_OK;
+    case SPH_OPT_SOLVER_LANES: *value = c->solver_tpp; return SPH_OK;
     default: return SPH_ERR_ARG;
     }
 }
@@ -1344,11 +1362,11 @@ int sph_autotune(sph_ctx* c, int trial_steps, const char* cache_path, int* confi
     if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_autotune before sph_init");
     if (trial_steps < 1) return fail(c, SPH_ERR_ARG, "trial_steps must be positive");
     const std::string key = tune_key(c);
-    int best[3] = {c->P.cell_order, c->solver_occ, c->pass_block};
+    int best[SPH_TUNE_COUNT] = {c->P.cell_order, c->solver_occ, c->pass_block, c->solver_tpp};
     int rc;
     if (tune_lookup(cache_path, key, best)) {
         if ((rc = apply_config(c, best)) != SPH_OK) return rc;
-        if (config) for (int i = 0; i < 3; ++i) config[i] = best[i];
+        if (config) for (int i = 0; i < SPH_TUNE_COUNT; ++i) config[i] = best[i];
         return SPH_OK;
     }
     if ((rc = snapshot(c, true)) != SPH_OK) return rc;
@@ -1359,12 +1377,15 @@ int sph_autotune(sph_ctx* c, int trial_steps, const char* cache_path, int* confi
     double best_ms = 1e300;
     const bool dfsph = c->desc.simulation_method == SPH_DFSPH;
     for (int order = 0; order < 2; ++order)
-        for (int occ : {8, 4}) {
-            if ((!dfsph || c->nscenes) && occ == 4) continue;  /* only the single-scene DFSPH solver has it */
+        for (int occ : {8, 4})
+            for (int tpp : {1, 2, 4}) {
+            /* only the single-scene DFSPH solver has these variants */
+            if ((!dfsph || c->nscenes) && (occ == 4 || tpp != 1)) continue;
             for (int blk : {256, 128}) {
-                const int cfg[3] = {order, occ, blk};
+                const int cfg[SPH_TUNE_COUNT] = {order, occ, blk, tpp};
                 if ((rc = snapshot(c, false)) != SPH_OK) return rc;
                 c->solver_occ = occ;
+                c->solver_tpp = tpp;
                 c->pass_block = blk;
                 rc = order != c->P.cell_order ? apply_cell_order(c, order) : refresh(c);
                 if (rc != SPH_OK) return rc;
@@ -1380,14 +1401,15 @@ int sph_autotune(sph_ctx* c, int trial_steps, const char* cache_path, int* confi
                 cudaEventElapsedTime(&ms, c->ev_begin, c->ev_end);
                 if (ms < best_ms) {
                     best_ms = ms;
-                    for (int i = 0; i < 3; ++i) best[i] = cfg[i];
+                    for (int i = 0; i < SPH_TUNE_COUNT; ++i) best[i] = cfg[i];
                 }
             }
-        }
+            }
     /* back to the snapshot with the chosen configuration */
     if ((rc = snapshot(c, false)) != SPH_OK) return rc;
     c->solver_occ = best[1];
     c->pass_block = best[2];
+    c->solver_tpp = best[3];
     rc = best[0] != c->P.cell_order ? apply_cell_order(c, best[0]) : refresh(c);
     if (rc != SPH_OK) return rc;
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -1396,7 +1418,7 @@ int sph_autotune(sph_ctx* c, int trial_steps, const char* cache_path, int* confi
     c->use_graphs = graphs;
     c->batch_open = false;
     tune_store(cache_path, key, best);
-    if (config) for (int i = 0; i < 3; ++i) config[i] = best[i];
+    if (config) for (int i = 0; i < SPH_TUNE_COUNT; ++i) config[i] = best[i];
     return SPH_OK;
 }
 

@@ -85,8 +85,10 @@ enum ForceMode : int {
 void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool eos, int block, cudaStream_t s);
 void launch_normals(const SimParams& P, const DeviceArrays& A, int block, cudaStream_t s);
 void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, int block, cudaStream_t s);
-/* occ: blocks per SM of the persistent DFSPH solver variant (4 or 8) */
-int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, int occ, cudaStream_t s);
+/* occ: blocks per SM of the persistent DFSPH solver variant (4 or 8);
+   tpp: lanes per particle in its neighbour passes (1, 2 or 4) */
+int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, int occ, int tpp,
+                       cudaStream_t s);
 int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s);
 int launch_dfsph_solve_batch(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s);
 int launch_barrier_timeout_probe(DevState* st, cudaStream_t s);
@@ -126,7 +128,7 @@ void launch_adjoint_step(const SimParams& P, const AdjointArrays& J, cudaStream_
 void launch_adjoint_unpack(int n, const float4* in, float* out3, cudaStream_t s);
 
 /* co-resident grid size of the persistent solver kernels (0 on error) */
-int persistent_grid(bool pcisph, bool divergence, bool batch = false, int occ = 8);
+int persistent_grid(bool pcisph, bool divergence, bool batch = false, int occ = 8, int tpp = 1);
 constexpr int kSolverBlock = 256;
 
 } // namespace sph

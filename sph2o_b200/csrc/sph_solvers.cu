@@ -268,32 +268,42 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
 /* ---------------------------------------------------------------------- */
 /* DFSPH pieces                                                             */
 
-/* predicted density (DIV=false) or divergence error (DIV=true) of particle i */
-template <bool DIV>
-__device__ __forceinline__ float dfsph_residual(const SimParams& P, const DeviceArrays& A, int i, size_t nf,
-                                                float dt)
+/* Sum of the residual terms of particle i over the neighbour-list entries
+   sub, sub + TPP, ... (fluid, then boundary). */
+template <bool DIV, int TPP>
+__device__ __forceinline__ float dfsph_residual_part(const SimParams& P, const DeviceArrays& A, int i, int sub,
+                                                     size_t nf)
 {
     const float4 xi = A.pos[i];
     const float4 vi = A.vel[i];
     float sum = 0.0f;
     const unsigned nF = A.cnt_f[i], nB = A.cnt_b[i];
-    for (unsigned kk = 0; kk < nF; ++kk) {
+    for (unsigned kk = sub; kk < nF; kk += TPP) {
         const unsigned j = A.nbr_f[kk * nf + i];
         const Pair p = make_pair(xi, A.pos[j]);
         const float4 vj = A.vel[j];
         const float f = cs_gradf(p.rl, p.inv_rl, P);
         sum += P.mass * (f * (((vi.x - vj.x) * p.rx + (vi.y - vj.y) * p.ry) + (vi.z - vj.z) * p.rz));
     }
-    for (unsigned kk = 0; kk < nB; ++kk) {
+    for (unsigned kk = sub; kk < nB; kk += TPP) {
         const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
         const Pair p = make_pair(xi, xb);
         const float f = cs_gradf(p.rl, p.inv_rl, P);
         sum += xb.w * (f * ((vi.x * p.rx + vi.y * p.ry) + vi.z * p.rz));
     }
+    return sum;
+}
+
+/* The residual from the summed terms: predicted density (DIV=false) or
+   divergence error (DIV=true) of particle i. */
+template <bool DIV>
+__device__ __forceinline__ float dfsph_residual_finish(const SimParams& P, const DeviceArrays& A, int i, float sum,
+                                                       float dt)
+{
     if (DIV) {
         /* particles with fewer than 20 neighbours within h are not corrected
            (DFSPHSolver.cpp:608-611); the lists hold exactly those neighbours */
-        if (nF + nB < 20u) return 0.0f;
+        if (A.cnt_f[i] + A.cnt_b[i] < 20u) return 0.0f;
         return fmaxf(sum, 0.0f);
     }
     /* rho_i + dt * change, rounded as the reference rounds it: the result
@@ -301,15 +311,26 @@ __device__ __forceinline__ float dfsph_residual(const SimParams& P, const Device
     return fmaxf(__fadd_rn(A.rho[i], __fmul_rn(sum, dt)), P.rho0);
 }
 
-/* v_i -= dt * sum_j m (k_i + k_j) gradW  (+ boundary with k_i) */
-__device__ __forceinline__ void dfsph_correct(const SimParams& P, const DeviceArrays& A, const float* __restrict__ K,
-                                              int i, size_t nf, float dt)
+/* predicted density (DIV=false) or divergence error (DIV=true) of particle i */
+template <bool DIV>
+__device__ __forceinline__ float dfsph_residual(const SimParams& P, const DeviceArrays& A, int i, size_t nf,
+                                                float dt)
+{
+    return dfsph_residual_finish<DIV>(P, A, i, dfsph_residual_part<DIV, 1>(P, A, i, 0, nf), dt);
+}
+
+/* Partial sums over list entries sub, sub + TPP, ... of
+   sum_j m (k_i + k_j) gradW  (+ boundary with k_i). */
+template <int TPP>
+__device__ __forceinline__ void dfsph_correct_part(const SimParams& P, const DeviceArrays& A,
+                                                   const float* __restrict__ K, int i, int sub, size_t nf,
+                                                   float& sx, float& sy, float& sz)
 {
     const float4 xi = A.pos[i];
     const float ki = K[i];
-    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    sx = sy = sz = 0.0f;
     const unsigned nF = A.cnt_f[i];
-    for (unsigned kk = 0; kk < nF; ++kk) {
+    for (unsigned kk = sub; kk < nF; kk += TPP) {
         const unsigned j = A.nbr_f[kk * nf + i];
         const float ks = ki + K[j];
         if (fabsf(ks) > P.eps) {
@@ -320,13 +341,17 @@ __device__ __forceinline__ void dfsph_correct(const SimParams& P, const DeviceAr
     }
     if (fabsf(ki) > P.eps) {
         const unsigned nB = A.cnt_b[i];
-        for (unsigned kk = 0; kk < nB; ++kk) {
+        for (unsigned kk = sub; kk < nB; kk += TPP) {
             const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
             const Pair p = make_pair(xi, xb);
             const float c = xb.w * ki * cs_gradf(p.rl, p.inv_rl, P);
             sx += c * p.rx; sy += c * p.ry; sz += c * p.rz;
         }
     }
+}
+
+__device__ __forceinline__ void dfsph_apply(const DeviceArrays& A, int i, float dt, float sx, float sy, float sz)
+{
     float4 v = A.vel[i];
     v.x = __fsub_rn(v.x, __fmul_rn(dt, sx));
     v.y = __fsub_rn(v.y, __fmul_rn(dt, sy));
@@ -334,11 +359,72 @@ __device__ __forceinline__ void dfsph_correct(const SimParams& P, const DeviceAr
     A.vel[i] = v;
 }
 
+/* v_i -= dt * sum_j m (k_i + k_j) gradW  (+ boundary with k_i) */
+__device__ __forceinline__ void dfsph_correct(const SimParams& P, const DeviceArrays& A, const float* __restrict__ K,
+                                              int i, size_t nf, float dt)
+{
+    float sx, sy, sz;
+    dfsph_correct_part<1>(P, A, K, i, 0, nf, sx, sy, sz);
+    dfsph_apply(A, i, dt, sx, sy, sz);
+}
+
+/* Sum over the TPP adjacent lanes that share a particle (all lanes call). */
+template <int TPP>
+__device__ __forceinline__ float lane_group_sum(float v)
+{
+    for (int o = TPP / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+/* Calls f(i, sub, valid) for every particle i < n, TPP adjacent lanes per
+   particle (sub = lane index within the group), 32 / TPP particles per warp,
+   warps striding over the grid. The trip count is uniform per warp, so f may
+   use warp shuffles; lanes past the end get valid = false. */
+template <int TPP, typename F>
+__device__ __forceinline__ void for_particles(int n, F&& f)
+{
+    constexpr int PPW = 32 / TPP;
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int base = gw * PPW; base < n; base += nw * PPW) {
+        const int i = base + lane / TPP;
+        f(i, lane % TPP, i < n);
+    }
+}
+
+/* residual of particle i with its list split over TPP lanes (all lanes call) */
+template <bool DIV, int TPP>
+__device__ __forceinline__ float dfsph_residual_lanes(const SimParams& P, const DeviceArrays& A, int i, int sub,
+                                                      bool valid, size_t nf, float dt)
+{
+    float part = valid ? dfsph_residual_part<DIV, TPP>(P, A, i, sub, nf) : 0.0f;
+    if (TPP > 1) part = lane_group_sum<TPP>(part);
+    return valid ? dfsph_residual_finish<DIV>(P, A, i, part, dt) : 0.0f;
+}
+
+/* velocity correction of particle i with its list split over TPP lanes */
+template <int TPP>
+__device__ __forceinline__ void dfsph_correct_lanes(const SimParams& P, const DeviceArrays& A,
+                                                    const float* __restrict__ K, int i, int sub, bool valid,
+                                                    size_t nf, float dt)
+{
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    if (valid) dfsph_correct_part<TPP>(P, A, K, i, sub, nf, sx, sy, sz);
+    if (TPP > 1) {
+        sx = lane_group_sum<TPP>(sx);
+        sy = lane_group_sum<TPP>(sy);
+        sz = lane_group_sum<TPP>(sz);
+    }
+    if (valid && sub == 0) dfsph_apply(A, i, dt, sx, sy, sz);
+}
+
 /* OCC blocks of 256 per SM: 8 (32 registers) by default -- the passes are
    bound by the latency of dependent neighbour gathers and full occupancy
    hides most of it; 4 (64 registers, no spills) is the autotuner's other
-   candidate */
-template <bool DIV, int OCC>
+   candidate. TPP lanes share a particle in the neighbour passes (1, 2 or 4):
+   more gathers in flight per particle, fewer particles per warp. */
+template <bool DIV, int OCC, int TPP>
 __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, DeviceArrays A)
 {
     __shared__ double s_red[32];
@@ -383,15 +469,20 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
 
     /* warm start: residual at the current velocities, keep the previous
        step's accumulated k only where the residual is positive */
-    for (int i = tid; i < nfi; i += nthr) {
-        const float r = dfsph_residual<DIV>(P, A, i, nf, dt);
-        if (DIV) kws[i] = r > 0.0f ? kws[i] / dt : 0.0f;
-        else kws[i] = r > P.rho0 ? kws[i] / ts2 : 0.0f;
-    }
+    for_particles<TPP>(nfi, [&](int i, int sub, bool valid) {
+        const float r = dfsph_residual_lanes<DIV, TPP>(P, A, i, sub, valid, nf, dt);
+        if (valid && sub == 0) {
+            if (DIV) kws[i] = r > 0.0f ? kws[i] / dt : 0.0f;
+            else kws[i] = r > P.rho0 ? kws[i] / ts2 : 0.0f;
+        }
+    });
     if (!grid_barrier(st)) return;
-    for (int i = tid; i < nfi; i += nthr) dfsph_correct(P, A, kws, i, nf, dt);
+    for_particles<TPP>(nfi, [&](int i, int sub, bool valid) { dfsph_correct_lanes<TPP>(P, A, kws, i, sub, valid, nf, dt); });
     if (!grid_barrier(st)) return;
-    for (int i = tid; i < nfi; i += nthr) kws[i] = 0.0f;
+    /* same particle-to-lane mapping as the accumulation below (no barrier between) */
+    for_particles<TPP>(nfi, [&](int i, int sub, bool valid) {
+        if (valid && sub == 0) kws[i] = 0.0f;
+    });
 
     const double limit = DIV ? (double)(P.eta_v / dt) : (double)P.eta;
     const unsigned min_it = DIV ? P.min_it_v : P.min_it;
@@ -402,8 +493,9 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
     double avg = 0.0;
     while ((avg > limit || it < min_it) && it < max_it) {
         double local = 0.0;
-        for (int i = tid; i < nfi; i += nthr) {
-            const float r = dfsph_residual<DIV>(P, A, i, nf, dt);
+        for_particles<TPP>(nfi, [&](int i, int sub, bool valid) {
+            const float r = dfsph_residual_lanes<DIV, TPP>(P, A, i, sub, valid, nf, dt);
+            if (!valid || sub != 0) return;
             float k;
             if (DIV) {
                 k = r * A.alpha[i] / (dt * A.rho[i]);
@@ -414,12 +506,12 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
             }
             A.k[i] = k;
             kws[i] += k;
-        }
+        });
         const double bs = block_sum(local, s_red);
         if (threadIdx.x == 0) atomicAdd(&A.accum[it], bs);
         if (!grid_barrier(st)) return;
         avg = *(volatile double*)&A.accum[it] / (double)nfi;
-        for (int i = tid; i < nfi; i += nthr) dfsph_correct(P, A, A.k, i, nf, dt);
+        for_particles<TPP>(nfi, [&](int i, int sub, bool valid) { dfsph_correct_lanes<TPP>(P, A, A.k, i, sub, valid, nf, dt); });
         if (!grid_barrier(st)) return;
         ++it;
     }
@@ -809,7 +901,18 @@ void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, int bloc
     }
 }
 
-int persistent_grid(bool pcisph, bool divergence, bool batch, int occ)
+/* k_dfsph_solve instance for (divergence, blocks per SM, lanes per particle) */
+static const void* dfsph_solve_fn(bool divergence, int occ, int tpp)
+{
+#define SPH_SOLVE_FN(D, O)                                                                          \
+    (tpp == 4 ? (const void*)k_dfsph_solve<D, O, 4>                                                 \
+              : tpp == 2 ? (const void*)k_dfsph_solve<D, O, 2> : (const void*)k_dfsph_solve<D, O, 1>)
+    if (divergence) return occ == 4 ? SPH_SOLVE_FN(true, 4) : SPH_SOLVE_FN(true, 8);
+    return occ == 4 ? SPH_SOLVE_FN(false, 4) : SPH_SOLVE_FN(false, 8);
+#undef SPH_SOLVE_FN
+}
+
+int persistent_grid(bool pcisph, bool divergence, bool batch, int occ, int tpp)
 {
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
@@ -817,8 +920,7 @@ int persistent_grid(bool pcisph, bool divergence, bool batch, int occ)
     const void* fn = pcisph ? (const void*)k_pcisph_solve
                      : batch ? (divergence ? (const void*)k_dfsph_solve_batch<true>
                                            : (const void*)k_dfsph_solve_batch<false>)
-                             : occ == 4 ? (divergence ? (const void*)k_dfsph_solve<true, 4> : (const void*)k_dfsph_solve<false, 4>)
-                                        : (divergence ? (const void*)k_dfsph_solve<true, 8> : (const void*)k_dfsph_solve<false, 8>);
+                             : dfsph_solve_fn(divergence, occ, tpp);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolverBlock, 0) != cudaSuccess) return 0;
     return per_sm * sms;
 }
@@ -831,13 +933,12 @@ static int coop_launch(const void* fn, const SimParams& P, const DeviceArrays& A
     return (int)cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kSolverBlock), args, 0, s);
 }
 
-int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, int occ, cudaStream_t s)
+int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, int occ, int tpp,
+                       cudaStream_t s)
 {
-    const int need = blocks_for(P.nf > 0 ? P.nf : 1, kSolverBlock);
+    const int need = blocks_for((long long)(P.nf > 0 ? P.nf : 1) * tpp, kSolverBlock);
     const int g = grid < need ? grid : need;
-    const void* fn = occ == 4 ? (divergence ? (const void*)k_dfsph_solve<true, 4> : (const void*)k_dfsph_solve<false, 4>)
-                              : (divergence ? (const void*)k_dfsph_solve<true, 8> : (const void*)k_dfsph_solve<false, 8>);
-    return coop_launch(fn, P, A, g > 0 ? g : 1, s);
+    return coop_launch(dfsph_solve_fn(divergence, occ, tpp), P, A, g > 0 ? g : 1, s);
 }
 
 int launch_dfsph_solve_batch(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s)

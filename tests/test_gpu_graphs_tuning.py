@@ -62,24 +62,34 @@ def test_graph_replay_odd_chunks(method):
 
 def test_options_round_trip_and_reject_bad_values():
     sim = small_sim(S.DFSPH)
-    defaults = {api.OPT_CUDA_GRAPHS: 1, api.OPT_CELL_ORDER: 0, api.OPT_SOLVER_OCCUPANCY: 8, api.OPT_PASS_BLOCK: 256}
+    defaults = {api.OPT_CUDA_GRAPHS: 1, api.OPT_CELL_ORDER: 0, api.OPT_SOLVER_OCCUPANCY: 8, api.OPT_PASS_BLOCK: 256,
+                api.OPT_SOLVER_LANES: 2}
     for k, v in defaults.items():
         assert sim.get_option(k) == v
-    for opt, bad in [(api.OPT_CELL_ORDER, 2), (api.OPT_SOLVER_OCCUPANCY, 6), (api.OPT_PASS_BLOCK, 64), (99, 0)]:
+    for opt, bad in [(api.OPT_CELL_ORDER, 2), (api.OPT_SOLVER_OCCUPANCY, 6), (api.OPT_PASS_BLOCK, 64),
+                     (api.OPT_SOLVER_LANES, 3), (99, 0)]:
         with pytest.raises(SphError):
             sim.set_option(opt, bad)
     sim.set_option(api.OPT_SOLVER_OCCUPANCY, 4)
     sim.set_option(api.OPT_PASS_BLOCK, 128)
+    sim.set_option(api.OPT_SOLVER_LANES, 4)
     assert sim.get_option(api.OPT_SOLVER_OCCUPANCY) == 4 and sim.get_option(api.OPT_PASS_BLOCK) == 128
+    assert sim.get_option(api.OPT_SOLVER_LANES) == 4
     sim.step(4)
     sim.close()
 
 
 @pytest.mark.parametrize("method", METHODS)
-def test_launch_shape_does_not_change_results(method):
-    (x0, v0, r0), t0, _ = run(method, 8)
-    (x1, v1, r1), t1, _ = run(method, 8, [(api.OPT_SOLVER_OCCUPANCY, 4), (api.OPT_PASS_BLOCK, 128)])
+@pytest.mark.parametrize("lanes", [1, 2, 4])
+def test_launch_shape_does_not_change_results(method, lanes):
+    """Launch shape changes no WCSPH/PCISPH bit; in DFSPH the FP64 residual
+    order and, with several lanes per particle, the FP32 summation order of
+    the solver passes change, within rounding."""
+    (x0, v0, r0), t0, s0 = run(method, 8)
+    (x1, v1, r1), t1, s1 = run(method, 8, [(api.OPT_SOLVER_OCCUPANCY, 4), (api.OPT_PASS_BLOCK, 128),
+                                           (api.OPT_SOLVER_LANES, lanes)])
     assert t0 == t1
+    assert s0["total_iterations"] == s1["total_iterations"]
     if method == S.WCSPH:
         assert np.array_equal(x0, x1) and np.array_equal(v0, v1)
     else:
@@ -123,6 +133,8 @@ def test_autotune_leaves_state_untouched(method, tmp_path):
     cache = tmp_path / "tune.json"
     cfg = sim.autotune(trial_steps=2, cache_path=str(cache))
     assert cfg["cell_order"] in (0, 1) and cfg["solver_occupancy"] in (4, 8) and cfg["pass_block"] in (128, 256)
+    assert cfg["solver_lanes"] in (1, 2, 4)
+    assert sim.get_option(api.OPT_SOLVER_LANES) == cfg["solver_lanes"]
     assert sim.get_option(api.OPT_CELL_ORDER) == cfg["cell_order"]
     assert sim.get_option(api.OPT_SOLVER_OCCUPANCY) == cfg["solver_occupancy"]
     assert sim.get_option(api.OPT_PASS_BLOCK) == cfg["pass_block"]
@@ -140,7 +152,8 @@ def test_autotune_leaves_state_untouched(method, tmp_path):
     np.testing.assert_allclose(sim.state()[0], x_ref, rtol=0, atol=atol)
     # the cache now holds the choice, and a second context reuses it
     table = json.loads(cache.read_text())
-    assert len(table) == 1 and list(table.values())[0] == [cfg["cell_order"], cfg["solver_occupancy"], cfg["pass_block"]]
+    assert len(table) == 1 and list(table.values())[0] == [cfg["cell_order"], cfg["solver_occupancy"],
+                                                            cfg["pass_block"], cfg["solver_lanes"]]
     other = small_sim(method)
     assert other.autotune(trial_steps=2, cache_path=str(cache)) == cfg
     assert len(json.loads(cache.read_text())) == 1
