@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(256, 4) k_adj_forces(SimParams P, AdjointArray
         float xrx = 0.0f, xry = 0.0f, xrz = 0.0f, vrx = 0.0f, vry = 0.0f, vrz = 0.0f;
         const unsigned nF = J.cnt_f[i];
         for (unsigned kk = 0; kk < nF; ++kk) {
-            const unsigned j = J.nbr_f[kk * nf + i];
+            const unsigned j = list_at(J.nbr_f, kk, nf, i);
             const float4 xj = J.pos[j];
             float rx, ry, rz, s, rl, inv_rl, f, g;
             pair_of(xi, xj, rx, ry, rz, s, rl, inv_rl);
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(256, 4) k_adj_forces(SimParams P, AdjointArray
         }
         const unsigned nB = J.cnt_b[i];
         for (unsigned kk = 0; kk < nB; ++kk) {
-            const float4 xb = J.bpos[J.nbr_b[kk * nf + i]];
+            const float4 xb = J.bpos[list_at(J.nbr_b, kk, nf, i)];
             float rx, ry, rz, s, rl, inv_rl, f, g;
             pair_of(xi, xb, rx, ry, rz, s, rl, inv_rl);
             cs_grad_fg(rl, inv_rl, P, f, g);
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(256, 6) k_adj_density(SimParams P, AdjointArra
     float sx = 0.0f, sy = 0.0f, sz = 0.0f;
     const unsigned nF = J.cnt_f[i];
     for (unsigned kk = 0; kk < nF; ++kk) {
-        const unsigned j = J.nbr_f[kk * nf + i];
+        const unsigned j = list_at(J.nbr_f, kk, nf, i);
         float rx, ry, rz, s, rl, inv_rl;
         pair_of(xi, J.pos[j], rx, ry, rz, s, rl, inv_rl);
         const float f = cs_gradf(rl, inv_rl, P);
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(256, 6) k_adj_density(SimParams P, AdjointArra
     }
     const unsigned nB = J.cnt_b[i];
     for (unsigned kk = 0; kk < nB; ++kk) {
-        const float4 xb = J.bpos[J.nbr_b[kk * nf + i]];
+        const float4 xb = J.bpos[list_at(J.nbr_b, kk, nf, i)];
         float rx, ry, rz, s, rl, inv_rl;
         pair_of(xi, xb, rx, ry, rz, s, rl, inv_rl);
         const float c = xb.w * rbi * cs_gradf(rl, inv_rl, P);

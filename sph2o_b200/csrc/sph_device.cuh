@@ -328,6 +328,15 @@ __device__ __forceinline__ bool within_h_exact(float4 a, float4 b, float h)
     return __fsqrt_rn(s) <= h;
 }
 
+/* Entry kk of sorted particle i's neighbour list (column-major). The lists
+   are streamed once per pass and at 1M particles are larger than the L2, so
+   they are loaded with the evict-first hint (ld.global.cs): they must not
+   push out of L2 the particle state that the neighbour gathers read. */
+__device__ __forceinline__ unsigned list_at(const unsigned* list, unsigned kk, size_t nf, int i)
+{
+    return __ldcs(list + kk * nf + i);
+}
+
 /* ---------------------------------------------------------------------- */
 /* Reductions                                                               */
 
@@ -377,27 +386,52 @@ __device__ __forceinline__ float block_max(float v, float* scratch)
 }
 
 /* ---------------------------------------------------------------------- */
-/* Grid-wide barrier for cooperative (co-resident) launches. The wait is
-   bounded: after kSpinLimit polls the block records ERRBIT_TIMEOUT and
-   returns false, and the caller leaves the kernel.                          */
+/* gpu-scope acquire load, acquire-release add and release store (PTX memory
+   model). A barrier built from plain loads and __threadfence() does not stop
+   an SM's L1 from serving lines it cached before the barrier, so values other
+   SMs wrote in between could be read stale; an acquire at gpu scope makes
+   them visible to the acquiring thread, and through bar.sync to its block. */
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v)
+{
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+/* Grid-wide barrier for cooperative (co-resident) launches. Each block's
+   thread 0 arrives with an acquire-release add (releasing its block's
+   writes, ordered by the preceding __syncthreads), the last arrival resets
+   the count and publishes the next generation with a release store, and the
+   waiters spin on an acquire load of the generation: every block sees every
+   other block's writes from before the barrier. The wait is bounded: after
+   kSpinLimit polls the block records ERRBIT_TIMEOUT and returns false, and
+   the caller leaves the kernel. */
 __device__ __forceinline__ bool grid_barrier(DevState* st)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* gen = &st->bar_gen;
-        const unsigned g = *gen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(&st->bar_count, 1u);
+        const unsigned g = ld_acquire_gpu(&st->bar_gen);
+        const unsigned arrived = atom_add_acq_rel_gpu(&st->bar_count, 1u);
         int ok = 1;
         if (arrived == gridDim.x - 1) {
             atomicExch(&st->bar_count, 0u);
-            __threadfence();
-            atomicAdd(&st->bar_gen, 1u);
+            st_release_gpu(&st->bar_gen, g + 1u);
         } else {
             unsigned long long spins = 0;
-            while (*gen == g) {
+            while (ld_acquire_gpu(&st->bar_gen) == g) {
                 __nanosleep(256);
                 if (++spins > kSpinLimit) {
                     atomicOr(&st->err, ERRBIT_TIMEOUT);
@@ -406,8 +440,7 @@ __device__ __forceinline__ bool grid_barrier(DevState* st)
                 }
             }
         }
-        __threadfence();
-        s_ok = ok && ((*(volatile int*)&st->err & ERRBIT_TIMEOUT) == 0);
+        s_ok = ok && ((ld_acquire_gpu(reinterpret_cast<const unsigned*>(&st->err)) & ERRBIT_TIMEOUT) == 0);
     }
     __syncthreads();
     return s_ok != 0;

@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
             const float dx = xi.x - xq.x, dy = xi.y - xq.y, dz = xi.z - xq.z;
             const float d2 = dx * dx + dy * dy + dz * dz;
             if (d2 < lo2 || (d2 <= hi2 && within_h_exact(xi, xq, P.h))) {
-                if (nF < P.capF) nbr_f[(size_t)nF * nf + i] = q;
+                if (nF < P.capF) __stcs(nbr_f + (size_t)nF * nf + i, q);
                 ++nF;
             }
         }
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
             const unsigned bs = bcell_start[c], be = bcell_start[c + 1];
             for (unsigned q = bs; q < be; ++q) {
                 if (within_h_exact(xi, bpos[q], P.h)) {
-                    if (nB < P.capB) nbr_b[(size_t)nB * nf + i] = q;
+                    if (nB < P.capB) __stcs(nbr_b + (size_t)nB * nf + i, q);
                     ++nB;
                 }
             }

@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
     float rho = 0.0f, sgx = 0.0f, sgy = 0.0f, sgz = 0.0f, ssq = 0.0f;
     const unsigned nF = A.cnt_f[i];
     for (unsigned kk = 0; kk < nF; ++kk) {
-        const unsigned j = A.nbr_f[kk * nf + i];
+        const unsigned j = list_at(A.nbr_f, kk, nf, i);
         const float4 xj = A.pos[j];
         rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(dist2_exact(xi, xj), P)));
         if (ALPHA) {
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
     }
     const unsigned nB = A.cnt_b[i];
     for (unsigned kk = 0; kk < nB; ++kk) {
-        const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
+        const float4 xb = A.bpos[list_at(A.nbr_b, kk, nf, i)];
         rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(dist2_exact(xi, xb), P)));
         if (ALPHA) {
             const Pair p = make_pair(xi, xb);
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(256, 8) k_normals(SimParams P, DeviceArrays A)
     float nx = 0.0f, ny = 0.0f, nz = 0.0f;
     const unsigned nF = A.cnt_f[i];
     for (unsigned kk = 0; kk < nF; ++kk) {
-        const unsigned j = A.nbr_f[kk * nf + i];
+        const unsigned j = list_at(A.nbr_f, kk, nf, i);
         const Pair p = make_pair(xi, A.pos[j]);
         const float f = (P.mass / A.rho[j]) * cs_gradf(p.rl, p.inv_rl, P);
         nx += f * p.rx; ny += f * p.ry; nz += f * p.rz;
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
         const float eps_h2 = 0.01f * P.h2;
         float svx = 0.0f, svy = 0.0f, svz = 0.0f; /* standard viscosity sum */
         for (unsigned kk = 0; kk < nF; ++kk) {
-            const unsigned j = A.nbr_f[kk * nf + i];
+            const unsigned j = list_at(A.nbr_f, kk, nf, i);
             const float4 xj = A.pos[j];
             const Pair p = make_pair(xi, xj);
             const float rho_j = A.rho[j];
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
         if (pressure || bvisc || (np && P.adh_on)) {
             float bvx = 0.0f, bvy = 0.0f, bvz = 0.0f;
             for (unsigned kk = 0; kk < nB; ++kk) {
-                const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
+                const float4 xb = A.bpos[list_at(A.nbr_b, kk, nf, i)];
                 const Pair p = make_pair(xi, xb);
                 const float psi = xb.w;
                 const float f = cs_gradf(p.rl, p.inv_rl, P);
@@ -269,8 +269,10 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
 /* DFSPH pieces                                                             */
 
 /* Sum of the residual terms of particle i over the neighbour-list entries
-   sub, sub + TPP, ... (fluid, then boundary). */
-template <bool DIV, int TPP>
+   sub, sub + TPP, ... (fluid, then boundary). The fluid loop issues the
+   gathers of U entries before using any of them (more loads in flight per
+   lane) and adds the terms in list order, so U changes no bit. */
+template <bool DIV, int TPP, int U = 1>
 __device__ __forceinline__ float dfsph_residual_part(const SimParams& P, const DeviceArrays& A, int i, int sub,
                                                      size_t nf)
 {
@@ -278,15 +280,33 @@ __device__ __forceinline__ float dfsph_residual_part(const SimParams& P, const D
     const float4 vi = A.vel[i];
     float sum = 0.0f;
     const unsigned nF = A.cnt_f[i], nB = A.cnt_b[i];
-    for (unsigned kk = sub; kk < nF; kk += TPP) {
-        const unsigned j = A.nbr_f[kk * nf + i];
+    unsigned kk = sub;
+    for (; kk + (U - 1) * TPP < nF; kk += U * TPP) {
+        unsigned jj[U];
+        float4 xj[U], vj[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) jj[u] = list_at(A.nbr_f, kk + u * TPP, nf, i);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            xj[u] = A.pos[jj[u]];
+            vj[u] = A.vel[jj[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const Pair p = make_pair(xi, xj[u]);
+            const float f = cs_gradf(p.rl, p.inv_rl, P);
+            sum += P.mass * (f * (((vi.x - vj[u].x) * p.rx + (vi.y - vj[u].y) * p.ry) + (vi.z - vj[u].z) * p.rz));
+        }
+    }
+    for (; kk < nF; kk += TPP) {
+        const unsigned j = list_at(A.nbr_f, kk, nf, i);
         const Pair p = make_pair(xi, A.pos[j]);
         const float4 vj = A.vel[j];
         const float f = cs_gradf(p.rl, p.inv_rl, P);
         sum += P.mass * (f * (((vi.x - vj.x) * p.rx + (vi.y - vj.y) * p.ry) + (vi.z - vj.z) * p.rz));
     }
     for (unsigned kk = sub; kk < nB; kk += TPP) {
-        const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
+        const float4 xb = A.bpos[list_at(A.nbr_b, kk, nf, i)];
         const Pair p = make_pair(xi, xb);
         const float f = cs_gradf(p.rl, p.inv_rl, P);
         sum += xb.w * (f * ((vi.x * p.rx + vi.y * p.ry) + vi.z * p.rz));
@@ -320,18 +340,42 @@ __device__ __forceinline__ float dfsph_residual(const SimParams& P, const Device
 }
 
 /* Partial sums over list entries sub, sub + TPP, ... of
-   sum_j m (k_i + k_j) gradW  (+ boundary with k_i). */
-template <int TPP>
-__device__ __forceinline__ void dfsph_correct_part(const SimParams& P, const DeviceArrays& A,
-                                                   const float* __restrict__ K, int i, int sub, size_t nf,
-                                                   float& sx, float& sy, float& sz)
+   sum_j m (k_i + k_j) gradW  (+ boundary with k_i), the fluid gathers issued
+   U at a time as in dfsph_residual_part. K is written inside the same
+   persistent kernel (before a grid barrier), so it is a plain pointer: a
+   read-only (non-coherent) load path would be wrong for it. */
+template <int TPP, int U = 1>
+__device__ __forceinline__ void dfsph_correct_part(const SimParams& P, const DeviceArrays& A, const float* K, int i,
+                                                   int sub, size_t nf, float& sx, float& sy, float& sz)
 {
     const float4 xi = A.pos[i];
     const float ki = K[i];
     sx = sy = sz = 0.0f;
     const unsigned nF = A.cnt_f[i];
-    for (unsigned kk = sub; kk < nF; kk += TPP) {
-        const unsigned j = A.nbr_f[kk * nf + i];
+    unsigned kk = sub;
+    for (; kk + (U - 1) * TPP < nF; kk += U * TPP) {
+        unsigned jj[U];
+        float kj[U];
+        float4 xj[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) jj[u] = list_at(A.nbr_f, kk + u * TPP, nf, i);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            kj[u] = K[jj[u]];
+            xj[u] = A.pos[jj[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const float ks = ki + kj[u];
+            if (fabsf(ks) > P.eps) {
+                const Pair p = make_pair(xi, xj[u]);
+                const float c = P.mass * ks * cs_gradf(p.rl, p.inv_rl, P);
+                sx += c * p.rx; sy += c * p.ry; sz += c * p.rz;
+            }
+        }
+    }
+    for (; kk < nF; kk += TPP) {
+        const unsigned j = list_at(A.nbr_f, kk, nf, i);
         const float ks = ki + K[j];
         if (fabsf(ks) > P.eps) {
             const Pair p = make_pair(xi, A.pos[j]);
@@ -342,7 +386,7 @@ __device__ __forceinline__ void dfsph_correct_part(const SimParams& P, const Dev
     if (fabsf(ki) > P.eps) {
         const unsigned nB = A.cnt_b[i];
         for (unsigned kk = sub; kk < nB; kk += TPP) {
-            const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
+            const float4 xb = A.bpos[list_at(A.nbr_b, kk, nf, i)];
             const Pair p = make_pair(xi, xb);
             const float c = xb.w * ki * cs_gradf(p.rl, p.inv_rl, P);
             sx += c * p.rx; sy += c * p.ry; sz += c * p.rz;
@@ -360,8 +404,8 @@ __device__ __forceinline__ void dfsph_apply(const DeviceArrays& A, int i, float 
 }
 
 /* v_i -= dt * sum_j m (k_i + k_j) gradW  (+ boundary with k_i) */
-__device__ __forceinline__ void dfsph_correct(const SimParams& P, const DeviceArrays& A, const float* __restrict__ K,
-                                              int i, size_t nf, float dt)
+__device__ __forceinline__ void dfsph_correct(const SimParams& P, const DeviceArrays& A, const float* K, int i,
+                                              size_t nf, float dt)
 {
     float sx, sy, sz;
     dfsph_correct_part<1>(P, A, K, i, 0, nf, sx, sy, sz);
@@ -394,23 +438,22 @@ __device__ __forceinline__ void for_particles(int n, F&& f)
 }
 
 /* residual of particle i with its list split over TPP lanes (all lanes call) */
-template <bool DIV, int TPP>
+template <bool DIV, int TPP, int U>
 __device__ __forceinline__ float dfsph_residual_lanes(const SimParams& P, const DeviceArrays& A, int i, int sub,
                                                       bool valid, size_t nf, float dt)
 {
-    float part = valid ? dfsph_residual_part<DIV, TPP>(P, A, i, sub, nf) : 0.0f;
+    float part = valid ? dfsph_residual_part<DIV, TPP, U>(P, A, i, sub, nf) : 0.0f;
     if (TPP > 1) part = lane_group_sum<TPP>(part);
     return valid ? dfsph_residual_finish<DIV>(P, A, i, part, dt) : 0.0f;
 }
 
 /* velocity correction of particle i with its list split over TPP lanes */
-template <int TPP>
-__device__ __forceinline__ void dfsph_correct_lanes(const SimParams& P, const DeviceArrays& A,
-                                                    const float* __restrict__ K, int i, int sub, bool valid,
-                                                    size_t nf, float dt)
+template <int TPP, int U>
+__device__ __forceinline__ void dfsph_correct_lanes(const SimParams& P, const DeviceArrays& A, const float* K, int i,
+                                                    int sub, bool valid, size_t nf, float dt)
 {
     float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-    if (valid) dfsph_correct_part<TPP>(P, A, K, i, sub, nf, sx, sy, sz);
+    if (valid) dfsph_correct_part<TPP, U>(P, A, K, i, sub, nf, sx, sy, sz);
     if (TPP > 1) {
         sx = lane_group_sum<TPP>(sx);
         sy = lane_group_sum<TPP>(sy);
@@ -423,10 +466,14 @@ __device__ __forceinline__ void dfsph_correct_lanes(const SimParams& P, const De
    bound by the latency of dependent neighbour gathers and full occupancy
    hides most of it; 4 (64 registers, no spills) is the autotuner's other
    candidate. TPP lanes share a particle in the neighbour passes (1, 2 or 4):
-   more gathers in flight per particle, fewer particles per warp. */
+   more gathers in flight per particle, fewer particles per warp. Each lane
+   issues U gathers before using them: 2 within the 32 registers of the
+   8-block variant, 4 in the 64-register variant (measured best for each on
+   the 1M-particle scene). */
 template <bool DIV, int OCC, int TPP>
 __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, DeviceArrays A)
 {
+    constexpr int U = OCC == 4 ? 4 : 2;
     __shared__ double s_red[32];
     DevState* st = A.st;
     const int nfi = P.nf;
@@ -470,14 +517,14 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
     /* warm start: residual at the current velocities, keep the previous
        step's accumulated k only where the residual is positive */
     for_particles<TPP>(nfi, [&](int i, int sub, bool valid) {
-        const float r = dfsph_residual_lanes<DIV, TPP>(P, A, i, sub, valid, nf, dt);
+        const float r = dfsph_residual_lanes<DIV, TPP, U>(P, A, i, sub, valid, nf, dt);
         if (valid && sub == 0) {
             if (DIV) kws[i] = r > 0.0f ? kws[i] / dt : 0.0f;
             else kws[i] = r > P.rho0 ? kws[i] / ts2 : 0.0f;
         }
     });
     if (!grid_barrier(st)) return;
-    for_particles<TPP>(nfi, [&](int i, int sub, bool valid) { dfsph_correct_lanes<TPP>(P, A, kws, i, sub, valid, nf, dt); });
+    for_particles<TPP>(nfi, [&](int i, int sub, bool valid) { dfsph_correct_lanes<TPP, U>(P, A, kws, i, sub, valid, nf, dt); });
     if (!grid_barrier(st)) return;
     /* same particle-to-lane mapping as the accumulation below (no barrier between) */
     for_particles<TPP>(nfi, [&](int i, int sub, bool valid) {
@@ -494,7 +541,7 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
     while ((avg > limit || it < min_it) && it < max_it) {
         double local = 0.0;
         for_particles<TPP>(nfi, [&](int i, int sub, bool valid) {
-            const float r = dfsph_residual_lanes<DIV, TPP>(P, A, i, sub, valid, nf, dt);
+            const float r = dfsph_residual_lanes<DIV, TPP, U>(P, A, i, sub, valid, nf, dt);
             if (!valid || sub != 0) return;
             float k;
             if (DIV) {
@@ -511,7 +558,7 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
         if (threadIdx.x == 0) atomicAdd(&A.accum[it], bs);
         if (!grid_barrier(st)) return;
         avg = *(volatile double*)&A.accum[it] / (double)nfi;
-        for_particles<TPP>(nfi, [&](int i, int sub, bool valid) { dfsph_correct_lanes<TPP>(P, A, A.k, i, sub, valid, nf, dt); });
+        for_particles<TPP>(nfi, [&](int i, int sub, bool valid) { dfsph_correct_lanes<TPP, U>(P, A, A.k, i, sub, valid, nf, dt); });
         if (!grid_barrier(st)) return;
         ++it;
     }
@@ -804,7 +851,7 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
             float ax = 0.0f, ay = 0.0f, az = 0.0f;
             const unsigned nF = A.cnt_f[i], nB = A.cnt_b[i];
             for (unsigned kk = 0; kk < nF; ++kk) {
-                const unsigned j = A.nbr_f[kk * nf + i];
+                const unsigned j = list_at(A.nbr_f, kk, nf, i);
                 const float4 xj = A.pos[j];
                 const float rho_j = A.rho[j];
                 float gx, gy, gz;
@@ -815,7 +862,7 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
                 az = __fsub_rn(az, __fmul_rn(c, gz));
             }
             for (unsigned kk = 0; kk < nB; ++kk) {
-                const float4 xb = A.bpos[A.nbr_b[kk * nf + i]];
+                const float4 xb = A.bpos[list_at(A.nbr_b, kk, nf, i)];
                 float gx, gy, gz;
                 cs_gradW_exact(__fsub_rn(xi.x, xb.x), __fsub_rn(xi.y, xb.y), __fsub_rn(xi.z, xb.z), P, gx, gy, gz);
                 const float c = __fmul_rn(xb.w, dpi);
