@@ -124,8 +124,14 @@ struct sph_ctx {
         int cap_seg = 0, cap_every = 0;
         float4 *ck_pos = nullptr, *ck_vel = nullptr;   /* checkpoints: state entering each segment */
         unsigned* ck_orig = nullptr;
-        float4 *sl_pos = nullptr, *sl_vel = nullptr;   /* state entering each step of one segment */
-        unsigned* sl_orig = nullptr;
+        float4 *sl_pos = nullptr, *sl_vel = nullptr;   /* per step of one segment: its input state, or */
+        unsigned* sl_orig = nullptr;                   /* its sorted state when lists are kept       */
+        /* per step of one segment, when they fit kAdjointListBudget: neighbour
+           lists, densities and pressures of the recomputed step */
+        bool keep_lists = false;
+        unsigned sl_capF = 0, sl_capB = 0;
+        unsigned *sl_nbr_f = nullptr, *sl_cnt_f = nullptr, *sl_nbr_b = nullptr, *sl_cnt_b = nullptr;
+        float *sl_rho = nullptr, *sl_press = nullptr;
         float4 *fin_pos = nullptr, *fin_vel = nullptr; /* state after the forward run */
         unsigned* fin_orig = nullptr;
         DevState *st0 = nullptr, *st1 = nullptr;       /* solver state at the start / end of the run */
@@ -1579,10 +1585,16 @@ int sph_debug_neighbors(sph_ctx* c, unsigned* f_offsets, unsigned* f_index, size
    segment, last first, the segment is recomputed from its checkpoint with
    the state entering each step kept (the recomputation is bit-identical:
    the sort ranks particles inside a cell by id and every pass is a
-   gather), then each step's neighbour search and densities are redone and
-   its adjoint kernels run, newest step first. Memory: (nsteps / K + K)
-   states of 36 B per particle for K = ckpt_every. */
+   gather), then each step's adjoint kernels run, newest step first. While
+   the recomputation keeps every step's neighbour lists, densities and
+   pressures (when K steps of them fit kAdjointListBudget) the backward step
+   is the three adjoint kernels alone; otherwise each step's neighbour search
+   and densities are redone from its kept input state. Memory: (nsteps / K +
+   K) states of 36 B per particle for K = ckpt_every, plus K x (capacity x 8
+   + 16) B per particle of lists and densities when they are kept. */
 namespace {
+
+constexpr size_t kAdjointListBudget = size_t(8) << 30;
 
 void dfree(sph_ctx* c, void* p)
 {
@@ -1625,12 +1637,28 @@ int adj_reserve(sph_ctx* c, int nseg, int every)
         AALLOC(ck_pos, (size_t)nseg * nf); AALLOC(ck_vel, (size_t)nseg * nf); AALLOC(ck_orig, (size_t)nseg * nf);
         a.cap_seg = nseg;
     }
-    if (every > a.cap_every) {
+    const size_t list_bytes = (size_t)every * nf * ((size_t)(c->P.capF + c->P.capB) * 4 + 16);
+    const bool keep = list_bytes <= kAdjointListBudget;
+    if (every > a.cap_every || keep != a.keep_lists ||
+        (keep && (a.sl_capF != c->P.capF || a.sl_capB != c->P.capB))) {
         drop_graphs(c);
-        dfree(c, a.sl_pos); dfree(c, a.sl_vel); dfree(c, a.sl_orig);
-        a.sl_pos = a.sl_vel = nullptr; a.sl_orig = nullptr; a.cap_every = 0;
-        AALLOC(sl_pos, (size_t)every * nf); AALLOC(sl_vel, (size_t)every * nf); AALLOC(sl_orig, (size_t)every * nf);
-        a.cap_every = every;
+        for (void* p : {(void*)a.sl_pos, (void*)a.sl_vel, (void*)a.sl_orig, (void*)a.sl_nbr_f, (void*)a.sl_cnt_f,
+                        (void*)a.sl_nbr_b, (void*)a.sl_cnt_b, (void*)a.sl_rho, (void*)a.sl_press})
+            dfree(c, p);
+        a.sl_pos = a.sl_vel = nullptr; a.sl_orig = a.sl_nbr_f = a.sl_cnt_f = a.sl_nbr_b = a.sl_cnt_b = nullptr;
+        a.sl_rho = a.sl_press = nullptr;
+        const int cap = std::max(every, a.cap_every);
+        a.cap_every = 0;
+        AALLOC(sl_pos, (size_t)cap * nf); AALLOC(sl_vel, (size_t)cap * nf); AALLOC(sl_orig, (size_t)cap * nf);
+        if (keep) {
+            AALLOC(sl_nbr_f, (size_t)cap * c->P.capF * nf); AALLOC(sl_nbr_b, (size_t)cap * c->P.capB * nf);
+            AALLOC(sl_cnt_f, (size_t)cap * nf); AALLOC(sl_cnt_b, (size_t)cap * nf);
+            AALLOC(sl_rho, (size_t)cap * nf); AALLOC(sl_press, (size_t)cap * nf);
+            a.sl_capF = c->P.capF;
+            a.sl_capB = c->P.capB;
+        }
+        a.keep_lists = keep;
+        a.cap_every = cap;
     }
 #undef AALLOC
     return SPH_OK;
@@ -1667,13 +1695,49 @@ AdjointArrays adj_arrays(sph_ctx* c)
     return J;
 }
 
+/* Adjoint arrays of step n of the segment from the kept lists and state. */
+AdjointArrays adj_arrays_kept(sph_ctx* c, int n)
+{
+    auto& a = c->adj;
+    const size_t nf = c->nf;
+    AdjointArrays J = adj_arrays(c);
+    J.pos = a.sl_pos + n * nf; J.vel = a.sl_vel + n * nf; J.orig = a.sl_orig + n * nf;
+    J.rho = a.sl_rho + n * nf; J.press = a.sl_press + n * nf;
+    J.nbr_f = a.sl_nbr_f + (size_t)n * a.sl_capF * nf; J.nbr_b = a.sl_nbr_b + (size_t)n * a.sl_capB * nf;
+    J.cnt_f = a.sl_cnt_f + n * nf; J.cnt_b = a.sl_cnt_b + n * nf;
+    return J;
+}
+
 /* Recompute a segment of len steps from the state in the current buffers,
-   keeping each step's input, then run the adjoint of its steps, last first. */
+   keeping what each step's adjoint needs, then run the adjoint of its
+   steps, last first. */
 int adj_segment_body(sph_ctx* c, int len)
 {
     auto& a = c->adj;
     const size_t nf = c->nf;
     int rc;
+    if (a.keep_lists) {
+        for (int n = 0; n < len; ++n) {
+            /* the step builds its lists and densities straight into slot n */
+            unsigned *lf = c->nbr_f, *cf = c->cnt_f, *lb = c->nbr_b, *cb = c->cnt_b;
+            float *rho = c->rho, *press = c->press;
+            c->nbr_f = a.sl_nbr_f + (size_t)n * a.sl_capF * nf; c->nbr_b = a.sl_nbr_b + (size_t)n * a.sl_capB * nf;
+            c->cnt_f = a.sl_cnt_f + n * nf; c->cnt_b = a.sl_cnt_b + n * nf;
+            c->rho = a.sl_rho + n * nf; c->press = a.sl_press + n * nf;
+            rc = step_wcsph(c);
+            c->nbr_f = lf; c->cnt_f = cf; c->nbr_b = lb; c->cnt_b = cb; c->rho = rho; c->press = press;
+            if (rc != SPH_OK) return rc;
+            /* the sorted state the step's forces read (integrated into the spare buffers) */
+            if ((rc = copy_state(c, a.sl_pos + n * nf, a.sl_vel + n * nf, a.sl_orig + n * nf, c->pos2, c->vel2, c->orig)) != SPH_OK)
+                return rc;
+        }
+        for (int n = len - 1; n >= 0; --n) {
+            launch_adjoint_step(c->P, adj_arrays_kept(c, n), c->stream);
+            c->launches += 3;
+        }
+        c->lists_valid = false;
+        return check_launch(c, "adjoint segment");
+    }
     for (int n = 0; n < len; ++n) {
         if ((rc = copy_state(c, a.sl_pos + n * nf, a.sl_vel + n * nf, a.sl_orig + n * nf, c->pos, c->vel, c->orig)) != SPH_OK)
             return rc;

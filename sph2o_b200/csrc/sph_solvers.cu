@@ -54,6 +54,30 @@ __device__ __forceinline__ Pair make_pair(float4 a, float4 b)
     return p;
 }
 
+/* Calls f(j, x_j) for the fluid neighbours of sorted particle i in list
+   order, issuing the list loads and position gathers of U entries before the
+   first of them is used (more loads in flight per thread; same order, so the
+   sums it feeds are unchanged). */
+template <int U, typename F>
+__device__ __forceinline__ void for_fluid_neighbors(const DeviceArrays& A, int i, size_t nf, unsigned n, F&& f)
+{
+    unsigned kk = 0;
+    for (; kk + U <= n; kk += U) {
+        unsigned jj[U];
+        float4 xj[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) jj[u] = list_at(A.nbr_f, kk + u, nf, i);
+#pragma unroll
+        for (int u = 0; u < U; ++u) xj[u] = A.pos[jj[u]];
+#pragma unroll
+        for (int u = 0; u < U; ++u) f(jj[u], xj[u]);
+    }
+    for (; kk < n; ++kk) {
+        const unsigned j = list_at(A.nbr_f, kk, nf, i);
+        f(j, A.pos[j]);
+    }
+}
+
 /* ---------------------------------------------------------------------- */
 
 template <bool ALPHA, bool EOS>
@@ -65,9 +89,7 @@ __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
     const float4 xi = A.pos[i];
     float rho = 0.0f, sgx = 0.0f, sgy = 0.0f, sgz = 0.0f, ssq = 0.0f;
     const unsigned nF = A.cnt_f[i];
-    for (unsigned kk = 0; kk < nF; ++kk) {
-        const unsigned j = list_at(A.nbr_f, kk, nf, i);
-        const float4 xj = A.pos[j];
+    for_fluid_neighbors<2>(A, i, nf, nF, [&](unsigned, const float4& xj) {
         rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(dist2_exact(xi, xj), P)));
         if (ALPHA) {
             const Pair p = make_pair(xi, xj);
@@ -76,7 +98,7 @@ __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
             sgx += gx; sgy += gy; sgz += gz;
             ssq += (gx * gx + gy * gy) + gz * gz;
         }
-    }
+    });
     const unsigned nB = A.cnt_b[i];
     for (unsigned kk = 0; kk < nB; ++kk) {
         const float4 xb = A.bpos[list_at(A.nbr_b, kk, nf, i)];
@@ -140,9 +162,7 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
         const float4 ni = st_on ? A.normal[i] : make_float4(0, 0, 0, 0);
         const float eps_h2 = 0.01f * P.h2;
         float svx = 0.0f, svy = 0.0f, svz = 0.0f; /* standard viscosity sum */
-        for (unsigned kk = 0; kk < nF; ++kk) {
-            const unsigned j = list_at(A.nbr_f, kk, nf, i);
-            const float4 xj = A.pos[j];
+        for_fluid_neighbors<2>(A, i, nf, nF, [&](unsigned j, const float4& xj) {
             const Pair p = make_pair(xi, xj);
             const float rho_j = A.rho[j];
             const float f = cs_gradf(p.rl, p.inv_rl, P);
@@ -174,7 +194,7 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
                 ay += kij * (-c * p.ry - P.st * (ni.y - nj.y));
                 az += kij * (-c * p.rz - P.st * (ni.z - nj.z));
             }
-        }
+        });
         if (vm == 0) {
             const float c = visc_c / rho_i;
             ax += svx * c; ay += svy * c; az += svz * c;
