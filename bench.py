@@ -77,8 +77,9 @@ def workloads():
     }
 
 
-def batched_run(steps, warmup, method=0, count=256, loop_steps=None):
-    """Batched scenes vs the plain per-scene GPU loop on the same scenes.
+def batched_run(steps, warmup, method=0, count=256, loop_steps=None, indices=None):
+    """Batched scenes vs the plain per-scene GPU loop on the same scenes
+    (`indices`: this rank's shard of the `count` scenes, default all).
     Returns particle-steps/s of both (device events for the batch, wall clock
     for both in the ratio) and the scene statistics."""
     import time as _t
@@ -89,6 +90,8 @@ def batched_run(steps, warmup, method=0, count=256, loop_steps=None):
     from sph2o_b200.api import Batch, Scene, Simulation
 
     dicts = S.batched_scenes(count, method=method)
+    if indices is not None:
+        dicts = [dicts[s] for s in indices]
     scs = [Scene.from_dict(d) for d in dicts]
     batch = Batch(scs)
     total = batch.nf
@@ -116,7 +119,7 @@ def batched_run(steps, warmup, method=0, count=256, loop_steps=None):
     batched = total * steps / (dev_ms / 1e3)
     batched_wall = total * steps / wall_batch
     loop = total * loop_steps / wall_loop
-    return {"scenes": count, "fluid_particles": total, "steps": steps, "value": batched,
+    return {"scenes": len(scs), "fluid_particles": total, "steps": steps, "value": batched,
             "value_wall": batched_wall, "per_scene_loop": loop, "speedup_vs_loop": batched_wall / loop,
             "ms_per_step": dev_ms / steps, "mean_iterations": st["total_iterations"] / max(1, steps) / count,
             "method": "WCSPH" if method == 0 else "DFSPH"}
@@ -446,8 +449,28 @@ def main():
     secondary = None
     if not args.no_secondary:
         secondary = {"adjoint_wcsph_32k": adjoint_run()}
+        # independent scenes shard across ranks: each steps its own subset as
+        # one batch; only the timing and particle totals are reduced
+        from sph2o_b200 import scenes as S
+        from sph2o_b200.sharding import scene_cost, shard_for_rank
+        costs = [scene_cost(p["dims"][0] * p["dims"][1] * p["dims"][2])
+                 for p in S.batched_scene_params(args.batch_scenes)]
+        shard = shard_for_rank(costs, world, rank)
         for m, name in ((0, "batched_wcsph_256"), (2, "batched_dfsph_256")):
-            secondary[name] = batched_run(50, 3, method=m, count=args.batch_scenes)
+            res = batched_run(50, 3, method=m, count=args.batch_scenes, indices=shard)
+            if world > 1:
+                red = torch.tensor([res["ms_per_step"], float(res["fluid_particles"])], dtype=torch.float64,
+                                   device="cuda")
+                tmax = red[:1].clone()
+                dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+                tot = red[1:].clone()
+                dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+                res["value"] = float(tot.item()) / (float(tmax.item()) / 1e3)
+                res["fluid_particles_all_ranks"] = int(tot.item())
+                res["ms_per_step_max_rank"] = float(tmax.item())
+            res["sharding"] = {"ranks": world, "scenes_this_rank": len(shard),
+                               "rule": "greedy longest-processing-time on fluid particles, no collective on particle data"}
+            secondary[name] = res
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
