@@ -184,7 +184,10 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
         if (P.nb > 0) {
             const unsigned bs = bcell_start[c], be = bcell_start[c + 1];
             for (unsigned q = bs; q < be; ++q) {
-                if (within_h_exact(xi, bpos[q], P.h)) {
+                const float4 xb = bpos[q];
+                const float dx = xi.x - xb.x, dy = xi.y - xb.y, dz = xi.z - xb.z;
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 < lo2 || (d2 <= hi2 && within_h_exact(xi, xb, P.h))) {
                     if (nB < P.capB) __stcs(nbr_b + (size_t)nB * nf + i, q);
                     ++nB;
                 }
