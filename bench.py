@@ -63,6 +63,12 @@ BYTES = {
 }
 
 
+# DRAM traffic of the density-solver launch per neighbour pass on the 1M
+# workload, measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of a
+# 3-iteration launch = 1.952 GB over 8 passes; profiles/dfsph_1m_pass_kernels.md).
+NCU_DENSITY_SOLVE_BYTES_PER_PASS = 1.952e9 / 8.0
+
+
 def workloads():
     from sph2o_b200 import scenes as S
     return {
@@ -397,8 +403,13 @@ def main():
     nb_active = nb  # upper bound of boundary particles with a fluid neighbour
     algo = bytes_per_launch(dom, nf, nb_active, it_for)
     achieved = algo / (avg_ms / 1e3) / 1e9
+    traffic, traffic_note = None, None
+    if dom == "density_solve" and name == "double_dam_break_dfsph_1m":
+        traffic = NCU_DENSITY_SOLVE_BYTES_PER_PASS * (2 + 2 * it_for)
+        traffic_note = ("ncu DRAM bytes per neighbour pass of this kernel on this workload (1.952 GB per "
+                        "3-iteration launch, profiles/dfsph_1m_pass_kernels.md) x the timed window's passes")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": dom, "peak_kind": f"of {peak_kind}",
+                "traffic": traffic, "traffic_note": traffic_note, "kernel": dom, "peak_kind": f"of {peak_kind}",
                 "algorithmic_bytes_per_launch": algo, "avg_launch_ms": avg_ms}
 
     # End to end through the C ABI with host buffers, over the same window:
