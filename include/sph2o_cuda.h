@@ -130,6 +130,37 @@ int sph_set_fluid(sph_ctx* ctx, unsigned n, const float* xyz, const float* v);
    order (AkinciBoundaryObject::r, AkinciBoundaryObject.cpp:36-95). */
 int sph_set_boundary(sph_ctx* ctx, unsigned n, const float* xyz);
 
+/* Particle emitter of the fluid model (Emitter.h:10-33; scene keys of
+   SceneLoader.cpp:128-143). An emitter holds num_particles inactive
+   particles; every time the simulated time reaches its next emission time
+   (start_time, then + spacing * 1.105 * 2r / velocity after each emission)
+   it activates one group -- a square lattice of width x height at spacing 2r
+   or concentric rings out to radius width -- moving at `velocity` along the
+   emitter's local z, rotated by `rotation` and placed at `position`
+   (Emitter.cpp:25-128). */
+enum sph_emitter_type { SPH_EMITTER_SQUARE = 0, SPH_EMITTER_CIRCLE = 1 };
+typedef struct sph_emitter_desc {
+    int type;                       /* sph_emitter_type */
+    unsigned num_particles;         /* particles it emits in total */
+    float position[3];
+    float rotation[4];              /* quaternion w, x, y, z (glm::quat order) */
+    float velocity;                 /* emission speed (> 0) */
+    float start_time;
+    float width, height;            /* square: width x height; circle: radius width */
+    float spacing;                  /* emission period factor */
+} sph_emitter_desc;
+
+/* Replaces FluidObject::addEmitter (FluidObject.cpp:177-194): adds an
+   emitter before sph_init; the context's fluid grows by num_particles
+   inactive particles (sph_num_fluid counts them, as FluidObject::getSize
+   does). Single scenes only. */
+int sph_add_emitter(sph_ctx* ctx, const sph_emitter_desc* emitter);
+
+/* Active fluid particles (FluidObject::getNumActiveParticles): the first n
+   of the caller order; emitted particles take the next caller ids in
+   emission order, as in the reference. Waits for queued work. */
+int sph_get_num_active(sph_ctx* ctx, unsigned* n);
+
 /* Replaces SPHSimulation::init (SPHSimulation.cpp:117-126): kernel constants,
    masses m = rho0 (2r)^3, boundary volumes (AkinciBoundaryObject::computeVolume,
    AkinciBoundaryObject.cpp:10-34) and the solver's init (DFSPHSolver::init,
@@ -180,11 +211,13 @@ int sph_get_option(const sph_ctx* ctx, int option, int* value);
 int sph_autotune(sph_ctx* ctx, int trial_steps, const char* cache_path, int* config);
 
 /* Fluid state in the caller's particle order. Any pointer may be NULL.
-   rho is FluidObject::density as SPH2O leaves it after a step. */
+   rho is FluidObject::density as SPH2O leaves it after a step. Arrays hold
+   sph_num_fluid particles; with emitters the inactive ones read as zero. */
 int sph_get_state(sph_ctx* ctx, float* xyz, float* v, float* rho);
 
 /* Replace positions/velocities (same order as sph_set_fluid) between steps;
-   replaces writes through FluidObject::getPosition/getVelocity. */
+   replaces writes through FluidObject::getPosition/getVelocity. With
+   emitters only the active particles are taken from the arrays. */
 int sph_set_state(sph_ctx* ctx, const float* xyz, const float* v);
 
 /* Akinci boundary volumes V_b in the sph_set_boundary order. */
@@ -346,12 +379,15 @@ int sph_scene_parse(const char* json_text, sph_scene** out);
 int sph_scene_get_desc(const sph_scene* s, sph_scene_desc* out);
 unsigned sph_scene_num_fluid(const sph_scene* s);
 unsigned sph_scene_num_boundary(const sph_scene* s);
+/* Emitters of the scene's fluid model ("emitters" key, SceneLoader.cpp:109-143). */
+unsigned sph_scene_num_emitters(const sph_scene* s);
+int sph_scene_get_emitter(const sph_scene* s, unsigned k, sph_emitter_desc* out);
 int sph_scene_get_fluid(const sph_scene* s, float* xyz, float* v);
 int sph_scene_get_boundary(const sph_scene* s, float* xyz);
 const char* sph_scene_error(void);
 void sph_scene_free(sph_scene* s);
 
-/* create + set_fluid + set_boundary + init from a loaded scene. */
+/* create + set_fluid + set_boundary + add_emitter + init from a loaded scene. */
 int sph_create_from_scene(const sph_scene* s, sph_ctx** out);
 
 #ifdef __cplusplus

@@ -401,9 +401,10 @@ int main(int argc, char** argv)
     }
     /* per-step: time, dt, iterations, iterationsV, solver avg error, solver avg div error,
        centroid xyz, kinetic energy, mean density error */
-    std::vector<double> stats;
+    std::vector<double> stats, active;
     for (int s = 0; s < o.steps; ++s) {
         sim->step();
+        active.push_back((double)fo->getNumActiveParticles());
         double agg[5];
         aggregates(sim, agg);
         double avg = 0, avgv = 0, itv = 0;
@@ -419,6 +420,7 @@ int main(int argc, char** argv)
         stats.insert(stats.end(), row, row + 11);
     }
     w.put("step_stats", stats, {(uint64_t)o.steps, 11});
+    w.put("active", active, {(uint64_t)o.steps});
     w.put("pos", fluid_vec3(fo, 0), {n, 3});
     w.put("vel", fluid_vec3(fo, 1), {n, 3});
     w.put("density", fluid_density(fo), {n});

@@ -51,6 +51,14 @@ class SceneDesc(C.Structure):
     ]
 
 
+class EmitterDesc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int), ("num_particles", C.c_uint), ("position", C.c_float * 3), ("rotation", C.c_float * 4),
+        ("velocity", C.c_float), ("start_time", C.c_float), ("width", C.c_float), ("height", C.c_float),
+        ("spacing", C.c_float),
+    ]
+
+
 class StepStats(C.Structure):
     _fields_ = [
         ("time", C.c_double), ("avg_density_error", C.c_double), ("avg_divergence_error", C.c_double),
@@ -125,6 +133,10 @@ def lib():
         "sph_scene_error": (C.c_char_p, []),
         "sph_scene_free": (None, [P]),
         "sph_create_from_scene": (I, [P, C.POINTER(P)]),
+        "sph_add_emitter": (I, [P, C.POINTER(EmitterDesc)]),
+        "sph_get_num_active": (I, [P, C.POINTER(U)]),
+        "sph_scene_num_emitters": (U, [P]),
+        "sph_scene_get_emitter": (I, [P, U, C.POINTER(EmitterDesc)]),
         "sph_wcsph_forward": (I, [P, I, I, F, C.POINTER(C.c_double)]),
         "sph_wcsph_backward": (I, [P, F, F, F]),
         "sph_wcsph_grad_x0": (I, [P, F]),
@@ -186,6 +198,14 @@ class Scene:
         lib().sph_scene_get_fluid(self._h, _fptr(x), _fptr(v))
         return x, v
 
+    def emitters(self):
+        out = []
+        for k in range(lib().sph_scene_num_emitters(self._h)):
+            e = EmitterDesc()
+            lib().sph_scene_get_emitter(self._h, k, C.byref(e))
+            out.append(e)
+        return out
+
     def boundary(self):
         n = lib().sph_scene_num_boundary(self._h)
         b = np.zeros((n, 3), np.float32)
@@ -207,7 +227,7 @@ class Scene:
 class Simulation:
     """One GPU simulation context (sph_ctx)."""
 
-    def __init__(self, desc: SceneDesc, fluid, boundary, vel=None):
+    def __init__(self, desc: SceneDesc, fluid, boundary, vel=None, emitters=()):
         L = lib()
         h = C.c_void_p()
         rc = L.sph_create(C.byref(desc), C.byref(h))
@@ -220,13 +240,20 @@ class Simulation:
         b = np.ascontiguousarray(boundary, np.float32).reshape(-1, 3)
         self._check(L.sph_set_fluid(h, x.shape[0], _fptr(x), _fptr(v)))
         self._check(L.sph_set_boundary(h, b.shape[0], _fptr(b)))
+        for e in emitters:
+            self._check(L.sph_add_emitter(h, C.byref(e)))
         self._check(L.sph_init(h))
-        self.nf, self.nb = x.shape[0], b.shape[0]
+        self.nf, self.nb = L.sph_num_fluid(h), b.shape[0]
 
     @classmethod
     def from_scene(cls, scene: Scene, vel=None):
         x, v = scene.fluid()
-        return cls(scene.desc(), x, scene.boundary(), v if vel is None else vel)
+        return cls(scene.desc(), x, scene.boundary(), v if vel is None else vel, emitters=scene.emitters())
+
+    def num_active(self):
+        n = C.c_uint()
+        self._check(lib().sph_get_num_active(self._h, C.byref(n)))
+        return n.value
 
     def _check(self, rc):
         if rc != SPH_OK:

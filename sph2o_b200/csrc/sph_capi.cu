@@ -118,6 +118,13 @@ struct sph_ctx {
     float4* pos_base = nullptr;
     unsigned* orig_base = nullptr;
     float* kws_base = nullptr;
+    /* emitters of a single scene (sph_add_emitter): descriptions, the fluid
+       particles active at init, the device table and group offsets */
+    std::vector<sph_emitter_desc> emitters;
+    unsigned n_init = 0;
+    EmitterState* d_emit = nullptr;
+    float4* d_group = nullptr;
+    EmitterState* snap_emit = nullptr;
     /* WCSPH adjoint (sph_wcsph_forward / sph_wcsph_backward) */
     struct Adjoint {
         int nsteps = 0, every = 0, nseg = 0;
@@ -273,12 +280,48 @@ void derive_params(sph_ctx* c)
     P.pcisph_delta = -1.0f / (beta * (-dot_sg - ssq));
 }
 
+/* Emitter::buildCircleGroup / buildSquareGroup (Emitter.cpp:25-80) with the
+   reference's types: float arithmetic, with sin, cos and floor in double
+   (the overloads its translation unit resolves to for float arguments) and
+   the result rounded to float. Appends x, y, z triples to out. */
+void emitter_group(const sph_emitter_desc& e, float radius, std::vector<float>& out)
+{
+    const float dist = 2.0f * radius;
+    if (e.type == SPH_EMITTER_CIRCLE) {
+        const unsigned levels = (unsigned)std::floor((double)((e.width - 0.5f * dist) / dist));
+        out.insert(out.end(), {0.0f, 0.0f, 0.0f});
+        for (unsigned i = 0; i < levels; ++i) {
+            const float rad = (float)(i + 1) * dist;
+            const float l = (float)(2.0 * M_PI) * rad;
+            const unsigned parts = (unsigned)std::floor((double)(l / dist));
+            const float inc = (float)(2.0 * M_PI) / (float)parts;
+            for (unsigned k = 0; k < parts; ++k) {
+                const float angle = (float)k * inc;
+                out.push_back((float)((double)rad * std::sin((double)angle)));
+                out.push_back((float)((double)rad * std::cos((double)angle)));
+                out.push_back(0.0f);
+            }
+        }
+    } else {
+        const unsigned nx = (unsigned)std::floor((double)(e.width / dist));
+        const unsigned ny = (unsigned)(e.height / dist);
+        const float rw = (float)(nx - 1) * dist, rh = (float)(ny - 1) * dist;
+        for (unsigned i = 0; i < nx; ++i)
+            for (unsigned j = 0; j < ny; ++j) {
+                out.push_back((float)((double)rw * 0.5 - (double)((float)i * dist)));
+                out.push_back((float)((double)rh * 0.5 - (double)((float)j * dist)));
+                out.push_back(0.0f);
+            }
+    }
+}
+
 DeviceArrays arrays(sph_ctx* c)
 {
     DeviceArrays A{};
     A.pos = c->pos; A.vel = c->vel; A.pos_alt = c->pos2; A.vel_alt = c->vel2;
     A.acc = c->acc; A.normal = c->normal; A.predr = c->predr; A.pacc = c->pacc;
     A.rho = c->rho; A.alpha = c->alpha; A.k = c->k; A.kws = c->kws; A.kvws = c->kvws; A.press = c->press;
+    A.orig_w = c->orig;
     A.cell_start = c->cell_start; A.cell_sorted = c->cell_sorted;
     A.bpos = c->bpos; A.bcell_start = c->bcell_start;
     A.nbr_f = c->nbr_f; A.cnt_f = c->cnt_f; A.nbr_b = c->nbr_b; A.cnt_b = c->cnt_b;
@@ -361,6 +404,7 @@ int alloc_lists(sph_ctx* c)
 int neighbor_search(sph_ctx* c)
 {
     GatherSet g{};
+    if (c->P.dynamic) g.n_dev = &c->st->n_active;
     g.orig_out = c->orig2;
     g.cell_out = c->cell_sorted;
     g.v4_in[0] = c->pos; g.v4_out[0] = c->pos2;
@@ -390,6 +434,14 @@ int neighbor_search(sph_ctx* c)
     return check_launch(c, "neighbour search");
 }
 
+/* Emission of the due emitter groups (a no-op without emitters). */
+void emit(sph_ctx* c, bool advance_time)
+{
+    if (!c->P.dynamic) return;
+    launch_emit(c->P, arrays(c), c->d_emit, c->d_group, (int)c->emitters.size(), advance_time, c->stream);
+    c->launches += 1;
+}
+
 int zero_accum(sph_ctx* c)
 {
     CUDA_TRY(c, cudaMemsetAsync(c->accum, 0, c->accum_len * sizeof(double), c->stream));
@@ -408,6 +460,7 @@ int step_wcsph(sph_ctx* c)
     std::swap(c->pos, c->pos2);
     std::swap(c->vel, c->vel2);
     c->lists_valid = false;
+    emit(c, true); /* WCSPHSolver.cpp:75: emission, then t += dt */
     return check_launch(c, "wcsph step");
 }
 
@@ -423,7 +476,8 @@ int step_pcisph(sph_ctx* c)
     int e;
     { Phase ph(c, SPH_PROF_PRESSURE_SOLVE, 1); e = launch_pcisph_solve(c->P, A, c->grid_pcisph, c->stream); }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("pcisph solver launch: ") + cudaGetErrorString((cudaError_t)e));
-    c->lists_valid = true;
+    c->lists_valid = !c->P.dynamic;
+    emit(c, true); /* PCISPHSolver.cpp:77: emission, then t += dt */
     return check_launch(c, "pcisph step");
 }
 
@@ -448,6 +502,7 @@ int step_dfsph(sph_ctx* c)
                        : launch_dfsph_solve(c->P, A, false, solve_grid(c, false), c->solver_occ, c->solver_tpp, c->stream);
     }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph density solver launch: ") + cudaGetErrorString((cudaError_t)e));
+    emit(c, false); /* DFSPHSolver.cpp:72: after the position update, before the neighbour search */
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     A = arrays(c);
     { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, true, false, c->pass_block, c->stream); }
@@ -467,6 +522,17 @@ int read_state(sph_ctx* c, DevState* out)
     CUDA_TRY(c, cudaMemcpyAsync(c->st_host, c->st, sizeof(DevState), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     *out = *c->st_host;
+    return SPH_OK;
+}
+
+/* Active fluid particles (reads the device state; waits for queued work). */
+int active_count(sph_ctx* c, unsigned* n)
+{
+    if (!c->P.dynamic) { *n = c->nf; return SPH_OK; }
+    DevState s{};
+    const int rc = read_state(c, &s);
+    if (rc != SPH_OK) return rc;
+    *n = s.n_active;
     return SPH_OK;
 }
 
@@ -687,6 +753,26 @@ int sph_set_boundary(sph_ctx* c, unsigned n, const float* xyz)
     return SPH_OK;
 }
 
+int sph_add_emitter(sph_ctx* c, const sph_emitter_desc* e)
+{
+    if (!c || !e) return SPH_ERR_ARG;
+    if (c->nscenes) return fail(c, SPH_ERR_ARG, "emitters apply to single scenes, not to batches");
+    if (c->initialized) return fail(c, SPH_ERR_STATE, "sph_add_emitter after sph_init");
+    if (e->type != SPH_EMITTER_SQUARE && e->type != SPH_EMITTER_CIRCLE)
+        return fail(c, SPH_ERR_ARG, "emitter type must be 0 (square) or 1 (circle)");
+    if (!(e->velocity > 0.0f) || !(e->spacing > 0.0f)) return fail(c, SPH_ERR_ARG, "emitter velocity and spacing must be > 0");
+    if ((unsigned long long)c->nf + e->num_particles > (1ull << 31)) return fail(c, SPH_ERR_CAPACITY, "too many particles");
+    c->emitters.push_back(*e);
+    return SPH_OK;
+}
+
+int sph_get_num_active(sph_ctx* c, unsigned* n)
+{
+    if (!c || !n) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_get_num_active before sph_init");
+    return active_count(c, n);
+}
+
 int sph_init(sph_ctx* c)
 {
     if (!c) return SPH_ERR_ARG;
@@ -709,6 +795,32 @@ int sph_init(sph_ctx* c)
         }
         c->nf = c->fsplit.back();
         c->nb = c->bsplit.back();
+    }
+    /* emitters: their particles are allocated inactive after the blocks */
+    c->n_init = c->nf;
+    std::vector<float> groups;
+    std::vector<EmitterState> etab;
+    if (!c->emitters.empty()) {
+        unsigned extra = 0;
+        for (const sph_emitter_desc& e : c->emitters) {
+            EmitterState es{};
+            es.px = e.position[0]; es.py = e.position[1]; es.pz = e.position[2];
+            es.qw = e.rotation[0]; es.qx = e.rotation[1]; es.qy = e.rotation[2]; es.qz = e.rotation[3];
+            es.v = e.velocity;
+            es.next = e.start_time;
+            /* nextTimeEmit += spacing * 1.105 * dist / v (Emitter.cpp:124) */
+            es.period = e.spacing * 1.105f * (2.0f * c->desc.particle_radius) / e.velocity;
+            es.remaining = e.num_particles;
+            es.group_begin = (unsigned)(groups.size() / 3);
+            emitter_group(e, c->desc.particle_radius, groups);
+            es.group_count = (unsigned)(groups.size() / 3) - es.group_begin;
+            etab.push_back(es);
+            extra += e.num_particles;
+        }
+        c->nf += extra;
+        c->h_fluid.resize(3ull * c->nf, 0.0f);
+        c->h_vel.resize(3ull * c->nf, 0.0f);
+        P.dynamic = 1;
     }
     P.nf = (int)c->nf;
     P.nb = (int)c->nb;
@@ -765,8 +877,14 @@ int sph_init(sph_ctx* c)
                 hi[k] = std::max(hi[k], (double)a[i + k]);
             }
     };
-    grow(c->h_fluid);
+    grow(std::vector<float>(c->h_fluid.begin(), c->h_fluid.begin() + 3ull * c->n_init));
     grow(c->h_bound);
+    /* emitted particles start around their emitter */
+    for (const sph_emitter_desc& e : c->emitters) {
+        const float ext = std::max(e.width, e.height) + 4.0f * P.h;
+        grow({e.position[0] - ext, e.position[1] - ext, e.position[2] - ext, e.position[0] + ext, e.position[1] + ext,
+              e.position[2] + ext});
+    }
     const sph_scene_desc& d = c->desc;
     if (d.domain_min[0] != 0 || d.domain_min[1] != 0 || d.domain_min[2] != 0 || d.domain_max[0] != 0 ||
         d.domain_max[1] != 0 || d.domain_max[2] != 0)
@@ -884,9 +1002,24 @@ int sph_init(sph_ctx* c)
         CUDA_TRY(c, cudaMemsetAsync(c->bcell_start, 0, ((size_t)P.ncells + 1) * sizeof(unsigned), c->stream));
     }
 
+    if (!etab.empty()) {
+        if ((rc = dalloc(c, &c->d_emit, etab.size())) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->snap_emit, etab.size())) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->d_group, std::max<size_t>(groups.size() / 3, 1))) != SPH_OK) return rc;
+        std::vector<float4> g4(groups.size() / 3);
+        for (size_t k = 0; k < g4.size(); ++k) g4[k] = make_float4(groups[3 * k], groups[3 * k + 1], groups[3 * k + 2], 0.0f);
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_emit, etab.data(), etab.size() * sizeof(EmitterState), cudaMemcpyHostToDevice,
+                                    c->stream));
+        if (!g4.empty())
+            CUDA_TRY(c, cudaMemcpyAsync(c->d_group, g4.data(), g4.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                                        c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    }
+
     /* solver state */
     DevState s0{};
     s0.dt = c->desc.time_step;
+    s0.n_active = c->n_init;
     CUDA_TRY(c, cudaMemcpyAsync(c->st, &s0, sizeof s0, cudaMemcpyHostToDevice, c->stream));
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     if (c->desc.simulation_method == SPH_DFSPH) {
@@ -990,16 +1123,23 @@ int sph_get_state(sph_ctx* c, float* xyz, float* v, float* rho)
     if (!c) return SPH_ERR_ARG;
     if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_get_state before sph_init");
     const size_t nf = c->nf;
+    unsigned na = 0;
+    int rc = active_count(c, &na);
+    if (rc != SPH_OK) return rc;
     float* tmp = nullptr;
     CUDA_TRY(c, cudaMallocAsync((void**)&tmp, 3 * nf * sizeof(float), c->stream));
-    int rc = SPH_OK;
+    if (na < nf) CUDA_TRY(c, cudaMemsetAsync(tmp, 0, 3 * nf * sizeof(float), c->stream)); /* inactive: 0 */
     auto copy_out = [&](float* dst, size_t count) -> int {
         CUDA_TRY(c, cudaMemcpyAsync(dst, tmp, count * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
         return SPH_OK;
     };
-    if (xyz) { launch_unsort_v4((int)nf, c->orig, c->pos, tmp, c->stream); rc = copy_out(xyz, 3 * nf); }
-    if (rc == SPH_OK && v) { launch_unsort_v4((int)nf, c->orig, c->vel, tmp, c->stream); rc = copy_out(v, 3 * nf); }
-    if (rc == SPH_OK && rho) { launch_unsort_f((int)nf, c->orig, c->rho, tmp, c->stream); rc = copy_out(rho, nf); }
+    if (xyz) { launch_unsort_v4((int)na, c->orig, c->pos, tmp, c->stream); rc = copy_out(xyz, 3 * nf); }
+    if (rc == SPH_OK && v) { launch_unsort_v4((int)na, c->orig, c->vel, tmp, c->stream); rc = copy_out(v, 3 * nf); }
+    if (rc == SPH_OK && rho) {
+        if (na < nf) CUDA_TRY(c, cudaMemsetAsync(tmp, 0, nf * sizeof(float), c->stream));
+        launch_unsort_f((int)na, c->orig, c->rho, tmp, c->stream);
+        rc = copy_out(rho, nf);
+    }
     cudaFreeAsync(tmp, c->stream);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     if (rc != SPH_OK) return rc;
@@ -1011,15 +1151,18 @@ int sph_set_state(sph_ctx* c, const float* xyz, const float* v)
     if (!c) return SPH_ERR_ARG;
     if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_set_state before sph_init");
     const size_t nf = c->nf;
+    unsigned na = 0;
+    int rc0 = active_count(c, &na);
+    if (rc0 != SPH_OK) return rc0;
     float* tmp = nullptr;
     CUDA_TRY(c, cudaMallocAsync((void**)&tmp, 3 * nf * sizeof(float), c->stream));
     if (xyz) {
         CUDA_TRY(c, cudaMemcpyAsync(tmp, xyz, 3 * nf * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-        launch_sort_v3((int)nf, c->orig, tmp, c->pos, c->stream);
+        launch_sort_v3((int)na, c->orig, tmp, c->pos, c->stream);
     }
     if (v) {
         CUDA_TRY(c, cudaMemcpyAsync(tmp, v, 3 * nf * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-        launch_sort_v3((int)nf, c->orig, tmp, c->vel, c->stream);
+        launch_sort_v3((int)na, c->orig, tmp, c->vel, c->stream);
     }
     cudaFreeAsync(tmp, c->stream);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -1128,28 +1271,31 @@ int sph_compute_phase(sph_ctx* c, int phase, float* out)
     if (phase < SPH_PHASE_DENSITY || phase > SPH_PHASE_PRESSURE_ACC) return fail(c, SPH_ERR_ARG, "unknown phase");
     if ((phase == SPH_PHASE_PRESSURE || phase == SPH_PHASE_PRESSURE_ACC) && c->desc.simulation_method != SPH_WCSPH)
         return fail(c, SPH_ERR_ARG, "pressure phases exist for WCSPH only");
-    int rc = neighbor_search(c);
+    unsigned na = 0;
+    int rc = active_count(c, &na);
     if (rc != SPH_OK) return rc;
+    if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     DeviceArrays A = arrays(c);
     const bool eos = phase == SPH_PHASE_PRESSURE || phase == SPH_PHASE_PRESSURE_ACC;
     launch_density(c->P, A, phase == SPH_PHASE_ALPHA || c->desc.simulation_method == SPH_DFSPH, eos, c->pass_block, c->stream);
     const size_t nf = c->nf;
     float* tmp = nullptr;
     CUDA_TRY(c, cudaMallocAsync((void**)&tmp, 3 * nf * sizeof(float), c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(tmp, 0, 3 * nf * sizeof(float), c->stream)); /* inactive particles read 0 */
     size_t count = nf;
     switch (phase) {
-    case SPH_PHASE_DENSITY: launch_unsort_f((int)nf, c->orig, c->rho, tmp, c->stream); break;
-    case SPH_PHASE_ALPHA: launch_unsort_f((int)nf, c->orig, c->alpha, tmp, c->stream); break;
-    case SPH_PHASE_PRESSURE: launch_unsort_f((int)nf, c->orig, c->press, tmp, c->stream); break;
+    case SPH_PHASE_DENSITY: launch_unsort_f((int)na, c->orig, c->rho, tmp, c->stream); break;
+    case SPH_PHASE_ALPHA: launch_unsort_f((int)na, c->orig, c->alpha, tmp, c->stream); break;
+    case SPH_PHASE_PRESSURE: launch_unsort_f((int)na, c->orig, c->press, tmp, c->stream); break;
     case SPH_PHASE_NONPRESSURE_ACC:
         if (c->P.st_on) launch_normals(c->P, A, c->pass_block, c->stream);
         launch_forces(c->P, A, FORCE_NP, c->pass_block, c->stream);
-        launch_unsort_v4((int)nf, c->orig, c->acc, tmp, c->stream);
+        launch_unsort_v4((int)na, c->orig, c->acc, tmp, c->stream);
         count = 3 * nf;
         break;
     default:
         launch_forces(c->P, A, FORCE_PRESSURE, c->pass_block, c->stream);
-        launch_unsort_v4((int)nf, c->orig, c->acc, tmp, c->stream);
+        launch_unsort_v4((int)na, c->orig, c->acc, tmp, c->stream);
         count = 3 * nf;
         break;
     }
@@ -1237,6 +1383,7 @@ int snapshot(sph_ctx* c, bool save)
     if ((rc = cp(c->rho, c->snap_rho, nf * sizeof(float))) != SPH_OK) return rc;
     if ((rc = cp(c->st, c->snap_st, sizeof(DevState))) != SPH_OK) return rc;
     if (c->nscenes && (rc = cp(c->d_sst, c->snap_sst, c->nscenes * sizeof(SceneState))) != SPH_OK) return rc;
+    if (c->d_emit && (rc = cp(c->d_emit, c->snap_emit, c->emitters.size() * sizeof(EmitterState))) != SPH_OK) return rc;
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return SPH_OK;
 }
@@ -1556,13 +1703,15 @@ int sph_debug_neighbors(sph_ctx* c, unsigned* f_offsets, unsigned* f_index, size
     DevState s{};
     if ((rc = read_state(c, &s)) != SPH_OK) return rc;
     if (s.err & ERRBIT_OVERFLOW) return fail(c, SPH_ERR_NEIGHBOR_OVERFLOW, "neighbour list capacity exceeded");
-    std::vector<size_t> slot_of(nf);
-    for (size_t i = 0; i < nf; ++i) slot_of[orig[i]] = i;
+    const size_t na = c->P.dynamic ? s.n_active : nf;
+    std::vector<size_t> slot_of(nf, (size_t)-1);
+    for (size_t i = 0; i < na; ++i) slot_of[orig[i]] = i;
     size_t tf = 0, tb = 0;
     for (size_t o = 0; o < nf; ++o) {
         const size_t i = slot_of[o];
         if (f_offsets) f_offsets[o] = (unsigned)tf;
         if (b_offsets) b_offsets[o] = (unsigned)tb;
+        if (i == (size_t)-1) continue; /* inactive (emitter) particle: no neighbours */
         for (unsigned k = 0; k < cntf[i]; ++k, ++tf)
             if (f_index && tf < f_cap) f_index[tf] = orig[nbrf[(size_t)k * nf + i]];
         for (unsigned k = 0; k < cntb[i]; ++k, ++tb)
@@ -1610,6 +1759,7 @@ int adj_supported(sph_ctx* c)
 {
     if (c->nscenes) return fail(c, SPH_ERR_ARG, "the WCSPH adjoint applies to a single scene, not to a batch");
     if (c->desc.simulation_method != SPH_WCSPH) return fail(c, SPH_ERR_ARG, "the adjoint differentiates the WCSPH step only");
+    if (c->P.dynamic) return fail(c, SPH_ERR_ARG, "the WCSPH adjoint does not cover emitters");
     if (c->P.st_on || c->P.adh_on)
         return fail(c, SPH_ERR_ARG, "the WCSPH adjoint covers neither surface tension nor adhesion");
     if (c->P.visc_method != -1 && c->P.visc_method != SPH_VISCOSITY_ARTIFICIAL)

@@ -60,6 +60,7 @@ struct SimParams {
     unsigned ncells;
     unsigned capF, capB;       /* neighbour-list capacity per particle   */
     int cell_order;            /* 0: 4^3 bricks, Morton inside; 1: linear, x fastest */
+    int dynamic;               /* emitters: passes cover DevState::n_active particles, nf is the capacity */
 };
 
 /* Device-resident solver state; read by the host after a step. */
@@ -77,6 +78,34 @@ struct DevState {
     unsigned overflow;
     unsigned bar_count, bar_gen;
     float last_vmax;
+    unsigned n_active;          /* active fluid particles (emitters append to them) */
+};
+
+/* Fluid particles a pass covers: all nf, or with emitters the active prefix
+   (slots [0, n_active) of the sorted arrays; nf stays the list stride). */
+__device__ __forceinline__ int active_n(const SimParams& P, const DevState* st)
+{
+    return P.dynamic ? (int)st->n_active : P.nf;
+}
+
+/* Simulated time advanced as the reference keeps it: a float sum (TimeHelper
+   holds Real time, TimeHelper.h:29, and steps add dt to it). */
+__device__ __forceinline__ double advance_time(double t, float dt)
+{
+    return (double)__fadd_rn((float)t, dt);
+}
+
+/* One particle emitter (Emitter.h:10-33) on the device: pose, speed, the
+   next emission time, what is left to emit and its group of particle
+   offsets in the group table. */
+struct EmitterState {
+    float px, py, pz;           /* position r */
+    float qw, qx, qy, qz;       /* rotation (glm::quat w, x, y, z) */
+    float v;                    /* speed along local z */
+    float next;                 /* nextTimeEmit */
+    float period;               /* spacing * 1.105 * 2r / v, added after each emission */
+    unsigned remaining;         /* numParticles still to emit */
+    unsigned group_begin, group_count;
     unsigned pad;
 };
 

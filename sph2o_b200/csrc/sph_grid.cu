@@ -25,12 +25,12 @@
 
 namespace sph {
 
-__global__ void __launch_bounds__(256) k_ns_count(SimParams P, SceneRef S, int n, const float4* __restrict__ pos,
-                                                  unsigned* __restrict__ cell_count, unsigned* __restrict__ cell_of,
-                                                  unsigned* __restrict__ slot)
+__global__ void __launch_bounds__(256) k_ns_count(SimParams P, SceneRef S, int n, const unsigned* n_dev,
+                                                  const float4* __restrict__ pos, unsigned* __restrict__ cell_count,
+                                                  unsigned* __restrict__ cell_of, unsigned* __restrict__ slot)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= (n_dev ? (int)*n_dev : n)) return;
     const unsigned c = cell_index(pos[i], P.h, grid_for(P, S, (unsigned)i));
     cell_of[i] = c;
     slot[i] = atomicAdd(&cell_count[c], 1u);
@@ -117,14 +117,14 @@ __global__ void __launch_bounds__(1024) k_scan_add(unsigned* __restrict__ start,
     *reinterpret_cast<uint4*>(start + base) = s;
 }
 
-__global__ void __launch_bounds__(256) k_ns_scatter(int n, const unsigned* __restrict__ cell_of,
+__global__ void __launch_bounds__(256) k_ns_scatter(int n, const unsigned* n_dev, const unsigned* __restrict__ cell_of,
                                                     const unsigned* __restrict__ slot,
                                                     const unsigned* __restrict__ cell_start,
                                                     const unsigned* __restrict__ orig,
                                                     unsigned* __restrict__ tmp_key, unsigned* __restrict__ tmp_src)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= (n_dev ? (int)*n_dev : n)) return;
     const unsigned p = cell_start[cell_of[i]] + slot[i];
     tmp_key[p] = orig[i];
     tmp_src[p] = (unsigned)i;
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(256) k_ns_rank_gather(int n, const unsigned* _
                                                         const unsigned* __restrict__ tmp_src, GatherSet g)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
+    if (p >= (g.n_dev ? (int)*g.n_dev : n)) return;
     const unsigned src = tmp_src[p];
     const unsigned c = cell_of[src];
     const unsigned key = tmp_key[p];
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
                                                         DevState* st)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.nf) return;
+    if (i >= active_n(P, st)) return;
     const float4 xi = pos[i];
     const size_t nf = (size_t)P.nf;
     /* a cheap float test settles clear cases; candidates within a relative
@@ -285,12 +285,12 @@ void launch_sort(const SimParams& P, const SceneRef& S, int n, const float4* pos
         cudaMemsetAsync(cell_start, 0, ((size_t)P.ncells + 1) * sizeof(unsigned), s);
         return;
     }
-    k_ns_count<<<blocks_for(n, 256), 256, 0, s>>>(P, S, n, pos_for_keys, cell_count, cell_of, slot);
+    k_ns_count<<<blocks_for(n, 256), 256, 0, s>>>(P, S, n, g.n_dev, pos_for_keys, cell_count, cell_of, slot);
     const int nblk = (int)(P.ncells / 4096);
     k_scan_local<<<nblk, 1024, 0, s>>>(cell_count, cell_start, block_sums);
     k_scan_blocks<<<1, 1024, 0, s>>>(block_sums, nblk, cell_start + P.ncells);
     k_scan_add<<<nblk, 1024, 0, s>>>(cell_start, block_sums);
-    k_ns_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, cell_of, slot, cell_start, orig_in, tmp_key, tmp_src);
+    k_ns_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, g.n_dev, cell_of, slot, cell_start, orig_in, tmp_key, tmp_src);
     k_ns_rank_gather<<<blocks_for(n, 256), 256, 0, s>>>(n, cell_of, cell_start, tmp_key, tmp_src, g);
 }
 

@@ -13,8 +13,11 @@
 
 namespace sph {
 
-/* Arrays moved by the rank/gather step of the sort (NULL entries skipped). */
+/* Arrays moved by the rank/gather step of the sort (NULL entries skipped).
+   n_dev (may be NULL): device count of the particles to sort, read by the
+   kernels in place of n (the fluid's active count when emitters add to it). */
 struct GatherSet {
+    const unsigned* n_dev;
     unsigned* orig_out;
     unsigned* cell_out;
     const float4* v4_in[2];
@@ -47,6 +50,7 @@ struct DeviceArrays {
     const unsigned* cnt_f;
     const unsigned* nbr_b;
     const unsigned* cnt_b;
+    unsigned* orig_w;     /* caller-order ids of the sorted slots (emitters write new ones) */
     double* accum;        /* per-iteration residual accumulators, zeroed per solve */
     DevState* st;
     SceneRef sref;        /* batch scene table (empty for a single scene) */
@@ -92,6 +96,9 @@ int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergenc
 int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s);
 int launch_dfsph_solve_batch(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s);
 int launch_barrier_timeout_probe(DevState* st, cudaStream_t s);
+/* emission of the nemit emitters' due groups (one block); advance: then t += dt */
+void launch_emit(const SimParams& P, const DeviceArrays& A, EmitterState* E, const float4* group, int nemit,
+                 bool advance, cudaStream_t s);
 
 /* sph_adjoint.cu: reverse-mode WCSPH step. Sorted-order arrays of the
    recomputed step (pos .. cnt_b), caller-order adjoint state (xbar, vbar),

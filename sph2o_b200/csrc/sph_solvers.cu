@@ -84,7 +84,7 @@ template <bool ALPHA, bool EOS>
 __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.nf) return;
+    if (i >= active_n(P, A.st)) return;
     const size_t nf = (size_t)P.nf;
     const float4 xi = A.pos[i];
     float rho = 0.0f, sgx = 0.0f, sgy = 0.0f, sgz = 0.0f, ssq = 0.0f;
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
 __global__ void __launch_bounds__(256, 8) k_normals(SimParams P, DeviceArrays A)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.nf) return;
+    if (i >= active_n(P, A.st)) return;
     const size_t nf = (size_t)P.nf;
     const float4 xi = A.pos[i];
     float nx = 0.0f, ny = 0.0f, nz = 0.0f;
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
 {
     __shared__ float s_red[32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool active = i < P.nf;
+    const bool active = i < active_n(P, A.st);
     const size_t nf = (size_t)P.nf;
     /* per-scene coefficients and time step of a batch */
     const unsigned scene = (A.sst && active) ? A.sref.scene_of[i] : 0u;
@@ -250,11 +250,12 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
         }
         if (A.sst) {
             if (active && (unsigned)i == A.sref.scenes[scene].fbegin) {
-                A.sst[scene].time += (double)dt;
+                A.sst[scene].time = advance_time(A.sst[scene].time, dt);
                 A.sst[scene].steps += 1u;
             }
-        } else if (blockIdx.x == 0 && threadIdx.x == 0) {
-            A.st->time += (double)dt;
+        } else if (blockIdx.x == 0 && threadIdx.x == 0 && !P.dynamic) {
+            /* with emitters the step's emission comes first (k_emit advances the time) */
+            A.st->time = advance_time(A.st->time, dt);
             A.st->steps += 1u;
         }
         return;
@@ -496,8 +497,8 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
     constexpr int U = OCC == 4 ? 4 : 2;
     __shared__ double s_red[32];
     DevState* st = A.st;
-    const int nfi = P.nf;
-    const size_t nf = (size_t)nfi;
+    const int nfi = active_n(P, st);
+    const size_t nf = (size_t)P.nf;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthr = gridDim.x * blockDim.x;
 
@@ -610,7 +611,7 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
             st->its_v = it;
             st->avg_div = avg;
             st->sum_its_v += it;
-            st->time += (double)dt;
+            st->time = advance_time(st->time, dt);
             st->steps += 1u;
             st->vmax_bits = 0u;
         }
@@ -785,7 +786,7 @@ __global__ void __launch_bounds__(kSolverBlock, 8) k_dfsph_solve_batch(SimParams
         } else {
             if (min_it == 0u || max_it == 0u) sst[s].its_v = 0u;
             sst[s].sum_its_v += sst[s].its_v;
-            sst[s].time += (double)sst[s].dt;
+            sst[s].time = advance_time(sst[s].time, sst[s].dt);
             sst[s].steps += 1u;
             sst[s].vmax_bits = 0u;
         }
@@ -800,8 +801,8 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
 {
     __shared__ double s_red[32];
     DevState* st = A.st;
-    const int nfi = P.nf;
-    const size_t nf = (size_t)nfi;
+    const int nfi = active_n(P, st);
+    const size_t nf = (size_t)P.nf;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthr = gridDim.x * blockDim.x;
     const float dt = st->dt;
@@ -919,9 +920,104 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
         st->pcisph_avg = avg;
         st->avg_dens = avg;
         st->sum_its += it;
-        st->time += (double)dt;
-        st->steps += 1u;
+        if (!P.dynamic) {
+            /* with emitters the step's emission comes first (k_emit advances the time) */
+            st->time = advance_time(st->time, dt);
+            st->steps += 1u;
+        }
     }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Emitters (Emitter::emitParticles / emitGroup, Emitter.cpp:82-128).       */
+
+/* glm's quat * vec3 (type_quat.inl:347-354) in FP32, operation for
+   operation: uv = cross(q.xyz, v), uuv = cross(q.xyz, uv),
+   v + ((uv * w) + uuv) * 2, cross as in func_geometric.inl:74-77. */
+__device__ __forceinline__ void quat_rotate(const EmitterState& e, float vx, float vy, float vz, float& ox, float& oy,
+                                            float& oz)
+{
+    const float uvx = __fsub_rn(__fmul_rn(e.qy, vz), __fmul_rn(vy, e.qz));
+    const float uvy = __fsub_rn(__fmul_rn(e.qz, vx), __fmul_rn(vz, e.qx));
+    const float uvz = __fsub_rn(__fmul_rn(e.qx, vy), __fmul_rn(vx, e.qy));
+    const float uuvx = __fsub_rn(__fmul_rn(e.qy, uvz), __fmul_rn(uvy, e.qz));
+    const float uuvy = __fsub_rn(__fmul_rn(e.qz, uvx), __fmul_rn(uvz, e.qx));
+    const float uuvz = __fsub_rn(__fmul_rn(e.qx, uvy), __fmul_rn(uvx, e.qy));
+    ox = __fadd_rn(vx, __fmul_rn(__fadd_rn(__fmul_rn(uvx, e.qw), uuvx), 2.0f));
+    oy = __fadd_rn(vy, __fmul_rn(__fadd_rn(__fmul_rn(uvy, e.qw), uuvy), 2.0f));
+    oz = __fadd_rn(vz, __fmul_rn(__fadd_rn(__fmul_rn(uvz, e.qw), uuvz), 2.0f));
+}
+
+/* One block. Emitters in order: one whose next emission time has come
+   (time >= next, the start-of-step time) and that still holds a whole group
+   appends the group after the active particles (slots and caller ids
+   n_active, n_active + 1, ...) with velocity rot (0, 0, v) at
+   rot (g + t (v_z + gravity t)) + r, t = time - next, then its next time
+   moves on by its period. With `advance` (WCSPH, PCISPH, whose step ends
+   with the emission) the time then moves on by dt. */
+__global__ void __launch_bounds__(256) k_emit(SimParams P, DeviceArrays A, EmitterState* E, const float4* group,
+                                              int nemit, int advance)
+{
+    __shared__ unsigned s_n;
+    __shared__ int s_go;
+    __shared__ float s_off;
+    DevState* st = A.st;
+    const float time = (float)st->time;
+    if (threadIdx.x == 0) s_n = st->n_active;
+    __syncthreads();
+    for (int e = 0; e < nemit; ++e) {
+        if (threadIdx.x == 0) {
+            const EmitterState& em = E[e];
+            s_go = time >= em.next && em.group_count <= em.remaining && s_n + em.group_count <= (unsigned)P.nf;
+            s_off = __fsub_rn(time, em.next);
+        }
+        __syncthreads();
+        if (s_go) {
+            const EmitterState em = E[e];
+            const float t = s_off;
+            /* velocity + gravity * t, with velocity = (0, 0, v) */
+            const float wx = __fadd_rn(0.0f, __fmul_rn(P.gx, t));
+            const float wy = __fadd_rn(0.0f, __fmul_rn(P.gy, t));
+            const float wz = __fadd_rn(em.v, __fmul_rn(P.gz, t));
+            float rvx, rvy, rvz;
+            quat_rotate(em, 0.0f, 0.0f, em.v, rvx, rvy, rvz);
+            for (unsigned k = threadIdx.x; k < em.group_count; k += blockDim.x) {
+                const float4 g = group[em.group_begin + k];
+                const float px = __fadd_rn(g.x, __fmul_rn(t, wx));
+                const float py = __fadd_rn(g.y, __fmul_rn(t, wy));
+                const float pz = __fadd_rn(g.z, __fmul_rn(t, wz));
+                float rx, ry, rz;
+                quat_rotate(em, px, py, pz, rx, ry, rz);
+                const unsigned slot = s_n + k;
+                A.pos[slot] = make_float4(__fadd_rn(rx, em.px), __fadd_rn(ry, em.py), __fadd_rn(rz, em.pz), 0.0f);
+                A.vel[slot] = make_float4(rvx, rvy, rvz, 0.0f);
+                A.acc[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                A.orig_w[slot] = slot;
+                if (A.kws) A.kws[slot] = 0.0f;
+                if (A.kvws) A.kvws[slot] = 0.0f;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && s_go) {
+            s_n += E[e].group_count;
+            E[e].remaining -= E[e].group_count;
+            E[e].next = __fadd_rn(E[e].next, E[e].period);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        st->n_active = s_n;
+        if (advance) {
+            st->time = advance_time(st->time, st->dt);
+            st->steps += 1u;
+        }
+    }
+}
+
+void launch_emit(const SimParams& P, const DeviceArrays& A, EmitterState* E, const float4* group, int nemit,
+                 bool advance, cudaStream_t s)
+{
+    k_emit<<<1, 256, 0, s>>>(P, A, E, group, nemit, advance ? 1 : 0);
 }
 
 /* Test kernel: block 1 never arrives, so block 0's wait must run out. */

@@ -16,8 +16,12 @@
  * particles are bit-identical to the reference's. This file is compiled with
  * -ffp-contract=off for that reason.
  *
+ * Emitters ("emitters" of the fluid model, SceneLoader.cpp:109-143) are
+ * read into sph_emitter_desc and handed to the context by
+ * sph_create_from_scene (FluidObject::addEmitter, FluidObject.cpp:177-194).
+ *
  * Not supported (rejected with SPH_ERR_ARG): more than one fluid model,
- * emitters, boundary methods other than Akinci, OBJ "geometry" boundaries.
+ * boundary methods other than Akinci, OBJ "geometry" boundaries.
  */
 #include "../../include/sph2o_cuda.h"
 #include "json_lite.h"
@@ -35,6 +39,7 @@ struct sph_scene {
     std::vector<float> fluid;     /* n*3 */
     std::vector<float> fluid_v;   /* n*3 */
     std::vector<float> boundary;  /* nb*3 */
+    std::vector<sph_emitter_desc> emitters;
     std::string path;
 };
 
@@ -187,7 +192,24 @@ sph_scene* build_scene(const std::string& text, const std::string& path)
     if (d.surface_tension_method > -1) d.surface_tension = num(fm.get("surfaceTension"), "surfaceTension");
     if (d.adhesion_method > -1) d.adhesion = num(fm.get("adhesion"), "adhesion");
     if (const sphjson::Value* em = fm.find("emitters"))
-        if (em->size() > 0) throw std::invalid_argument("emitters are not supported");
+        for (size_t i = 0; i < em->size(); ++i) {
+            /* SceneLoader.cpp:128-143; rotation is glm::quat(w, x, y, z) */
+            const sphjson::Value& e = em->at(i);
+            sph_emitter_desc ed{};
+            const V3 p = vec3(e.get("position"), "emitters.position");
+            ed.position[0] = p.x; ed.position[1] = p.y; ed.position[2] = p.z;
+            const sphjson::Value& q = e.get("rotation");
+            if (!q.is_array() || q.size() < 4) throw sphjson::JsonError("expected [w,x,y,z] for emitters.rotation");
+            for (int k = 0; k < 4; ++k) ed.rotation[k] = num(q.at(k), "emitters.rotation");
+            ed.velocity = num(e.get("velocity"), "emitters.velocity");
+            ed.num_particles = (unsigned)e.get("numParticles").as_number("emitters.numParticles");
+            ed.start_time = num(e.get("startTime"), "emitters.startTime");
+            ed.type = (int)e.get("type").as_number("emitters.type");
+            ed.width = num(e.get("width"), "emitters.width");
+            ed.height = num(e.get("height"), "emitters.height");
+            ed.spacing = num(e.get("spacing"), "emitters.spacing");
+            scene->emitters.push_back(ed);
+        }
     std::vector<std::pair<V3, V3>> blocks;
     const sphjson::Value& fb = fm.get("fluidBlocks");
     for (size_t i = 0; i < fb.size(); ++i)
@@ -276,6 +298,14 @@ int sph_scene_get_desc(const sph_scene* s, sph_scene_desc* out)
 }
 
 unsigned sph_scene_num_fluid(const sph_scene* s) { return s ? (unsigned)(s->fluid.size() / 3) : 0u; }
+unsigned sph_scene_num_emitters(const sph_scene* s) { return s ? (unsigned)s->emitters.size() : 0u; }
+
+int sph_scene_get_emitter(const sph_scene* s, unsigned k, sph_emitter_desc* out)
+{
+    if (!s || !out || k >= s->emitters.size()) return SPH_ERR_ARG;
+    *out = s->emitters[k];
+    return SPH_OK;
+}
 unsigned sph_scene_num_boundary(const sph_scene* s) { return s ? (unsigned)(s->boundary.size() / 3) : 0u; }
 
 int sph_scene_get_fluid(const sph_scene* s, float* xyz, float* v)
@@ -304,9 +334,11 @@ int sph_create_from_scene(const sph_scene* s, sph_ctx** out)
     if (rc != SPH_OK) return rc;
     sph_ctx* ctx = *out;
     if ((rc = sph_set_fluid(ctx, sph_scene_num_fluid(s), s->fluid.data(), s->fluid_v.data())) != SPH_OK ||
-        (rc = sph_set_boundary(ctx, sph_scene_num_boundary(s), s->boundary.data())) != SPH_OK ||
-        (rc = sph_init(ctx)) != SPH_OK)
+        (rc = sph_set_boundary(ctx, sph_scene_num_boundary(s), s->boundary.data())) != SPH_OK)
         return rc; /* the context stays valid; sph_last_error(ctx) explains */
+    for (const sph_emitter_desc& e : s->emitters)
+        if ((rc = sph_add_emitter(ctx, &e)) != SPH_OK) return rc;
+    if ((rc = sph_init(ctx)) != SPH_OK) return rc;
     return SPH_OK;
 }
 

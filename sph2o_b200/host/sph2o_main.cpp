@@ -57,13 +57,13 @@ std::string frame_path(const std::string& scene, unsigned frame)
 }
 
 /* Keys in the order nlohmann::json (an ordered std::map) writes them. */
-bool write_frame(const std::string& path, const std::vector<float>& x, const std::vector<float>& v, double time,
-                 float dt)
+bool write_frame(const std::string& path, const std::vector<float>& x, const std::vector<float>& v, size_t n_active,
+                 double time, float dt)
 {
     FILE* f = std::fopen(path.c_str(), "w");
     if (!f) return false;
     const size_t n = x.size() / 3;
-    std::fprintf(f, "{\"numActiveParticles\":%zu,\"numParticles\":%zu,\"positions\":[", n, n);
+    std::fprintf(f, "{\"numActiveParticles\":%zu,\"numParticles\":%zu,\"positions\":[", n_active, n);
     for (size_t i = 0; i < n; ++i)
         std::fprintf(f, "%s[%s,%s,%s]", i ? "," : "", sphjson::format_double((double)x[3 * i]).c_str(),
                      sphjson::format_double((double)x[3 * i + 1]).c_str(),
@@ -176,6 +176,12 @@ int main(int argc, char** argv)
     float last_save = 0.0f;
     float time = 0.0f;
     std::vector<float> x(3ull * nf), v(3ull * nf);
+    if (a.frame >= 0 && sph_scene_num_emitters(scene) > 0) {
+        /* SPH2O's importFluidState exits before it would restore emitters
+           (SPHSimulation.cpp:547-551); there is no state to resume them from */
+        std::fprintf(stderr, "resuming a scene with emitters is not supported\n");
+        return 1;
+    }
     if (a.frame >= 0) {
         double t = 0.0;
         float dt = 0.0f;
@@ -216,8 +222,10 @@ int main(int argc, char** argv)
                     std::fprintf(stderr, "%s\n", sph_last_error(ctx));
                     return 1;
                 }
+                unsigned na = nf;
+                sph_get_num_active(ctx, &na);
                 const std::string path = frame_path(a.scene, frame);
-                if (!write_frame(path, x, v, (double)time, st.dt)) std::fprintf(stderr, "Cannot write fluid state\n");
+                if (!write_frame(path, x, v, na, (double)time, st.dt)) std::fprintf(stderr, "Cannot write fluid state\n");
             }
             if (!a.quiet)
                 std::printf("frame %u  t=%.5f s  dt=%.3g s  its=%u/%u\n", frame, (double)time, (double)st.dt,

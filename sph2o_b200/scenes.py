@@ -214,6 +214,32 @@ def small(method=DFSPH, n=(10, 10, 10), radius=0.025, surface_tension=0.0,
     )
 
 
+def with_emitter(scene_dict, *, etype=0, position, rotation=(1.0, 0.0, 0.0, 0.0), velocity=1.0, num_particles=100,
+                 start_time=0.0, width=0.1, height=0.1, spacing=1.0):
+    """Adds an emitter to the scene's fluid model (SceneLoader.cpp:128-143
+    keys; rotation is the quaternion w, x, y, z)."""
+    scene_dict["Fluid"]["FluidModel"][0].setdefault("emitters", []).append({
+        "type": int(etype), "position": f32(list(position)), "rotation": f32(list(rotation)),
+        "velocity": f32(velocity), "numParticles": int(num_particles), "startTime": f32(start_time),
+        "width": f32(width), "height": f32(height), "spacing": f32(spacing)})
+    return scene_dict
+
+
+def emitter_scenes():
+    """Small scenes with an emitter shooting along +x (local z turned by 90
+    degrees about y) from the middle of the tank, emitting from t = 0."""
+    q = (math.cos(math.pi / 4), 0.0, math.sin(math.pi / 4), 0.0)
+    wc = small(method=WCSPH, n=(6, 6, 6), time_step=2e-4, seed=31)
+    tank = wc["Boundary"][0]["box"][0]["max"]
+    with_emitter(wc, etype=0, position=(0.35 * tank[0], 0.5 * tank[1], 0.5 * tank[2]), rotation=q, velocity=5.0,
+                 num_particles=4 * 16, width=0.2, height=0.2, spacing=1.0)
+    df = small(method=DFSPH, n=(6, 6, 6), time_step=5e-4, seed=32)
+    tank = df["Boundary"][0]["box"][0]["max"]
+    with_emitter(df, etype=1, position=(0.35 * tank[0], 0.5 * tank[1], 0.5 * tank[2]), rotation=q, velocity=4.0,
+                 num_particles=3 * 19, width=0.11, spacing=1.2)
+    return {"emitter_wcsph_square": wc, "emitter_dfsph_circle": df}
+
+
 def batched_scene_params(count=256, seed=4):
     """Per-scene parameters of the batched workload: N_f log-uniform in
     [2000, 40000], block aspect ratios uniform in [0.5, 2] (normalised so the

@@ -37,7 +37,12 @@ def built_library():
 
 
 def golden_names():
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+    """Fixed-particle golden scenes (the emitter scenes have their own tests)."""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("emitter_"))
+
+
+def emitter_golden_names():
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("emitter_"))
 
 
 def load_golden(name):

@@ -20,9 +20,14 @@ For every small scene below it stores, in <name>.npz:
   trace_f32, trace_f64   per-step [time, dt, iterations, iterationsV,
                    avg density residual, avg divergence residual,
                    centroid x y z, kinetic energy, mean density error] over
-                   NSTEPS steps, from the FP32-strict and FP64 builds (the FP64
+                   NSTEPS steps (STEPS for the emitter scenes), from the FP32-strict and FP64 builds (the FP64
                    run starts from the same float inputs)
   final_pos_f64, final_vel_f64   FP64 state after NSTEPS steps
+  active_f32, active_f64   active fluid particles after every step (emitter
+                   scenes; emitted particles take the slots after the active ones)
+
+    python tests/golden/make_golden.py [name ...]    # default: every scene
+
 Test infrastructure only.
 """
 import json
@@ -41,12 +46,15 @@ from oracle import sphd  # noqa: E402
 from sph2o_b200 import scenes as S  # noqa: E402
 
 NSTEPS = 20
+# emitter scenes run long enough for several emissions
+STEPS = {"emitter_wcsph_square": 120, "emitter_dfsph_circle": 120}
 REF32 = os.path.join(ROOT, "oracle", "_ref", "sph2o_ref_f32")
 REF64 = os.path.join(ROOT, "oracle", "_ref", "sph2o_ref_f64")
 
 
 def golden_scenes():
     return {
+        **S.emitter_scenes(),
         "dfsph_st_sphere": S.small(method=S.DFSPH, surface_tension=0.05, sphere=True),
         "wcsph_artificial": S.small(method=S.WCSPH, n=(12, 10, 10)),
         "pcisph_artificial": S.small(method=S.PCISPH, n=(10, 10, 12), eta=0.01, time_step=5e-4),
@@ -82,8 +90,10 @@ def make(name, scene, td):
             g[k] = ph[k]
     s1 = run(REF32, path, "step", os.path.join(td, "s1.sphd"), "--steps", "1")
     g["step1_pos"], g["step1_vel"], g["step1_density"] = s1["pos"], s1["vel"], s1["density"]
-    sn = run(REF32, path, "step", os.path.join(td, "sn.sphd"), "--steps", str(NSTEPS))
+    nsteps = STEPS.get(name, NSTEPS)
+    sn = run(REF32, path, "step", os.path.join(td, "sn.sphd"), "--steps", str(nsteps))
     g["trace_f32"] = sn["step_stats"]
+    g["active_f32"] = sn["active"]
     g["final_pos_f32"], g["final_vel_f32"] = sn["pos"], sn["vel"]
     state = os.path.join(td, "state.sphd")
     sphd.write(state, {"pos": nb["init_pos"].astype(np.float64)})
@@ -92,9 +102,10 @@ def make(name, scene, td):
     s1d = run(REF64, path, "step", os.path.join(td, "s1d.sphd"), "--steps", "1", "--state-in", state,
               "--boundary-in", bnd)
     g["step1_pos_f64"], g["step1_vel_f64"], g["step1_density_f64"] = s1d["pos"], s1d["vel"], s1d["density"]
-    s64 = run(REF64, path, "step", os.path.join(td, "s64.sphd"), "--steps", str(NSTEPS), "--state-in", state,
+    s64 = run(REF64, path, "step", os.path.join(td, "s64.sphd"), "--steps", str(nsteps), "--state-in", state,
               "--boundary-in", bnd)
     g["trace_f64"] = s64["step_stats"]
+    g["active_f64"] = s64["active"]
     g["final_pos_f64"], g["final_vel_f64"] = s64["pos"], s64["vel"]
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **g)
     return g
@@ -104,8 +115,11 @@ def main():
     for b in (REF32, REF64):
         if not os.path.exists(b):
             raise SystemExit(f"{b} missing: run make -C oracle first")
+    want = set(sys.argv[1:])
     with tempfile.TemporaryDirectory() as td:
         for name, scene in golden_scenes().items():
+            if want and name not in want:
+                continue
             g = make(name, scene, td)
             print(name, g["init_pos"].shape[0], "fluid", g["bpos"].shape[0], "boundary")
 

@@ -45,7 +45,7 @@ def test_missing_sphere_geometry_keys_tolerated():
     (lambda d: d["Configuration"].pop("timeStep"), -8),
     (lambda d: d["Fluid"]["FluidModel"].append(copy.deepcopy(d["Fluid"]["FluidModel"][0])), -1),
     (lambda d: d["Configuration"].__setitem__("boundaryMethod", 0), -1),
-    (lambda d: d["Fluid"]["FluidModel"][0].__setitem__("emitters", [{"type": 0}]), -1),
+    (lambda d: d["Fluid"]["FluidModel"][0].__setitem__("emitters", [{"type": 0}]), -8),
     (lambda d: d["Boundary"][0].__setitem__("geometry", [{"path": "x.obj", "spacing": 1.0}]), -1),
     (lambda d: d["Configuration"].__setitem__("simulationMethod", 7), -8),
 ])
@@ -55,6 +55,24 @@ def test_bad_scenes_rejected(mutate, code):
     with pytest.raises(SphError) as e:
         Scene.from_dict(d)
     assert e.value.code == code
+
+
+def test_emitters_parsed():
+    """The "emitters" keys of SceneLoader.cpp:128-143; rotation is (w, x, y, z)."""
+    d = S.small()
+    d["Fluid"]["FluidModel"][0]["emitters"] = [
+        {"position": [0.5, 0.25, 0.75], "rotation": [0.5, 0.5, -0.5, 0.5], "velocity": 2.0, "numParticles": 300,
+         "startTime": 0.01, "type": 1, "width": 0.1, "height": 0.0, "spacing": 1.5},
+        {"position": [0.1, 0.2, 0.3], "rotation": [1.0, 0.0, 0.0, 0.0], "velocity": 1.0, "numParticles": 64,
+         "startTime": 0.0, "type": 0, "width": 0.2, "height": 0.2, "spacing": 1.0}]
+    sc = Scene.from_dict(d)
+    em = sc.emitters()
+    assert len(em) == 2
+    e = em[0]
+    assert e.type == 1 and e.num_particles == 300 and list(e.position) == [0.5, 0.25, 0.75]
+    assert list(e.rotation) == [0.5, 0.5, -0.5, 0.5] and e.velocity == 2.0 and e.spacing == 1.5
+    assert e.start_time == float(np.float32(0.01)) and e.width == float(np.float32(0.1))
+    assert em[1].type == 0 and em[1].num_particles == 64
 
 
 def test_malformed_json():
