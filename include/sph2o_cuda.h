@@ -58,7 +58,7 @@ enum sph_status {
    that the particle path reads. */
 typedef struct sph_scene_desc {
     int simulation_method;          /* sph_method */
-    int boundary_method;            /* only SPH_BOUNDARY_AKINCI is implemented */
+    int boundary_method;            /* SPH_BOUNDARY_AKINCI or SPH_BOUNDARY_CUBE */
     int viscosity_method;           /* -1 none, 0 standard, 1 artificial, 2 XSPH */
     int surface_tension_method;     /* -1 none, 3 Akinci */
     int adhesion_method;            /* -1 none, 4 Akinci */
@@ -129,6 +129,18 @@ int sph_set_fluid(sph_ctx* ctx, unsigned n, const float* xyz, const float* v);
 /* Akinci boundary particles of all boundary objects, concatenated in object
    order (AkinciBoundaryObject::r, AkinciBoundaryObject.cpp:36-95). */
 int sph_set_boundary(sph_ctx* ctx, unsigned n, const float* xyz);
+
+/* Cube boundary (boundary_method SPH_BOUNDARY_CUBE; CubeBoundaryObject,
+   CubeBoundaryObject.cpp:10-88): no boundary particles; after each step's
+   integration every fluid particle outside [min, max] is put back on the
+   violated face, the velocity component pointing out scaled by
+   -normal_fct and the other two by tangential_fct, axis by axis (x, y, z),
+   cube by cube in the order added. SPH2O's loader never reads the factors
+   for this method, so scenes loaded by sph_scene_load carry 0 and 0 (a
+   particle that hits a wall stops there), as in the reference. Before
+   sph_init; single scenes only. */
+int sph_add_cube_boundary(sph_ctx* ctx, const float min[3], const float max[3], float normal_fct,
+                          float tangential_fct);
 
 /* Particle emitter of the fluid model (Emitter.h:10-33; scene keys of
    SceneLoader.cpp:128-143). An emitter holds num_particles inactive
@@ -379,6 +391,11 @@ int sph_scene_parse(const char* json_text, sph_scene** out);
 int sph_scene_get_desc(const sph_scene* s, sph_scene_desc* out);
 unsigned sph_scene_num_fluid(const sph_scene* s);
 unsigned sph_scene_num_boundary(const sph_scene* s);
+/* Cube boundaries of a scene with boundaryMethod 0 (the first "box" of each
+   boundary object, SPHSimulation.cpp:459-477). */
+unsigned sph_scene_num_cube_boundaries(const sph_scene* s);
+int sph_scene_get_cube_boundary(const sph_scene* s, unsigned k, float min[3], float max[3], float* normal_fct,
+                                float* tangential_fct);
 /* Emitters of the scene's fluid model ("emitters" key, SceneLoader.cpp:109-143). */
 unsigned sph_scene_num_emitters(const sph_scene* s);
 int sph_scene_get_emitter(const sph_scene* s, unsigned k, sph_emitter_desc* out);
@@ -387,7 +404,8 @@ int sph_scene_get_boundary(const sph_scene* s, float* xyz);
 const char* sph_scene_error(void);
 void sph_scene_free(sph_scene* s);
 
-/* create + set_fluid + set_boundary + add_emitter + init from a loaded scene. */
+/* create + set_fluid + set_boundary + add_cube_boundary + add_emitter + init
+   from a loaded scene. */
 int sph_create_from_scene(const sph_scene* s, sph_ctx** out);
 
 #ifdef __cplusplus

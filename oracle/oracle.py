@@ -23,6 +23,7 @@ def lib():
         L.sph_oracle_set_fluid.argtypes = [P, C.c_uint, F, F]
         L.sph_oracle_set_boundary.argtypes = [P, C.c_uint, F]
         L.sph_oracle_init.argtypes = [P]
+        L.sph_oracle_add_cube.argtypes = [P, F, F, C.c_float, C.c_float]
         L.sph_oracle_step.argtypes = [P, C.c_int, D]
         L.sph_oracle_get_state.argtypes = [P, D, D, D]
         L.sph_oracle_get_boundary_volume.argtypes = [P, D]
@@ -51,15 +52,18 @@ def _u(a):
 class Oracle:
     """CPU restatement of the reference; fp64=False reproduces its FP32 build."""
 
-    def __init__(self, desc, fluid, boundary, vel=None, fp64=False):
+    def __init__(self, desc, fluid, boundary, vel=None, fp64=False, cubes=()):
         L = lib()
         self.h = L.sph_oracle_create(C.addressof(desc), 1 if fp64 else 0)
         x = np.ascontiguousarray(fluid, np.float32)
-        b = np.ascontiguousarray(boundary, np.float32)
+        b = np.ascontiguousarray(boundary, np.float32).reshape(-1, 3)
         v = None if vel is None else np.ascontiguousarray(vel, np.float32)
         self.nf, self.nb = x.shape[0], b.shape[0]
         L.sph_oracle_set_fluid(self.h, self.nf, _f(x), _f(v))
         L.sph_oracle_set_boundary(self.h, self.nb, _f(b))
+        for mn, mx, nfct, tfct in cubes:
+            L.sph_oracle_add_cube(self.h, _f(np.ascontiguousarray(mn, np.float32)),
+                                  _f(np.ascontiguousarray(mx, np.float32)), float(nfct), float(tfct))
         L.sph_oracle_init(self.h)
 
     def step(self, n=1):

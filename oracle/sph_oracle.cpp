@@ -52,6 +52,8 @@ template <typename R> struct Oracle {
     std::vector<R> rho, alpha, press, kk, kv, kws, kvws, pred, div;
     std::vector<V3<R>> bx;
     std::vector<R> bvol;
+    struct Cube { V3<R> mn, mx; R nf, tf; };
+    std::vector<Cube> cubes;
     struct Cell { std::vector<uint32_t> f, b; };
     std::unordered_map<uint64_t, Cell> cells;
 
@@ -366,6 +368,31 @@ template <typename R> struct Oracle {
             a[i] = V3<R>();
         }
     }
+    /* CubeBoundaryObject::correctPositionAndVelocity (CubeBoundaryObject.cpp:10-88) */
+    static void cube_axis(R& p, R& v, R& t1, R& t2, R lo, R hi, R nf, R tf)
+    {
+        if (p < lo) {
+            p = lo;
+            if (v < 0.0) v *= -nf;
+            t1 *= tf;
+            t2 *= tf;
+        } else if (p > hi) {
+            p = hi;
+            if (v > 0.0) v *= -nf;
+            t1 *= tf;
+            t2 *= tf;
+        }
+    }
+    void cube_correct()
+    {
+        for (const Cube& c : cubes)
+            for (size_t i = 0; i < x.size(); ++i) {
+                cube_axis(x[i].x, v[i].x, v[i].y, v[i].z, c.mn.x, c.mx.x, c.nf, c.tf);
+                cube_axis(x[i].y, v[i].y, v[i].x, v[i].z, c.mn.y, c.mx.y, c.nf, c.tf);
+                cube_axis(x[i].z, v[i].z, v[i].x, v[i].y, c.mn.z, c.mx.z, c.nf, c.tf);
+            }
+    }
+
     void wcsph_step()
     {
         insert_fluid();
@@ -374,6 +401,7 @@ template <typename R> struct Oracle {
         wcsph_pressure_force();
         nonpressure();
         integrate();
+        cube_correct();
         time += dt;
     }
 
@@ -444,6 +472,7 @@ template <typename R> struct Oracle {
             x[i] += v[i] * dt;
             a[i] = V3<R>();
         }
+        cube_correct();
         time += dt;
     }
 
@@ -576,6 +605,7 @@ template <typename R> struct Oracle {
         for (size_t i = 0; i < n; ++i) kvws[i] *= dt;
         its_v = it;
         avg_div = avgv;
+        cube_correct();
         time += dt;
     }
 
@@ -656,6 +686,19 @@ int sph_oracle_set_boundary(sph_oracle* o, unsigned n, const float* xyz)
     };
     fill(o->f);
     fill(o->dd);
+    return SPH_OK;
+}
+
+int sph_oracle_add_cube(sph_oracle* o, const float* mn, const float* mx, float normal_fct, float tangential_fct)
+{
+    if (!o || !mn || !mx) return SPH_ERR_ARG;
+    auto add = [&](auto& S) {
+        using R = std::remove_reference_t<decltype(S.r)>;
+        S.cubes.push_back({V3<R>((R)mn[0], (R)mn[1], (R)mn[2]), V3<R>((R)mx[0], (R)mx[1], (R)mx[2]), (R)normal_fct,
+                           (R)tangential_fct});
+    };
+    add(o->f);
+    add(o->dd);
     return SPH_OK;
 }
 

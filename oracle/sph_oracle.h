@@ -26,6 +26,8 @@ typedef struct sph_oracle sph_oracle;
 sph_oracle* sph_oracle_create(const sph_scene_desc* desc, int fp64);
 int sph_oracle_set_fluid(sph_oracle* o, unsigned n, const float* xyz, const float* v);
 int sph_oracle_set_boundary(sph_oracle* o, unsigned n, const float* xyz);
+/* cube boundary (boundary method 0), applied after integration in order */
+int sph_oracle_add_cube(sph_oracle* o, const float* mn, const float* mx, float normal_fct, float tangential_fct);
 int sph_oracle_init(sph_oracle* o);
 /* stats: [time, dt, iterations, iterationsV, avg density residual, avg divergence residual] per step */
 int sph_oracle_step(sph_oracle* o, int nsteps, double* stats);

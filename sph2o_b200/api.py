@@ -134,6 +134,9 @@ def lib():
         "sph_scene_free": (None, [P]),
         "sph_create_from_scene": (I, [P, C.POINTER(P)]),
         "sph_add_emitter": (I, [P, C.POINTER(EmitterDesc)]),
+        "sph_add_cube_boundary": (I, [P, F, F, C.c_float, C.c_float]),
+        "sph_scene_num_cube_boundaries": (U, [P]),
+        "sph_scene_get_cube_boundary": (I, [P, U, F, F, F, F]),
         "sph_get_num_active": (I, [P, C.POINTER(U)]),
         "sph_scene_num_emitters": (U, [P]),
         "sph_scene_get_emitter": (I, [P, U, C.POINTER(EmitterDesc)]),
@@ -198,6 +201,17 @@ class Scene:
         lib().sph_scene_get_fluid(self._h, _fptr(x), _fptr(v))
         return x, v
 
+    def cube_boundaries(self):
+        """[(min, max, normal_fct, tangential_fct)] of a boundaryMethod-0 scene."""
+        out = []
+        for k in range(lib().sph_scene_num_cube_boundaries(self._h)):
+            mn = np.zeros(3, np.float32)
+            mx = np.zeros(3, np.float32)
+            nf, tf = C.c_float(), C.c_float()
+            lib().sph_scene_get_cube_boundary(self._h, k, _fptr(mn), _fptr(mx), C.byref(nf), C.byref(tf))
+            out.append((mn, mx, nf.value, tf.value))
+        return out
+
     def emitters(self):
         out = []
         for k in range(lib().sph_scene_num_emitters(self._h)):
@@ -227,7 +241,7 @@ class Scene:
 class Simulation:
     """One GPU simulation context (sph_ctx)."""
 
-    def __init__(self, desc: SceneDesc, fluid, boundary, vel=None, emitters=()):
+    def __init__(self, desc: SceneDesc, fluid, boundary, vel=None, emitters=(), cubes=()):
         L = lib()
         h = C.c_void_p()
         rc = L.sph_create(C.byref(desc), C.byref(h))
@@ -240,6 +254,10 @@ class Simulation:
         b = np.ascontiguousarray(boundary, np.float32).reshape(-1, 3)
         self._check(L.sph_set_fluid(h, x.shape[0], _fptr(x), _fptr(v)))
         self._check(L.sph_set_boundary(h, b.shape[0], _fptr(b)))
+        for mn, mx, nfct, tfct in cubes:
+            mn = np.ascontiguousarray(mn, np.float32)
+            mx = np.ascontiguousarray(mx, np.float32)
+            self._check(L.sph_add_cube_boundary(h, _fptr(mn), _fptr(mx), float(nfct), float(tfct)))
         for e in emitters:
             self._check(L.sph_add_emitter(h, C.byref(e)))
         self._check(L.sph_init(h))
@@ -248,7 +266,8 @@ class Simulation:
     @classmethod
     def from_scene(cls, scene: Scene, vel=None):
         x, v = scene.fluid()
-        return cls(scene.desc(), x, scene.boundary(), v if vel is None else vel, emitters=scene.emitters())
+        return cls(scene.desc(), x, scene.boundary(), v if vel is None else vel, emitters=scene.emitters(),
+                   cubes=scene.cube_boundaries())
 
     def num_active(self):
         n = C.c_uint()

@@ -121,6 +121,8 @@ struct sph_ctx {
     /* emitters of a single scene (sph_add_emitter): descriptions, the fluid
        particles active at init, the device table and group offsets */
     std::vector<sph_emitter_desc> emitters;
+    std::vector<CubeBox> cubes;      /* cube boundaries (boundary method 0) */
+    CubeBox* d_cubes = nullptr;
     unsigned n_init = 0;
     EmitterState* d_emit = nullptr;
     float4* d_group = nullptr;
@@ -434,6 +436,15 @@ int neighbor_search(sph_ctx* c)
     return check_launch(c, "neighbour search");
 }
 
+/* Cube boundaries after integration (a no-op without them). */
+void cube_correct(sph_ctx* c)
+{
+    if (c->cubes.empty()) return;
+    launch_cube_correct(c->P, arrays(c), c->d_cubes, (int)c->cubes.size(), c->stream);
+    c->launches += 1;
+    c->lists_valid = false;
+}
+
 /* Emission of the due emitter groups (a no-op without emitters). */
 void emit(sph_ctx* c, bool advance_time)
 {
@@ -460,6 +471,7 @@ int step_wcsph(sph_ctx* c)
     std::swap(c->pos, c->pos2);
     std::swap(c->vel, c->vel2);
     c->lists_valid = false;
+    cube_correct(c); /* WCSPHSolver.cpp:51-60 */
     emit(c, true); /* WCSPHSolver.cpp:75: emission, then t += dt */
     return check_launch(c, "wcsph step");
 }
@@ -476,7 +488,8 @@ int step_pcisph(sph_ctx* c)
     int e;
     { Phase ph(c, SPH_PROF_PRESSURE_SOLVE, 1); e = launch_pcisph_solve(c->P, A, c->grid_pcisph, c->stream); }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("pcisph solver launch: ") + cudaGetErrorString((cudaError_t)e));
-    c->lists_valid = !c->P.dynamic;
+    c->lists_valid = !c->P.dynamic && c->cubes.empty();
+    cube_correct(c); /* PCISPHSolver.cpp:53-62 */
     emit(c, true); /* PCISPHSolver.cpp:77: emission, then t += dt */
     return check_launch(c, "pcisph step");
 }
@@ -514,6 +527,18 @@ int step_dfsph(sph_ctx* c)
                        : launch_dfsph_solve(c->P, A, true, solve_grid(c, true), c->solver_occ, c->solver_tpp, c->stream);
     }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph divergence solver launch: ") + cudaGetErrorString((cudaError_t)e));
+    cube_correct(c); /* DFSPHSolver.cpp:94-103 */
+    if (!c->cubes.empty()) {
+        /* The next step's force and solver passes run on this step's lists,
+           but the cube correction has moved particles since they were built.
+           SPH2O's loops take the candidates of the cells around each
+           particle's current position, with the cell contents of the last
+           insertion, and evaluate distances at current positions: rebuild
+           the lists from the current positions against the same cell table. */
+        Phase ph(c, SPH_PROF_LISTS, 1);
+        launch_build_lists(c->P, SceneRef{c->d_scenes, c->d_scene_of}, c->pos, c->cell_start, c->bpos, c->bcell_start,
+                           c->nbr_f, c->cnt_f, c->nbr_b, c->cnt_b, c->st, c->stream);
+    }
     return check_launch(c, "dfsph step");
 }
 
@@ -703,8 +728,8 @@ int sph_create(const sph_scene_desc* desc, sph_ctx** out)
     *out = nullptr;
     if (desc->simulation_method < SPH_WCSPH || desc->simulation_method > SPH_DFSPH)
         return fail(nullptr, SPH_ERR_ARG, "simulation_method must be 0, 1 or 2");
-    if (desc->boundary_method != SPH_BOUNDARY_AKINCI)
-        return fail(nullptr, SPH_ERR_ARG, "only the Akinci boundary method (2) is implemented");
+    if (desc->boundary_method != SPH_BOUNDARY_AKINCI && desc->boundary_method != SPH_BOUNDARY_CUBE)
+        return fail(nullptr, SPH_ERR_ARG, "boundary methods 2 (Akinci) and 0 (cube) are implemented");
     if (!(desc->particle_radius > 0.0f) || !(desc->density0 > 0.0f) || !(desc->time_step > 0.0f) || !(desc->fps > 0.0f))
         return fail(nullptr, SPH_ERR_ARG, "particle_radius, density0, time_step and fps must be positive");
     if (desc->simulation_method == SPH_WCSPH && !(desc->gamma != 0.0f))
@@ -753,6 +778,17 @@ int sph_set_boundary(sph_ctx* c, unsigned n, const float* xyz)
     return SPH_OK;
 }
 
+int sph_add_cube_boundary(sph_ctx* c, const float mn[3], const float mx[3], float normal_fct, float tangential_fct)
+{
+    if (!c || !mn || !mx) return SPH_ERR_ARG;
+    if (c->nscenes) return fail(c, SPH_ERR_ARG, "cube boundaries apply to single scenes, not to batches");
+    if (c->initialized) return fail(c, SPH_ERR_STATE, "sph_add_cube_boundary after sph_init");
+    if (c->desc.boundary_method != SPH_BOUNDARY_CUBE)
+        return fail(c, SPH_ERR_ARG, "cube boundaries need boundary_method SPH_BOUNDARY_CUBE");
+    c->cubes.push_back({mn[0], mn[1], mn[2], mx[0], mx[1], mx[2], normal_fct, tangential_fct});
+    return SPH_OK;
+}
+
 int sph_add_emitter(sph_ctx* c, const sph_emitter_desc* e)
 {
     if (!c || !e) return SPH_ERR_ARG;
@@ -796,6 +832,8 @@ int sph_init(sph_ctx* c)
         c->nf = c->fsplit.back();
         c->nb = c->bsplit.back();
     }
+    if (c->desc.boundary_method == SPH_BOUNDARY_CUBE && c->nb > 0)
+        return fail(c, SPH_ERR_ARG, "the cube boundary method has no boundary particles");
     /* emitters: their particles are allocated inactive after the blocks */
     c->n_init = c->nf;
     std::vector<float> groups;
@@ -879,6 +917,8 @@ int sph_init(sph_ctx* c)
     };
     grow(std::vector<float>(c->h_fluid.begin(), c->h_fluid.begin() + 3ull * c->n_init));
     grow(c->h_bound);
+    /* cube boundaries keep the fluid inside their boxes */
+    for (const CubeBox& b : c->cubes) grow({b.minx, b.miny, b.minz, b.maxx, b.maxy, b.maxz});
     /* emitted particles start around their emitter */
     for (const sph_emitter_desc& e : c->emitters) {
         const float ext = std::max(e.width, e.height) + 4.0f * P.h;
@@ -1002,6 +1042,11 @@ int sph_init(sph_ctx* c)
         CUDA_TRY(c, cudaMemsetAsync(c->bcell_start, 0, ((size_t)P.ncells + 1) * sizeof(unsigned), c->stream));
     }
 
+    if (!c->cubes.empty()) {
+        if ((rc = dalloc(c, &c->d_cubes, c->cubes.size())) != SPH_OK) return rc;
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_cubes, c->cubes.data(), c->cubes.size() * sizeof(CubeBox), cudaMemcpyHostToDevice,
+                                    c->stream));
+    }
     if (!etab.empty()) {
         if ((rc = dalloc(c, &c->d_emit, etab.size())) != SPH_OK) return rc;
         if ((rc = dalloc(c, &c->snap_emit, etab.size())) != SPH_OK) return rc;

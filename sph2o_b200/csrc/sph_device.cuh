@@ -95,6 +95,12 @@ __device__ __forceinline__ double advance_time(double t, float dt)
     return (double)__fadd_rn((float)t, dt);
 }
 
+/* A cube boundary (CubeBoundaryObject.h:6-27): box and velocity factors. */
+struct CubeBox {
+    float minx, miny, minz, maxx, maxy, maxz;
+    float normal_fct, tangential_fct;
+};
+
 /* One particle emitter (Emitter.h:10-33) on the device: pose, speed, the
    next emission time, what is left to emit and its group of particle
    offsets in the group table. */

@@ -96,6 +96,8 @@ int launch_dfsph_solve(const SimParams& P, const DeviceArrays& A, bool divergenc
 int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s);
 int launch_dfsph_solve_batch(const SimParams& P, const DeviceArrays& A, bool divergence, int grid, cudaStream_t s);
 int launch_barrier_timeout_probe(DevState* st, cudaStream_t s);
+/* cube boundaries: clamp the active particles into each box in order */
+void launch_cube_correct(const SimParams& P, const DeviceArrays& A, const CubeBox* cubes, int ncubes, cudaStream_t s);
 /* emission of the nemit emitters' due groups (one block); advance: then t += dt */
 void launch_emit(const SimParams& P, const DeviceArrays& A, EmitterState* E, const float4* group, int nemit,
                  bool advance, cudaStream_t s);

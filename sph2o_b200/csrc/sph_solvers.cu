@@ -929,6 +929,49 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
 }
 
 /* ---------------------------------------------------------------------- */
+/* CubeBoundaryObject::correctPositionAndVelocity (CubeBoundaryObject.cpp:10-88):
+   per axis in x, y, z order, a particle below min (above max) is put on the
+   face; an outward velocity component is scaled by -normal_fct and the
+   other two by tangential_fct; cubes in order.                             */
+
+__device__ __forceinline__ void cube_axis(float& p, float& v, float& t1, float& t2, float lo, float hi, float nf,
+                                          float tf)
+{
+    if (p < lo) {
+        p = lo;
+        if (v < 0.0f) v = __fmul_rn(v, -nf);
+        t1 = __fmul_rn(t1, tf);
+        t2 = __fmul_rn(t2, tf);
+    } else if (p > hi) {
+        p = hi;
+        if (v > 0.0f) v = __fmul_rn(v, -nf);
+        t1 = __fmul_rn(t1, tf);
+        t2 = __fmul_rn(t2, tf);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_cube_correct(SimParams P, DeviceArrays A, const CubeBox* cubes, int ncubes)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= active_n(P, A.st)) return;
+    float4 x = A.pos[i], v = A.vel[i];
+    for (int c = 0; c < ncubes; ++c) {
+        const CubeBox b = cubes[c];
+        cube_axis(x.x, v.x, v.y, v.z, b.minx, b.maxx, b.normal_fct, b.tangential_fct);
+        cube_axis(x.y, v.y, v.x, v.z, b.miny, b.maxy, b.normal_fct, b.tangential_fct);
+        cube_axis(x.z, v.z, v.x, v.y, b.minz, b.maxz, b.normal_fct, b.tangential_fct);
+    }
+    A.pos[i] = x;
+    A.vel[i] = v;
+}
+
+void launch_cube_correct(const SimParams& P, const DeviceArrays& A, const CubeBox* cubes, int ncubes, cudaStream_t s)
+{
+    if (P.nf <= 0 || ncubes <= 0) return;
+    k_cube_correct<<<(P.nf + 255) / 256, 256, 0, s>>>(P, A, cubes, ncubes);
+}
+
+/* ---------------------------------------------------------------------- */
 /* Emitters (Emitter::emitParticles / emitGroup, Emitter.cpp:82-128).       */
 
 /* glm's quat * vec3 (type_quat.inl:347-354) in FP32, operation for

@@ -20,8 +20,12 @@
  * read into sph_emitter_desc and handed to the context by
  * sph_create_from_scene (FluidObject::addEmitter, FluidObject.cpp:177-194).
  *
- * Not supported (rejected with SPH_ERR_ARG): more than one fluid model,
- * boundary methods other than Akinci, OBJ "geometry" boundaries.
+ * With boundaryMethod 0 each boundary object contributes its first box as a
+ * cube boundary (SPHSimulation.cpp:459-477), with the zero velocity factors
+ * SPH2O's loader leaves it.
+ *
+ * Not supported (rejected with SPH_ERR_ARG): more than one fluid model, the
+ * PCISPH boundary method (1), OBJ "geometry" boundaries.
  */
 #include "../../include/sph2o_cuda.h"
 #include "json_lite.h"
@@ -40,6 +44,8 @@ struct sph_scene {
     std::vector<float> fluid_v;   /* n*3 */
     std::vector<float> boundary;  /* nb*3 */
     std::vector<sph_emitter_desc> emitters;
+    struct Cube { float mn[3], mx[3]; };
+    std::vector<Cube> cubes;      /* boundary method 0: first box of each boundary object */
     std::string path;
 };
 
@@ -173,8 +179,8 @@ sph_scene* build_scene(const std::string& text, const std::string& path)
     } else {
         throw sphjson::JsonError("simulationMethod must be 0 (WCSPH), 1 (PCISPH) or 2 (DFSPH)");
     }
-    if (d.boundary_method != SPH_BOUNDARY_AKINCI)
-        throw std::invalid_argument("only boundaryMethod 2 (Akinci) is implemented");
+    if (d.boundary_method != SPH_BOUNDARY_AKINCI && d.boundary_method != SPH_BOUNDARY_CUBE)
+        throw std::invalid_argument("boundaryMethod 2 (Akinci) and 0 (cube) are implemented");
 
     /* SceneLoader::readFluidInfo (SceneLoader.cpp:80-146) */
     const sphjson::Value& fl = root.get("Fluid");
@@ -231,6 +237,19 @@ sph_scene* build_scene(const std::string& text, const std::string& path)
         }
     }
 
+    /* SceneLoader::readBoundaryInfo (SceneLoader.cpp:148-209) + importScene
+       (:459-477) for the cube method: the first box of each boundary object */
+    if (d.boundary_method == SPH_BOUNDARY_CUBE) {
+        if (const sphjson::Value* bnd = root.find("Boundary"))
+            for (size_t i = 0; i < bnd->size(); ++i) {
+                const sphjson::Value* boxes = bnd->at(i).find("box");
+                if (!boxes || boxes->size() == 0)
+                    throw std::invalid_argument("a cube boundary object needs a box");
+                const V3 mn = vec3(boxes->at(0).get("min"), "box.min"), mx = vec3(boxes->at(0).get("max"), "box.max");
+                scene->cubes.push_back({{mn.x, mn.y, mn.z}, {mx.x, mx.y, mx.z}});
+            }
+        return scene.release();
+    }
     /* SceneLoader::readBoundaryInfo (SceneLoader.cpp:148-209) + importScene (:407-426) */
     if (const sphjson::Value* bnd = root.find("Boundary")) {
         for (size_t i = 0; i < bnd->size(); ++i) {
@@ -299,6 +318,23 @@ int sph_scene_get_desc(const sph_scene* s, sph_scene_desc* out)
 
 unsigned sph_scene_num_fluid(const sph_scene* s) { return s ? (unsigned)(s->fluid.size() / 3) : 0u; }
 unsigned sph_scene_num_emitters(const sph_scene* s) { return s ? (unsigned)s->emitters.size() : 0u; }
+unsigned sph_scene_num_cube_boundaries(const sph_scene* s) { return s ? (unsigned)s->cubes.size() : 0u; }
+
+int sph_scene_get_cube_boundary(const sph_scene* s, unsigned k, float mn[3], float mx[3], float* normal_fct,
+                                float* tangential_fct)
+{
+    if (!s || k >= s->cubes.size()) return SPH_ERR_ARG;
+    for (int q = 0; q < 3; ++q) {
+        if (mn) mn[q] = s->cubes[k].mn[q];
+        if (mx) mx[q] = s->cubes[k].mx[q];
+    }
+    /* SceneLoader::readBoundaryInfo reads normalFct / tangFct only for the
+       PCISPH method (SceneLoader.cpp:168-172): the cube objects get the zero
+       of a value-initialised Boundary */
+    if (normal_fct) *normal_fct = 0.0f;
+    if (tangential_fct) *tangential_fct = 0.0f;
+    return SPH_OK;
+}
 
 int sph_scene_get_emitter(const sph_scene* s, unsigned k, sph_emitter_desc* out)
 {
@@ -336,6 +372,8 @@ int sph_create_from_scene(const sph_scene* s, sph_ctx** out)
     if ((rc = sph_set_fluid(ctx, sph_scene_num_fluid(s), s->fluid.data(), s->fluid_v.data())) != SPH_OK ||
         (rc = sph_set_boundary(ctx, sph_scene_num_boundary(s), s->boundary.data())) != SPH_OK)
         return rc; /* the context stays valid; sph_last_error(ctx) explains */
+    for (const sph_scene::Cube& b : s->cubes)
+        if ((rc = sph_add_cube_boundary(ctx, b.mn, b.mx, 0.0f, 0.0f)) != SPH_OK) return rc;
     for (const sph_emitter_desc& e : s->emitters)
         if ((rc = sph_add_emitter(ctx, &e)) != SPH_OK) return rc;
     if ((rc = sph_init(ctx)) != SPH_OK) return rc;

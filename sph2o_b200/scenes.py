@@ -75,6 +75,7 @@ def scene(
     density0=1000.0,
     jitter=0.01,
     seed=1,
+    boundary_method=BOUNDARY_AKINCI,
 ):
     """Build one scene dict. `blocks` are (min, max) pairs; `tank` is (min, max)."""
     cfg = {
@@ -87,7 +88,7 @@ def scene(
         "gravity": f32(list(gravity)),
         "particleRadius": f32(radius),
         "simulationMethod": int(method),
-        "boundaryMethod": BOUNDARY_AKINCI,
+        "boundaryMethod": int(boundary_method),
         "cflFactor": f32(cfl),
         "jitter": f32(jitter),
         "jitterSeed": int(seed),
@@ -238,6 +239,19 @@ def emitter_scenes():
     with_emitter(df, etype=1, position=(0.35 * tank[0], 0.5 * tank[1], 0.5 * tank[2]), rotation=q, velocity=4.0,
                  num_particles=3 * 19, width=0.11, spacing=1.2)
     return {"emitter_wcsph_square": wc, "emitter_dfsph_circle": df}
+
+
+def cube_scenes():
+    """Cube-boundary scenes (boundaryMethod 0: no boundary particles, the
+    fluid is clamped into the box after every step). WCSPH: the block's last
+    x layers start outside the box, so the first step clamps them. DFSPH: the
+    block's bottom layer starts below the floor and the rest falls onto it."""
+    r = 0.025
+    wc = scene(method=WCSPH, radius=r, blocks=[block((8, 6, 6), r, (4 * r,) * 3)],
+               tank=((0, 0, 0), (0.4, 1.0, 1.0)), time_step=2e-4, seed=41, boundary_method=BOUNDARY_CUBE)
+    df = scene(method=DFSPH, radius=r, blocks=[block((6, 6, 6), r, (4 * r, 4 * r, -2 * r))],
+               tank=((0, 0, 0), (1.0, 1.0, 1.0)), time_step=5e-4, seed=42, boundary_method=BOUNDARY_CUBE)
+    return {"cube_wcsph_outside": wc, "cube_dfsph_floor": df}
 
 
 def batched_scene_params(count=256, seed=4):

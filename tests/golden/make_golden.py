@@ -47,7 +47,7 @@ from sph2o_b200 import scenes as S  # noqa: E402
 
 NSTEPS = 20
 # emitter scenes run long enough for several emissions
-STEPS = {"emitter_wcsph_square": 120, "emitter_dfsph_circle": 120}
+STEPS = {"emitter_wcsph_square": 120, "emitter_dfsph_circle": 120, "cube_dfsph_floor": 120}
 REF32 = os.path.join(ROOT, "oracle", "_ref", "sph2o_ref_f32")
 REF64 = os.path.join(ROOT, "oracle", "_ref", "sph2o_ref_f64")
 
@@ -55,6 +55,7 @@ REF64 = os.path.join(ROOT, "oracle", "_ref", "sph2o_ref_f64")
 def golden_scenes():
     return {
         **S.emitter_scenes(),
+        **S.cube_scenes(),
         "dfsph_st_sphere": S.small(method=S.DFSPH, surface_tension=0.05, sphere=True),
         "wcsph_artificial": S.small(method=S.WCSPH, n=(12, 10, 10)),
         "pcisph_artificial": S.small(method=S.PCISPH, n=(10, 10, 12), eta=0.01, time_step=5e-4),
@@ -82,7 +83,7 @@ def make(name, scene, td):
     for k in ("init_pos", "bpos", "nbr_f_offsets", "nbr_f", "nbr_b_offsets", "nbr_b"):
         g[k] = nb[k]
     ph = run(REF32, path, "phases", os.path.join(td, "ph.sphd"))
-    g["bvol"] = ph["bvol"]
+    g["bvol"] = ph.get("bvol", np.zeros(0, np.float32))  # absent without Akinci boundary particles
     g["density"] = ph["density"]
     g["a_np"] = ph["a_nonpressure"]
     for k in ("alpha", "pressure", "a_pressure"):

@@ -92,7 +92,7 @@ def test_call_order_errors():
     L.sph_destroy(h)
     bad = SceneDesc()
     C.memmove(C.byref(bad), C.byref(d), C.sizeof(d))
-    bad.boundary_method = 0
+    bad.boundary_method = 1  # PCISPH boundary particles: not implemented
     assert L.sph_create(C.byref(bad), C.byref(h)) == -1
 
 

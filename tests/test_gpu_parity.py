@@ -11,10 +11,12 @@ Tolerances (FP32 everywhere, as the reference):
     FP32 build is ~1e-4 away from its FP64 build after one step; the bar is
     that the GPU is no further from the FP64 oracle than 1.5x the FP32
     reference's own distance (and within 2e-4 of the FP32 reference);
-  * 20-step trajectories: iteration counts equal to the FP32 reference's at
-    every step, time and dt within 1e-5 relative, and against the FP64
-    reference: centroid within 1e-6 m, kinetic energy within 2e-3 relative,
-    mean density error within 1e-6 (absolute, in units of rho0).
+  * 20-step trajectories (120 for the cube-boundary DFSPH scene): iteration
+    counts equal to the FP32 reference's at every step, time and dt within
+    1e-5 relative, and against the FP64 reference: centroid within 1e-6 m,
+    kinetic energy within 2e-3 relative, mean density error within 1e-6
+    (absolute, in units of rho0) -- or within twice the FP32 reference's own
+    distance from the FP64 one, where that is larger.
 """
 import numpy as np
 import pytest
@@ -120,7 +122,10 @@ def test_trajectory(name):
     centroid = x64.mean(axis=0)
     ke = 0.5 * mass * float((v64 * v64).sum())
     derr = float(np.mean(np.maximum(rho.astype(np.float64) - rho0, 0.0) / rho0))
-    last = ref64[-1]
-    assert np.max(np.abs(centroid - last[6:9])) <= 1e-6
-    assert abs(ke - last[9]) <= 2e-3 * abs(last[9])
-    assert abs(derr - last[10]) <= 1e-6
+    last, last32 = ref64[-1], ref32[-1]
+    # within the bars, or within twice the FP32 reference's own distance from
+    # FP64 where that is larger (long or violent traces, e.g. the cube scene)
+    spread = np.abs(last32 - last)
+    assert np.max(np.abs(centroid - last[6:9])) <= max(1e-6, 2 * float(np.max(spread[6:9])))
+    assert abs(ke - last[9]) <= max(2e-3 * abs(last[9]), 2 * float(spread[9]))
+    assert abs(derr - last[10]) <= max(1e-6, 2 * float(spread[10]))
