@@ -384,8 +384,13 @@ typedef struct sph_scene sph_scene;
 /* Replaces SceneLoader::readConfiguration (SceneLoader.cpp:11-209) and the
    object construction of SPHSimulation::importScene (SPHSimulation.cpp:299-481):
    FluidObject::build lattice (FluidObject.cpp:30-61), seeded jitter,
-   AkinciBoundaryObject::sampleCube/sampleSphere (AkinciBoundaryObject.cpp:97-153).
-   Missing "sphere"/"geometry" keys are tolerated. */
+   AkinciBoundaryObject::sampleCube/sampleSphere (AkinciBoundaryObject.cpp:97-153)
+   and addGeometry (:74-95) for OBJ "geometry" entries (see sph_sample_geometry).
+   Missing "sphere"/"geometry" keys are tolerated. A relative geometry path
+   is opened as given, else relative to the scene file's directory.
+   Returns SPH_ERR_IO for unreadable files or malformed JSON, SPH_ERR_ARG for
+   unsupported options or malformed meshes, SPH_ERR_CAPACITY for a mesh
+   sampled into more than 2^30 points. */
 int sph_scene_load(const char* json_path, sph_scene** out);
 int sph_scene_parse(const char* json_text, sph_scene** out);
 int sph_scene_get_desc(const sph_scene* s, sph_scene_desc* out);
@@ -403,6 +408,33 @@ int sph_scene_get_fluid(const sph_scene* s, float* xyz, float* v);
 int sph_scene_get_boundary(const sph_scene* s, float* xyz);
 const char* sph_scene_error(void);
 void sph_scene_free(sph_scene* s);
+
+/* ---- triangle meshes as boundary particles --------------------------- */
+
+/* Replaces SPH::RegularTriangleSampling::sampleMesh
+   (extern/RegularTriangleSampling/RegularTriangleSampling.cpp:12-20):
+   `vertices` holds num_vertices xyz triples, `faces` num_faces 0-based index
+   triples. The samples are every vertex, then the interior stops of each
+   unique edge, then the interior stops of each face's lines parallel to
+   its longest edge, at most max_distance apart, bit-identical to the
+   reference's FP32 build. Two-call convention: *count receives the number
+   of xyz samples; `samples` (NULL to query) receives them when `capacity`
+   (in points) suffices, else SPH_ERR_CAPACITY. SPH_ERR_ARG for a bad index,
+   a non-finite vertex or max_distance <= 0; text in sph_scene_error(). */
+int sph_sample_mesh(const float* vertices, unsigned num_vertices, const unsigned* faces, unsigned num_faces,
+                    float max_distance, float* samples, size_t capacity, size_t* count);
+
+/* Replaces AkinciBoundaryObject::sampleGeometry
+   (src/SPH2O/BoundaryObject/AkinciBoundaryObject.cpp:155-214): reads a
+   triangulated OBJ file (OBJLoader::loadObj, extern/OBJLoader/OBJLoader.h:31-158;
+   coordinates times `scale`), samples it as sph_sample_mesh does, then maps
+   each sample p to R (p, 1) + translate with R = glm::rotate(I, rotate[0], x)
+   -> (.., rotate[1], y) -> (.., rotate[2], z). NULL scale/translate/rotate
+   mean 1, 0, 0. Scene geometries use scale 1, translate 0, rotate (pi/2, 0, 0)
+   (AkinciBoundaryObject::addGeometry, :74-80). SPH_ERR_IO for an unreadable
+   file; otherwise as sph_sample_mesh. */
+int sph_sample_geometry(const char* obj_path, float max_distance, const float scale[3], const float translate[3],
+                        const float rotate[3], float* samples, size_t capacity, size_t* count);
 
 /* create + set_fluid + set_boundary + add_cube_boundary + add_emitter + init
    from a loaded scene. */

@@ -144,6 +144,8 @@ def lib():
         "sph_wcsph_backward": (I, [P, F, F, F]),
         "sph_wcsph_grad_x0": (I, [P, F]),
         "sph_wcsph_timing": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "sph_sample_mesh": (I, [F, U, C.POINTER(U), U, C.c_float, F, C.c_size_t, C.POINTER(C.c_size_t)]),
+        "sph_sample_geometry": (I, [C.c_char_p, C.c_float, F, F, F, F, C.c_size_t, C.POINTER(C.c_size_t)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
@@ -165,6 +167,37 @@ def select_device(device: int):
     rc = lib().sph_select_device(int(device))
     if rc != SPH_OK:
         raise SphError(rc, lib().sph_global_error().decode())
+
+
+def _two_call(call):
+    """Runs a sampler entry point twice: once for the count, once to fill."""
+    n = C.c_size_t()
+    rc = call(None, 0, C.byref(n))
+    if rc != SPH_OK:
+        raise SphError(rc, lib().sph_scene_error().decode())
+    out = np.zeros((n.value, 3), np.float32)
+    rc = call(_fptr(out), n.value, C.byref(n))
+    if rc != SPH_OK:
+        raise SphError(rc, lib().sph_scene_error().decode())
+    return out
+
+
+def sample_mesh(vertices, faces, max_distance):
+    """Regular triangle sampling of a mesh (RegularTriangleSampling::sampleMesh):
+    vertices (V, 3) float, faces (F, 3) 0-based indices -> samples (S, 3)."""
+    v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+    f = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
+    return _two_call(lambda out, cap, n: lib().sph_sample_mesh(_fptr(v), len(v), _uptr(f), len(f),
+                                                                float(max_distance), out, cap, n))
+
+
+def sample_geometry(path, max_distance, scale=None, translate=None, rotate=None):
+    """OBJ file -> boundary samples (AkinciBoundaryObject::sampleGeometry):
+    scaled, sampled, turned by glm::rotate about x, y, z (radians), translated."""
+    vec = lambda a: None if a is None else np.ascontiguousarray(a, np.float32).reshape(3)
+    s, t, r = vec(scale), vec(translate), vec(rotate)
+    return _two_call(lambda out, cap, n: lib().sph_sample_geometry(os.fsencode(path), float(max_distance), _fptr(s),
+                                                                    _fptr(t), _fptr(r), out, cap, n))
 
 
 class Scene:

@@ -23,7 +23,7 @@ DRIVER = os.path.join(HERE, "bin", "sph2o")
 
 CUDA_SOURCES = ["csrc/sph_grid.cu", "csrc/sph_solvers.cu", "csrc/sph_capi.cu", "csrc/sph_noalloc.cu",
                 "csrc/sph_adjoint.cu"]
-HOST_SOURCES = ["host/scene.cpp"]
+HOST_SOURCES = ["host/scene.cpp", "host/geometry.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -6,10 +6,15 @@
  *   - SceneLoader::readSceneInfo/readFluidInfo/readBoundaryInfo
  *     (src/SPH2O/SceneLoader.cpp:40-209): same keys, same conditional reads;
  *   - SPHSimulation::importScene (src/SPH2O/SPHSimulation.cpp:299-481): one
- *     fluid model, Akinci boundary objects built box-then-sphere per object;
+ *     fluid model, Akinci boundary objects built box, then sphere, then
+ *     geometry per object;
  *   - FluidObject::build (src/SPH2O/FluidObject/FluidObject.cpp:30-61);
  *   - AkinciBoundaryObject::sampleCube / sampleSphere
- *     (src/SPH2O/BoundaryObject/AkinciBoundaryObject.cpp:97-153).
+ *     (src/SPH2O/BoundaryObject/AkinciBoundaryObject.cpp:97-153);
+ *   - AkinciBoundaryObject::addGeometry (:74-95): OBJ "geometry" entries
+ *     sampled at spacing * particleRadius * 2 (SPHSimulation.cpp:422-423)
+ *     with scale 1, no translation and a fixed rotation of pi/2 about x
+ *     (geometry.cpp holds the loader and the sampler).
  * The arithmetic keeps SPH2O's types operation by operation (float where the
  * reference computes in float, double where its unqualified pow/sin/cos/
  * round/floor calls resolve to the double overloads), so the generated
@@ -24,17 +29,25 @@
  * cube boundary (SPHSimulation.cpp:459-477), with the zero velocity factors
  * SPH2O's loader leaves it.
  *
+ * A relative geometry path is opened as given (relative to the working
+ * directory, as the reference does) and, failing that, relative to the
+ * directory of the scene file.
+ *
  * Not supported (rejected with SPH_ERR_ARG): more than one fluid model, the
- * PCISPH boundary method (1), OBJ "geometry" boundaries.
+ * PCISPH boundary method (1).
  */
 #include "../../include/sph2o_cuda.h"
+#include "geometry.h"
 #include "json_lite.h"
 #include "scene_rng.h"
 
 #include <cmath>
+#include <cstring>
 #include <fstream>
 #include <math.h>
+#include <memory>
 #include <sstream>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -138,6 +151,23 @@ unsigned uint_field(const sphjson::Value& cfg, const char* key)
     const double d = cfg.get(key).as_number(key);
     if (d < 0) throw sphjson::JsonError(std::string(key) + " must be non-negative");
     return (unsigned)d;
+}
+
+/* AkinciBoundaryObject::addGeometry (AkinciBoundaryObject.cpp:78-80): the
+   fixed placement of every scene geometry; the angle is M_PI * 0.5 rounded
+   to the reference's float Real */
+const float kGeomScale[3] = {1.0f, 1.0f, 1.0f};
+const float kGeomTranslate[3] = {0.0f, 0.0f, 0.0f};
+const float kGeomRotate[3] = {(float)(M_PI * 0.5), 0.0f, 0.0f};
+
+/* The path as given when it opens (the reference's behaviour), else a
+   relative path taken from the scene file's directory. */
+std::string resolve_geometry(const std::string& file, const std::string& scene_path)
+{
+    if (std::ifstream(file) || file.empty() || file[0] == '/' || scene_path.empty()) return file;
+    const size_t slash = scene_path.find_last_of('/');
+    if (slash == std::string::npos) return file;
+    return scene_path.substr(0, slash + 1) + file;
 }
 
 sph_scene* build_scene(const std::string& text, const std::string& path)
@@ -263,10 +293,51 @@ sph_scene* build_scene(const std::string& text, const std::string& path)
                     sample_sphere(vec3(sph->at(j).get("pos"), "sphere.pos"),
                                   num(sph->at(j).get("radius"), "sphere.radius"), d.particle_radius, scene->boundary);
             if (const sphjson::Value* geo = b.find("geometry"))
-                if (geo->size() > 0) throw std::invalid_argument("OBJ geometry boundaries are not supported");
+                for (size_t j = 0; j < geo->size(); ++j) {
+                    const float spacing = num(geo->at(j).get("spacing"), "geometry.spacing");
+                    const std::string file = resolve_geometry(geo->at(j).get("path").as_string("geometry.path"), path);
+                    std::vector<float> pts;
+                    sphgeo::sample_geometry(file, spacing * d.particle_radius * 2.0f, kGeomScale, kGeomTranslate,
+                                            kGeomRotate, pts);
+                    scene->boundary.insert(scene->boundary.end(), pts.begin(), pts.end());
+                }
         }
     }
     return scene.release();
+}
+
+/* Copies `pts` out through the two-call convention of the mesh entry points. */
+int emit_samples(const std::vector<float>& pts, float* samples, size_t capacity, size_t* count)
+{
+    const size_t n = pts.size() / 3;
+    if (count) *count = n;
+    if (!samples) return SPH_OK;
+    if (capacity < n) {
+        g_scene_error = "sample buffer holds " + std::to_string(capacity) + " points, " + std::to_string(n) +
+                        " needed";
+        return SPH_ERR_CAPACITY;
+    }
+    std::memcpy(samples, pts.data(), pts.size() * sizeof(float));
+    return SPH_OK;
+}
+
+template <class F>
+int guarded(F&& f)
+{
+    try {
+        const int rc = f();
+        if (rc == SPH_OK) g_scene_error.clear();
+        return rc;
+    } catch (const std::invalid_argument& e) {
+        g_scene_error = e.what();
+        return SPH_ERR_ARG;
+    } catch (const std::length_error& e) {
+        g_scene_error = e.what();
+        return SPH_ERR_CAPACITY;
+    } catch (const std::exception& e) {
+        g_scene_error = e.what();
+        return SPH_ERR_IO;
+    }
 }
 
 int load_common(const std::string& text, const std::string& path, sph_scene** out)
@@ -283,6 +354,9 @@ int load_common(const std::string& text, const std::string& path, sph_scene** ou
     } catch (const std::invalid_argument& e) {
         g_scene_error = e.what();
         return SPH_ERR_ARG;
+    } catch (const std::length_error& e) {
+        g_scene_error = e.what();
+        return SPH_ERR_CAPACITY;
     } catch (const std::exception& e) {
         g_scene_error = e.what();
         return SPH_ERR_IO;
@@ -360,6 +434,36 @@ int sph_scene_get_boundary(const sph_scene* s, float* xyz)
 }
 
 const char* sph_scene_error(void) { return g_scene_error.c_str(); }
+
+int sph_sample_mesh(const float* vertices, unsigned num_vertices, const unsigned* faces, unsigned num_faces,
+                    float max_distance, float* samples, size_t capacity, size_t* count)
+{
+    if ((!vertices && num_vertices) || (!faces && num_faces)) {
+        g_scene_error = "null mesh array";
+        return SPH_ERR_ARG;
+    }
+    return guarded([&] {
+        std::vector<float> pts;
+        sphgeo::sample_mesh(vertices, num_vertices, faces, num_faces, max_distance, pts);
+        return emit_samples(pts, samples, capacity, count);
+    });
+}
+
+int sph_sample_geometry(const char* obj_path, float max_distance, const float scale[3], const float translate[3],
+                        const float rotate[3], float* samples, size_t capacity, size_t* count)
+{
+    if (!obj_path) {
+        g_scene_error = "null path";
+        return SPH_ERR_ARG;
+    }
+    const float one[3] = {1.0f, 1.0f, 1.0f}, zero[3] = {0.0f, 0.0f, 0.0f};
+    return guarded([&] {
+        std::vector<float> pts;
+        sphgeo::sample_geometry(obj_path, max_distance, scale ? scale : one, translate ? translate : zero,
+                                rotate ? rotate : zero, pts);
+        return emit_samples(pts, samples, capacity, count);
+    });
+}
 
 void sph_scene_free(sph_scene* s) { delete s; }
 

@@ -254,6 +254,91 @@ def cube_scenes():
     return {"cube_wcsph_outside": wc, "cube_dfsph_floor": df}
 
 
+def cup_obj(*, segments=12, r_bottom=0.3, r_top=0.4, height=0.45):
+    """OBJ text of a flared open cup in y-up coordinates (a scene geometry is
+    turned by pi/2 about x, so y becomes z): a fan floor at y = 0 and a ring
+    of wall quads split in two triangles, written with vertex normals
+    ("f v//n"), comment, object and smoothing lines."""
+    lines = ["# flared cup, y up", "o cup"]
+    ring = [2 * math.pi * k / segments for k in range(segments)]
+    lines.append("v 0 0 0")
+    for rad, y in ((r_bottom, 0.0), (r_top, height)):
+        for t in ring:
+            lines.append("v %.9g %.9g %.9g" % (f32(rad * math.cos(t)), f32(y), f32(rad * math.sin(t))))
+    lines += ["vn 0 1 0", "s off"]
+    b = lambda k: 2 + k % segments              # bottom ring, 1-based
+    t = lambda k: 2 + segments + k % segments   # top ring
+    for k in range(segments):
+        lines.append("f 1//1 %d//1 %d//1" % (b(k + 1), b(k)))
+        lines.append("f %d//1 %d//1 %d//1" % (b(k), b(k + 1), t(k + 1)))
+        lines.append("f %d//1 %d//1 %d//1" % (b(k), t(k + 1), t(k)))
+    return "\n".join(lines) + "\n"
+
+
+def quirks_obj():
+    """OBJ text that exercises the loader's and the sampler's corner cases:
+    "v/vt/vn" faces, a face with a repeated vertex (a zero-length edge), a
+    face whose vertices are (nearly) collinear, a long thin face, a
+    four-entry face (only its first three entries count), CRLF line ends."""
+    lines = [
+        "# corner cases", "o quirks", "g part",
+        "v 0 0 0", "v 0.37 0.01 -0.02", "v 0.05 0.29 0.11", "v 0.4 0.33 0.2",
+        "v 0.2 0.165 0.1", "v 1.3 -0.2 0.05", "v 1.31 -0.18 0.06",
+        "vt 0 0", "vt 1 0", "vt 0 1", "vn 0 0 1",
+        "f 1/1/1 2/2/1 3/3/1", "f 2/1/1 4/2/1 3/3/1", "f 1/1/1 5/2/1 4/3/1",
+        "f 2/1/1 2/2/1 6/3/1", "f 2/1/1 6/2/1 7/3/1", "f 7/1/1 6/2/1 2/3/1 4/1/1",
+    ]
+    return "\r\n".join(lines) + "\r\n"
+
+
+def shards_obj(seed=7, vertices=12, faces=16):
+    """OBJ text of a seeded soup of random triangles (plain "f a b c"
+    faces): irregular float coordinates, so the sampler's rounding order
+    shows in the last bits of the samples."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.array([0.6, -0.1, -0.3]), np.array([1.4, 0.3, 0.2])
+    v = (lo + rng.random((vertices, 3)) * (hi - lo)).astype(np.float32)
+    lines = ["v %.9g %.9g %.9g" % tuple(float(c) for c in p) for p in v]
+    for _ in range(faces):
+        a, b, c = rng.choice(vertices, 3, replace=False) + 1
+        lines.append("f %d %d %d" % (a, b, c))
+    return "\n".join(lines) + "\n"
+
+
+GEOMETRY_MESHES = {"cup.obj": cup_obj, "quirks.obj": quirks_obj, "shards.obj": shards_obj}
+
+
+def geometry_scenes():
+    """Akinci scenes whose boundary includes OBJ geometries (the files of
+    GEOMETRY_MESHES, referenced by bare file name). DFSPH: a block resting
+    just above the floor of the cup, with an outer tank box in the same
+    boundary object (box samples first, then the mesh). WCSPH: a
+    second boundary object of two meshes, the corner-case mesh sampled at
+    0.8 x 2r and a random triangle soup, beside a tank, a block above them."""
+    r = 0.025
+    df = scene(method=DFSPH, radius=r, blocks=[block((6, 6, 6), r, (-0.15, -0.15, 0.0))],
+               tank=((-0.6, -0.6, -0.3), (0.6, 0.6, 0.8)), time_step=5e-4, seed=51)
+    df["Boundary"][0]["geometry"] = [{"path": "cup.obj", "spacing": 1.0}]
+    wc = scene(method=WCSPH, radius=r, blocks=[block((6, 4, 4), r, (0.1, -0.3, 0.3))],
+               tank=((-0.2, -0.5, -0.3), (1.5, 0.4, 0.7)), time_step=2e-4, seed=52)
+    wc["Boundary"].append({"box": [], "sphere": [], "geometry": [{"path": "quirks.obj", "spacing": f32(0.8)},
+                                                                 {"path": "shards.obj", "spacing": 1.0}]})
+    return {"geometry_dfsph_cup": df, "geometry_wcsph_quirks": wc}
+
+
+def resolve_geometry_paths(scene_dict, directory):
+    """Copy of the scene with every relative geometry path joined to `directory`."""
+    import copy
+    import os
+
+    out = copy.deepcopy(scene_dict)
+    for b in out.get("Boundary", []):
+        for g in b.get("geometry", []):
+            if not os.path.isabs(g["path"]):
+                g["path"] = os.path.join(directory, g["path"])
+    return out
+
+
 def batched_scene_params(count=256, seed=4):
     """Per-scene parameters of the batched workload: N_f log-uniform in
     [2000, 40000], block aspect ratios uniform in [0.5, 2] (normalised so the

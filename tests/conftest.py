@@ -46,8 +46,12 @@ def emitter_golden_names():
 
 
 def load_golden(name):
+    """Fixture arrays; the scene's relative OBJ geometry paths point into
+    the golden directory."""
+    from sph2o_b200.scenes import resolve_geometry_paths
+
     g = dict(np.load(os.path.join(GOLDEN, name + ".npz")))
-    g["scene"] = json.loads(str(g["scene"]))
+    g["scene"] = resolve_geometry_paths(json.loads(str(g["scene"])), GOLDEN)
     return g
 
 

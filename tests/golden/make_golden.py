@@ -26,6 +26,10 @@ For every small scene below it stores, in <name>.npz:
   active_f32, active_f64   active fluid particles after every step (emitter
                    scenes; emitted particles take the slots after the active ones)
 
+The OBJ meshes of the geometry scenes (sph2o_b200.scenes.GEOMETRY_MESHES)
+are written beside the fixtures as <name>.obj; the stored scene refers to
+them by bare file name, the reference is run on a copy with absolute paths.
+
     python tests/golden/make_golden.py [name ...]    # default: every scene
 
 Test infrastructure only.
@@ -56,6 +60,7 @@ def golden_scenes():
     return {
         **S.emitter_scenes(),
         **S.cube_scenes(),
+        **S.geometry_scenes(),
         "dfsph_st_sphere": S.small(method=S.DFSPH, surface_tension=0.05, sphere=True),
         "wcsph_artificial": S.small(method=S.WCSPH, n=(12, 10, 10)),
         "pcisph_artificial": S.small(method=S.PCISPH, n=(10, 10, 12), eta=0.01, time_step=5e-4),
@@ -74,10 +79,16 @@ def run(binary, scene_path, mode, out, *extra):
     return sphd.read(out)
 
 
+def write_meshes():
+    for fname, text in S.GEOMETRY_MESHES.items():
+        with open(os.path.join(HERE, fname), "w", newline="") as f:
+            f.write(text())
+
+
 def make(name, scene, td):
     path = os.path.join(td, name + ".json")
     with open(path, "w") as f:
-        json.dump(scene, f)
+        json.dump(S.resolve_geometry_paths(scene, HERE), f)
     g = {"scene": np.array(json.dumps(scene))}
     nb = run(REF32, path, "neighbors", os.path.join(td, "nb.sphd"))
     for k in ("init_pos", "bpos", "nbr_f_offsets", "nbr_f", "nbr_b_offsets", "nbr_b"):
@@ -117,6 +128,7 @@ def main():
         if not os.path.exists(b):
             raise SystemExit(f"{b} missing: run make -C oracle first")
     want = set(sys.argv[1:])
+    write_meshes()
     with tempfile.TemporaryDirectory() as td:
         for name, scene in golden_scenes().items():
             if want and name not in want:

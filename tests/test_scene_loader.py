@@ -46,7 +46,8 @@ def test_missing_sphere_geometry_keys_tolerated():
     (lambda d: d["Fluid"]["FluidModel"].append(copy.deepcopy(d["Fluid"]["FluidModel"][0])), -1),
     (lambda d: d["Configuration"].__setitem__("boundaryMethod", 1), -1),
     (lambda d: d["Fluid"]["FluidModel"][0].__setitem__("emitters", [{"type": 0}]), -8),
-    (lambda d: d["Boundary"][0].__setitem__("geometry", [{"path": "x.obj", "spacing": 1.0}]), -1),
+    (lambda d: d["Boundary"][0].__setitem__("geometry", [{"path": "missing.obj", "spacing": 1.0}]), -8),
+    (lambda d: d["Boundary"][0].__setitem__("geometry", [{"spacing": 1.0}]), -8),
     (lambda d: d["Configuration"].__setitem__("simulationMethod", 7), -8),
 ])
 def test_bad_scenes_rejected(mutate, code):
