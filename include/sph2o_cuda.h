@@ -390,7 +390,8 @@ typedef struct sph_scene sph_scene;
    is opened as given, else relative to the scene file's directory.
    Returns SPH_ERR_IO for unreadable files or malformed JSON, SPH_ERR_ARG for
    unsupported options or malformed meshes, SPH_ERR_CAPACITY for a mesh
-   sampled into more than 2^30 points. */
+   sampled into more than 2^30 points. Scenes with geometry entries are
+   sampled on the current CUDA device (SPH_ERR_NO_DEVICE without one). */
 int sph_scene_load(const char* json_path, sph_scene** out);
 int sph_scene_parse(const char* json_text, sph_scene** out);
 int sph_scene_get_desc(const sph_scene* s, sph_scene_desc* out);
@@ -411,16 +412,27 @@ void sph_scene_free(sph_scene* s);
 
 /* ---- triangle meshes as boundary particles --------------------------- */
 
+/* Replaces Utilities::OBJLoader::loadObj (extern/OBJLoader/OBJLoader.h:31-158)
+   for triangulated meshes, on the host: vertex coordinates times `scale`
+   (NULL: 1) and 0-based triangle indices. *num_vertices / *num_faces
+   receive the counts; the arrays (NULL to query) receive the data when
+   their capacities suffice, else SPH_ERR_CAPACITY. SPH_ERR_IO for an
+   unreadable file, SPH_ERR_ARG for a malformed mesh. */
+int sph_load_obj(const char* obj_path, const float scale[3], float* vertices, size_t vertex_capacity,
+                 size_t* num_vertices, unsigned* faces, size_t face_capacity, size_t* num_faces);
+
 /* Replaces SPH::RegularTriangleSampling::sampleMesh
-   (extern/RegularTriangleSampling/RegularTriangleSampling.cpp:12-20):
-   `vertices` holds num_vertices xyz triples, `faces` num_faces 0-based index
-   triples. The samples are every vertex, then the interior stops of each
-   unique edge, then the interior stops of each face's lines parallel to
-   its longest edge, at most max_distance apart, bit-identical to the
-   reference's FP32 build. Two-call convention: *count receives the number
-   of xyz samples; `samples` (NULL to query) receives them when `capacity`
-   (in points) suffices, else SPH_ERR_CAPACITY. SPH_ERR_ARG for a bad index,
-   a non-finite vertex or max_distance <= 0; text in sph_scene_error(). */
+   (extern/RegularTriangleSampling/RegularTriangleSampling.cpp:12-20), run
+   on the current CUDA device (sph_select_device): `vertices` holds
+   num_vertices xyz triples, `faces` num_faces 0-based index triples. The
+   samples are every vertex, then the interior stops of each unique edge,
+   then the interior stops of each face's lines parallel to its longest
+   edge, at most max_distance apart, bit-identical to the reference's FP32
+   build. Two-call convention: *count receives the number of xyz samples;
+   `samples` (NULL to query) receives them when `capacity` (in points)
+   suffices, else SPH_ERR_CAPACITY. SPH_ERR_ARG for a bad index, a
+   non-finite vertex or max_distance <= 0; SPH_ERR_NO_DEVICE without a GPU;
+   text in sph_scene_error(). */
 int sph_sample_mesh(const float* vertices, unsigned num_vertices, const unsigned* faces, unsigned num_faces,
                     float max_distance, float* samples, size_t capacity, size_t* count);
 

@@ -33,6 +33,8 @@ def lib():
         L.sph_oracle_destroy.argtypes = [P]
         L.sph_oracle_wcsph_adjoint.argtypes = [P, C.c_double, C.c_double, C.c_uint, D, D, C.c_uint, D, C.c_int, D,
                                                D, D, D, D, D, D]
+        L.sph_oracle_sample_mesh.argtypes = [F, C.c_uint, U, C.c_uint, C.c_float, F, F, F, C.c_size_t,
+                                             C.POINTER(C.c_size_t)]
         _lib = L
     return _lib
 
@@ -110,6 +112,27 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+
+def sample_mesh(vertices, faces, max_distance, rotate=None, translate=None):
+    """Regular triangle sampling of a mesh on the CPU (mesh_sampling.cpp);
+    rotate / translate place the samples as sampleGeometry does."""
+    v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+    f = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
+    r = None if rotate is None else np.ascontiguousarray(rotate, np.float32).reshape(3)
+    t = None if translate is None else np.ascontiguousarray(translate, np.float32).reshape(3)
+    n = C.c_size_t()
+    L = lib()
+    rc = L.sph_oracle_sample_mesh(_f(v), len(v), _u(f), len(f), float(max_distance), _f(r), _f(t), None, 0,
+                                  C.byref(n))
+    if rc != 0:
+        raise ValueError(f"mesh sampling failed ({rc})")
+    out = np.zeros((n.value, 3), np.float32)
+    rc = L.sph_oracle_sample_mesh(_f(v), len(v), _u(f), len(f), float(max_distance), _f(r), _f(t), _f(out),
+                                  n.value, C.byref(n))
+    if rc != 0:
+        raise ValueError(f"mesh sampling failed ({rc})")
+    return out
 
 
 def wcsph_adjoint(desc, x0, v0, boundary, nsteps, target, nu=None, k=None, grad=True):

@@ -47,6 +47,14 @@ int sph_oracle_wcsph_adjoint(const sph_scene_desc* d, double nu, double k, unsig
                              const double* v0, unsigned nb, const double* bxyz, int nsteps, const double* target,
                              double* loss, double* x_out, double* dx0, double* dv0, double* dnu, double* dk);
 
+/* Regular triangle sampling of a mesh (mesh_sampling.cpp): vertices xyz,
+   0-based faces, spacing max_distance; rotate_xyz / translate (NULL: none)
+   place the samples as AkinciBoundaryObject::sampleGeometry does. Two-call
+   convention as sph_sample_mesh. */
+int sph_oracle_sample_mesh(const float* vertices, unsigned nv, const unsigned* faces, unsigned nf,
+                           float max_distance, const float rotate_xyz[3], const float translate[3], float* out,
+                           size_t capacity, size_t* count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -144,6 +144,8 @@ def lib():
         "sph_wcsph_backward": (I, [P, F, F, F]),
         "sph_wcsph_grad_x0": (I, [P, F]),
         "sph_wcsph_timing": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "sph_load_obj": (I, [C.c_char_p, F, F, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(U), C.c_size_t,
+                             C.POINTER(C.c_size_t)]),
         "sph_sample_mesh": (I, [F, U, C.POINTER(U), U, C.c_float, F, C.c_size_t, C.POINTER(C.c_size_t)]),
         "sph_sample_geometry": (I, [C.c_char_p, C.c_float, F, F, F, F, C.c_size_t, C.POINTER(C.c_size_t)]),
     }
@@ -182,9 +184,26 @@ def _two_call(call):
     return out
 
 
+def load_obj(path, scale=None):
+    """Triangulated OBJ file -> (vertices (V, 3) float32, faces (F, 3) uint32, 0-based)."""
+    s = None if scale is None else np.ascontiguousarray(scale, np.float32).reshape(3)
+    nv, nf = C.c_size_t(), C.c_size_t()
+    rc = lib().sph_load_obj(os.fsencode(path), _fptr(s), None, 0, C.byref(nv), None, 0, C.byref(nf))
+    if rc != SPH_OK:
+        raise SphError(rc, lib().sph_scene_error().decode())
+    v = np.zeros((nv.value, 3), np.float32)
+    f = np.zeros((nf.value, 3), np.uint32)
+    rc = lib().sph_load_obj(os.fsencode(path), _fptr(s), _fptr(v), nv.value, C.byref(nv), _uptr(f), nf.value,
+                            C.byref(nf))
+    if rc != SPH_OK:
+        raise SphError(rc, lib().sph_scene_error().decode())
+    return v, f
+
+
 def sample_mesh(vertices, faces, max_distance):
-    """Regular triangle sampling of a mesh (RegularTriangleSampling::sampleMesh):
-    vertices (V, 3) float, faces (F, 3) 0-based indices -> samples (S, 3)."""
+    """Regular triangle sampling of a mesh on the current GPU
+    (RegularTriangleSampling::sampleMesh): vertices (V, 3) float, faces
+    (F, 3) 0-based indices -> samples (S, 3)."""
     v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
     f = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
     return _two_call(lambda out, cap, n: lib().sph_sample_mesh(_fptr(v), len(v), _uptr(f), len(f),
@@ -192,8 +211,9 @@ def sample_mesh(vertices, faces, max_distance):
 
 
 def sample_geometry(path, max_distance, scale=None, translate=None, rotate=None):
-    """OBJ file -> boundary samples (AkinciBoundaryObject::sampleGeometry):
-    scaled, sampled, turned by glm::rotate about x, y, z (radians), translated."""
+    """OBJ file -> boundary samples on the current GPU
+    (AkinciBoundaryObject::sampleGeometry): scaled, sampled, turned by
+    glm::rotate about x, y, z (radians), translated."""
     vec = lambda a: None if a is None else np.ascontiguousarray(a, np.float32).reshape(3)
     s, t, r = vec(scale), vec(translate), vec(rotate)
     return _two_call(lambda out, cap, n: lib().sph_sample_geometry(os.fsencode(path), float(max_distance), _fptr(s),

@@ -22,7 +22,7 @@ LIB = os.path.join(HERE, "libsph2o_cuda.so")
 DRIVER = os.path.join(HERE, "bin", "sph2o")
 
 CUDA_SOURCES = ["csrc/sph_grid.cu", "csrc/sph_solvers.cu", "csrc/sph_capi.cu", "csrc/sph_noalloc.cu",
-                "csrc/sph_adjoint.cu"]
+                "csrc/sph_adjoint.cu", "csrc/sph_mesh.cu"]
 HOST_SOURCES = ["host/scene.cpp", "host/geometry.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -1,8 +1,9 @@
 /*
  * Host-side declarations of the kernel launchers (one CUDA stream each).
  * Kernels live in sph_grid.cu (neighbour search, sort, boundary volumes),
- * sph_solvers.cu (density, forces, WCSPH / PCISPH / DFSPH steps) and
- * sph_adjoint.cu (reverse-mode WCSPH step).
+ * sph_solvers.cu (density, forces, WCSPH / PCISPH / DFSPH steps),
+ * sph_adjoint.cu (reverse-mode WCSPH step); sph_mesh.h declares the mesh
+ * sampler of sph_mesh.cu.
  */
 #ifndef SPH2O_INTERNAL_H
 #define SPH2O_INTERNAL_H

@@ -328,6 +328,9 @@ int guarded(F&& f)
         const int rc = f();
         if (rc == SPH_OK) g_scene_error.clear();
         return rc;
+    } catch (const sphgeo::StatusError& e) {
+        g_scene_error = e.what();
+        return e.code;
     } catch (const std::invalid_argument& e) {
         g_scene_error = e.what();
         return SPH_ERR_ARG;
@@ -351,6 +354,9 @@ int load_common(const std::string& text, const std::string& path, sph_scene** ou
     } catch (const sphjson::JsonError& e) {
         g_scene_error = e.what();
         return SPH_ERR_IO;
+    } catch (const sphgeo::StatusError& e) {
+        g_scene_error = e.what();
+        return e.code;
     } catch (const std::invalid_argument& e) {
         g_scene_error = e.what();
         return SPH_ERR_ARG;
@@ -435,13 +441,33 @@ int sph_scene_get_boundary(const sph_scene* s, float* xyz)
 
 const char* sph_scene_error(void) { return g_scene_error.c_str(); }
 
+int sph_load_obj(const char* obj_path, const float scale[3], float* vertices, size_t vertex_capacity,
+                 size_t* num_vertices, unsigned* faces, size_t face_capacity, size_t* num_faces)
+{
+    if (!obj_path) {
+        g_scene_error = "null path";
+        return SPH_ERR_ARG;
+    }
+    const float one[3] = {1.0f, 1.0f, 1.0f};
+    return guarded([&] {
+        std::vector<float> v;
+        std::vector<unsigned> f;
+        sphgeo::load_obj(obj_path, scale ? scale : one, v, f);
+        if (num_vertices) *num_vertices = v.size() / 3;
+        if (num_faces) *num_faces = f.size() / 3;
+        if ((vertices && vertex_capacity < v.size() / 3) || (faces && face_capacity < f.size() / 3)) {
+            g_scene_error = "output arrays too small for the mesh";
+            return (int)SPH_ERR_CAPACITY;
+        }
+        if (vertices) std::memcpy(vertices, v.data(), v.size() * sizeof(float));
+        if (faces) std::memcpy(faces, f.data(), f.size() * sizeof(unsigned));
+        return (int)SPH_OK;
+    });
+}
+
 int sph_sample_mesh(const float* vertices, unsigned num_vertices, const unsigned* faces, unsigned num_faces,
                     float max_distance, float* samples, size_t capacity, size_t* count)
 {
-    if ((!vertices && num_vertices) || (!faces && num_faces)) {
-        g_scene_error = "null mesh array";
-        return SPH_ERR_ARG;
-    }
     return guarded([&] {
         std::vector<float> pts;
         sphgeo::sample_mesh(vertices, num_vertices, faces, num_faces, max_distance, pts);
