@@ -58,7 +58,7 @@ enum sph_status {
    that the particle path reads. */
 typedef struct sph_scene_desc {
     int simulation_method;          /* sph_method */
-    int boundary_method;            /* SPH_BOUNDARY_AKINCI or SPH_BOUNDARY_CUBE */
+    int boundary_method;            /* SPH_BOUNDARY_AKINCI, SPH_BOUNDARY_PCISPH or SPH_BOUNDARY_CUBE */
     int viscosity_method;           /* -1 none, 0 standard, 1 artificial, 2 XSPH */
     int surface_tension_method;     /* -1 none, 3 Akinci */
     int adhesion_method;            /* -1 none, 4 Akinci */
@@ -139,6 +139,22 @@ int sph_set_boundary(sph_ctx* ctx, unsigned n, const float* xyz);
    for this method, so scenes loaded by sph_scene_load carry 0 and 0 (a
    particle that hits a wall stops there), as in the reference. Before
    sph_init; single scenes only. */
+/* Replaces the per-particle normals n[] and setNormalFct / setTangentialFct
+   of PCISPHBoundaryObject (PCISPHBoundaryObject.h:8-26) for boundary_method
+   SPH_BOUNDARY_PCISPH: one normal per boundary particle of sph_set_boundary
+   (same order), before sph_init. The boundary particles then carry the mass
+   rho0 (2r)^3 and their own densities and pressures, and fluid particles
+   closer than h/2 are pushed out along the weighted boundary normal with
+   their velocity split into normal_fct and tangential_fct parts
+   (PCISPHBoundaryObject.cpp:218-447). One boundary object: SPH2O indexes a
+   boundary object's arrays with the candidates of all objects
+   (PCISPHBoundaryObject.cpp:242), which is well defined for one. */
+int sph_set_boundary_normals(sph_ctx* ctx, unsigned n, const float* normals, float normal_fct,
+                             float tangential_fct);
+/* Boundary densities and pressures of the PCISPH boundary method (the last
+   computed: by a step or sph_compute_phase), caller order; either pointer
+   may be NULL. */
+int sph_get_boundary_state(sph_ctx* ctx, float* density, float* pressure);
 int sph_add_cube_boundary(sph_ctx* ctx, const float min[3], const float max[3], float normal_fct,
                           float tangential_fct);
 
@@ -402,6 +418,11 @@ unsigned sph_scene_num_boundary(const sph_scene* s);
 unsigned sph_scene_num_cube_boundaries(const sph_scene* s);
 int sph_scene_get_cube_boundary(const sph_scene* s, unsigned k, float min[3], float max[3], float* normal_fct,
                                 float* tangential_fct);
+/* Boundary normals (nb x 3, the order of sph_scene_get_boundary) and the
+   object's normalFct / tangFct of a scene with boundaryMethod 1, sampled by
+   PCISPHBoundaryObject::sampleCube / sampleSphere
+   (PCISPHBoundaryObject.cpp:6-213); SPH_ERR_ARG for other methods. */
+int sph_scene_get_boundary_normals(const sph_scene* s, float* xyz, float* normal_fct, float* tangential_fct);
 /* Emitters of the scene's fluid model ("emitters" key, SceneLoader.cpp:109-143). */
 unsigned sph_scene_num_emitters(const sph_scene* s);
 int sph_scene_get_emitter(const sph_scene* s, unsigned k, sph_emitter_desc* out);
@@ -448,8 +469,8 @@ int sph_sample_mesh(const float* vertices, unsigned num_vertices, const unsigned
 int sph_sample_geometry(const char* obj_path, float max_distance, const float scale[3], const float translate[3],
                         const float rotate[3], float* samples, size_t capacity, size_t* count);
 
-/* create + set_fluid + set_boundary + add_cube_boundary + add_emitter + init
-   from a loaded scene. */
+/* create + set_fluid + set_boundary (+ set_boundary_normals) +
+   add_cube_boundary + add_emitter + init from a loaded scene. */
 int sph_create_from_scene(const sph_scene* s, sph_ctx** out);
 
 #ifdef __cplusplus

@@ -29,6 +29,7 @@
 #include "SPH2O/SPHSolver/PCISPHSolver.h"
 #include "SPH2O/SPHSolver/WCSPHSolver.h"
 #include "SPH2O/BoundaryObject/AkinciBoundaryObject.h"
+#include "SPH2O/BoundaryObject/PCISPHBoundaryObject.h"
 #include "SPH2O/HashTable.h"
 #include "json/json.hpp"
 
@@ -54,6 +55,10 @@ struct DFAccess : DFSPHSolver {
 };
 struct PCIAccess : PCISPHSolver {
     static Real& avgDens(PCISPHSolver* s) { return s->*(&PCIAccess::avgDensityError); }
+};
+/* Normals of PCISPH boundary particles (a protected member without a getter). */
+struct PCIBoundaryAccess : PCISPHBoundaryObject {
+    static std::vector<Vector3r>& normals(PCISPHBoundaryObject* o) { return o->*(&PCIBoundaryAccess::n); }
 };
 
 namespace {
@@ -239,6 +244,30 @@ std::vector<Real> fluid_density(FluidObject* fo)
     return out;
 }
 
+/* PCISPH boundary method: per-particle normals, and densities / pressures */
+bool pcisph_boundary(SPHSimulation* sim) { return sim->getBoundaryHandlingMethod() == SPHSimulation::PCISPH_BOUNDARY_METHOD; }
+
+std::vector<Real> boundary_scalars(SPHSimulation* sim, bool pressure)
+{
+    std::vector<Real> out;
+    for (uint b = 0; b < sim->numberBoundaryModels(); ++b) {
+        PCISPHBoundaryObject* bo = static_cast<PCISPHBoundaryObject*>(sim->getBoundaryModel(b));
+        for (uint i = 0; i < bo->getSize(); ++i) out.push_back(pressure ? bo->getPressure(i) : bo->getDensity(i));
+    }
+    return out;
+}
+
+std::vector<Real> boundary_normals(SPHSimulation* sim)
+{
+    std::vector<Real> out;
+    for (uint b = 0; b < sim->numberBoundaryModels(); ++b) {
+        PCISPHBoundaryObject* bo = static_cast<PCISPHBoundaryObject*>(sim->getBoundaryModel(b));
+        for (const Vector3r& v : PCIBoundaryAccess::normals(bo))
+            for (int k = 0; k < 3; ++k) out.push_back(v[k]);
+    }
+    return out;
+}
+
 void boundary_arrays(SPHSimulation* sim, std::vector<Real>& pos, std::vector<Real>& vol)
 {
     for (uint b = 0; b < sim->numberBoundaryModels(); ++b) {
@@ -351,6 +380,7 @@ int main(int argc, char** argv)
     w.put("init_vel", init_vel, {n, 3});
     w.put("bpos", bpos, {nb, 3});
     if (!bvol.empty()) w.put("bvol", bvol, {nb});
+    if (pcisph_boundary(sim)) w.put("bnormal", boundary_normals(sim), {nb, 3});
     std::vector<Real> mass(n);
     for (uint64_t i = 0; i < n; ++i) mass[i] = fo->getMass((uint)i);
     w.put("mass", mass, {n});
@@ -367,6 +397,7 @@ int main(int argc, char** argv)
         solver->neighborhoodSearch();
         solver->computeDensities();
         w.put("density", fluid_density(fo), {n});
+        if (pcisph_boundary(sim)) w.put("bdensity", boundary_scalars(sim, false), {nb});
         if (method == SPHSimulation::DFSPH_METHOD) {
             DFSPHSolver* df = static_cast<DFSPHSolver*>(solver);
             df->computeAlpha();
@@ -384,6 +415,7 @@ int main(int argc, char** argv)
             std::vector<Real> p(n);
             for (uint64_t i = 0; i < n; ++i) p[i] = fo->getPressure((uint)i);
             w.put("pressure", p, {n});
+            if (pcisph_boundary(sim)) w.put("bpressure", boundary_scalars(sim, true), {nb});
             wc->computePressureForce(0);
             w.put("a_pressure", fluid_vec3(fo, 2), {n, 3});
         }

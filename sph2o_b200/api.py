@@ -147,6 +147,9 @@ def lib():
         "sph_load_obj": (I, [C.c_char_p, F, F, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(U), C.c_size_t,
                              C.POINTER(C.c_size_t)]),
         "sph_sample_mesh": (I, [F, U, C.POINTER(U), U, C.c_float, F, C.c_size_t, C.POINTER(C.c_size_t)]),
+        "sph_set_boundary_normals": (I, [P, U, F, C.c_float, C.c_float]),
+        "sph_get_boundary_state": (I, [P, F, F]),
+        "sph_scene_get_boundary_normals": (I, [P, F, F, F]),
         "sph_sample_geometry": (I, [C.c_char_p, C.c_float, F, F, F, F, C.c_size_t, C.POINTER(C.c_size_t)]),
     }
     for name, (res, args) in sigs.items():
@@ -273,6 +276,17 @@ class Scene:
             out.append(e)
         return out
 
+    def boundary_normals(self):
+        """(normals (nb, 3), normal_fct, tangential_fct) of a boundaryMethod-1
+        scene, else None."""
+        if self.desc().boundary_method != 1:
+            return None
+        n = lib().sph_scene_num_boundary(self._h)
+        nrm = np.zeros((n, 3), np.float32)
+        nf, tf = C.c_float(), C.c_float()
+        lib().sph_scene_get_boundary_normals(self._h, _fptr(nrm), C.byref(nf), C.byref(tf))
+        return nrm, nf.value, tf.value
+
     def boundary(self):
         n = lib().sph_scene_num_boundary(self._h)
         b = np.zeros((n, 3), np.float32)
@@ -294,7 +308,9 @@ class Scene:
 class Simulation:
     """One GPU simulation context (sph_ctx)."""
 
-    def __init__(self, desc: SceneDesc, fluid, boundary, vel=None, emitters=(), cubes=()):
+    def __init__(self, desc: SceneDesc, fluid, boundary, vel=None, emitters=(), cubes=(), boundary_normals=None):
+        """boundary_normals: (normals (nb, 3), normal_fct, tangential_fct) for
+        the PCISPH boundary method (boundary_method 1)."""
         L = lib()
         h = C.c_void_p()
         rc = L.sph_create(C.byref(desc), C.byref(h))
@@ -307,6 +323,10 @@ class Simulation:
         b = np.ascontiguousarray(boundary, np.float32).reshape(-1, 3)
         self._check(L.sph_set_fluid(h, x.shape[0], _fptr(x), _fptr(v)))
         self._check(L.sph_set_boundary(h, b.shape[0], _fptr(b)))
+        if boundary_normals is not None:
+            nrm, nfct, tfct = boundary_normals
+            nrm = np.ascontiguousarray(nrm, np.float32).reshape(-1, 3)
+            self._check(L.sph_set_boundary_normals(h, nrm.shape[0], _fptr(nrm), float(nfct), float(tfct)))
         for mn, mx, nfct, tfct in cubes:
             mn = np.ascontiguousarray(mn, np.float32)
             mx = np.ascontiguousarray(mx, np.float32)
@@ -320,7 +340,7 @@ class Simulation:
     def from_scene(cls, scene: Scene, vel=None):
         x, v = scene.fluid()
         return cls(scene.desc(), x, scene.boundary(), v if vel is None else vel, emitters=scene.emitters(),
-                   cubes=scene.cube_boundaries())
+                   cubes=scene.cube_boundaries(), boundary_normals=scene.boundary_normals())
 
     def num_active(self):
         n = C.c_uint()
@@ -343,6 +363,13 @@ class Simulation:
         s = StepStats()
         self._check(lib().sph_sync(self._h, C.byref(s)))
         return s.as_dict()
+
+    def boundary_state(self):
+        """(densities, pressures) of PCISPH boundary particles, caller order."""
+        d = np.zeros(self.nb, np.float32)
+        p = np.zeros(self.nb, np.float32)
+        self._check(lib().sph_get_boundary_state(self._h, _fptr(d), _fptr(p)))
+        return d, p
 
     def state(self):
         x = np.zeros((self.nf, 3), np.float32)

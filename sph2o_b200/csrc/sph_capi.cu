@@ -40,6 +40,7 @@ struct Buffers {
     float4 *pos, *pos2, *vel, *vel2;
     unsigned *orig, *orig2;
     float *kws, *kws2, *kvws, *kvws2;
+    float4 *normal, *normal2;
     bool lists_valid;
 };
 
@@ -107,6 +108,15 @@ struct sph_ctx {
     int solver_tpp = 2;  /* measured best on B200 for the 1M-particle scene (1, 2, 4: 1.03, 0.84, 0.92 ms) */
     float4* braw = nullptr;      /* boundary in caller order (re-sorted when the cell order changes) */
     unsigned* bid = nullptr;
+    /* PCISPH boundary method: boundary normals (caller order on the host,
+       sorted on the device), boundary densities / pressures / p over rho^2,
+       predicted velocities, the spare normal buffer of the DFSPH sort and
+       the per-cell search that first listed each cell */
+    std::vector<float> h_bnormal;
+    float pcib_nf = 0.0f, pcib_tf = 0.0f;
+    float4 *bnormal = nullptr, *normal2 = nullptr, *predv = nullptr;
+    float *bdens = nullptr, *bpress = nullptr, *bdp = nullptr;
+    unsigned* cell_entry = nullptr;
     /* autotune snapshot */
     float4 *snap_pos = nullptr, *snap_vel = nullptr;
     unsigned* snap_orig = nullptr;
@@ -265,6 +275,13 @@ void derive_params(sph_ctx* c)
     P.st = d.surface_tension;
     P.adh_on = (d.adhesion_method == SPH_ADHESION_AKINCI && d.adhesion != 0.0f) ? 1 : 0;
     P.adh = d.adhesion;
+    /* PCISPH boundary method: boundary viscosity is an Akinci-only term
+       (ArtificialViscosity.cpp:39 and the other viscosity forces) */
+    P.pcib = d.boundary_method == SPH_BOUNDARY_PCISPH ? 1 : 0;
+    if (P.pcib) P.bvisc = 0.0f;
+    P.rest_r = 0.5f * h;
+    P.poly6_c = 315.0f / ((float)(64.0 * M_PI) * h9);
+    P.spiky_g = 45.0f / ((float)M_PI * h6);
     /* PCISPHSolver::computeScalingFactor (PCISPHSolver.cpp:403-436) at the initial dt */
     float sg[3] = {0, 0, 0}, ssq = 0.0f;
     for (int i = -1; i <= 1; i++)
@@ -328,6 +345,8 @@ DeviceArrays arrays(sph_ctx* c)
     A.bpos = c->bpos; A.bcell_start = c->bcell_start;
     A.nbr_f = c->nbr_f; A.cnt_f = c->cnt_f; A.nbr_b = c->nbr_b; A.cnt_b = c->cnt_b;
     A.accum = c->accum; A.st = c->st;
+    A.bnormal = c->bnormal; A.bdens = c->bdens; A.bpress = c->bpress; A.bdp = c->bdp;
+    A.predv = c->predv; A.cell_entry = c->cell_entry;
     if (c->nscenes) {
         A.sref.scenes = c->d_scenes;
         A.sref.scene_of = c->d_scene_of;
@@ -414,6 +433,9 @@ int neighbor_search(sph_ctx* c)
     if (c->desc.simulation_method == SPH_DFSPH) {
         g.f_in[0] = c->kws; g.f_out[0] = c->kws2;
         g.f_in[1] = c->kvws; g.f_out[1] = c->kvws2;
+        /* PCISPH boundary method: the collision normals of this step feed the
+           next step's velocity correction */
+        if (c->P.pcib) { g.v4_in[2] = c->normal; g.v4_out[2] = c->normal2; }
     }
     {
         Phase ph(c, SPH_PROF_SORT, 6);
@@ -426,11 +448,18 @@ int neighbor_search(sph_ctx* c)
     if (c->desc.simulation_method == SPH_DFSPH) {
         std::swap(c->kws, c->kws2);
         std::swap(c->kvws, c->kvws2);
+        if (c->P.pcib) std::swap(c->normal, c->normal2);
     }
     {
         Phase ph(c, SPH_PROF_LISTS, 1);
         launch_build_lists(c->P, SceneRef{c->d_scenes, c->d_scene_of}, c->pos, c->cell_start, c->bpos, c->bcell_start, c->nbr_f, c->cnt_f, c->nbr_b,
                            c->cnt_b, c->st, c->stream);
+    }
+    if (c->P.pcib) {
+        /* the fluid's cells get candidate lists at this search */
+        Phase ph(c, SPH_PROF_LISTS, 2);
+        launch_mark_entries(c->P, c->pos, (int)c->nf, c->P.dynamic ? &c->st->n_active : nullptr, c->cell_entry, c->st,
+                            true, c->stream);
     }
     c->lists_valid = true;
     return check_launch(c, "neighbour search");
@@ -466,12 +495,17 @@ int step_wcsph(sph_ctx* c)
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     DeviceArrays A = arrays(c);
     { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, false, true, c->pass_block, c->stream); }
+    if (c->P.pcib) { Phase ph(c, SPH_PROF_DENSITY, 1); launch_boundary_density(c->P, A, c->stream); }
     if (c->P.st_on) { Phase ph(c, SPH_PROF_NORMALS, 1); launch_normals(c->P, A, c->pass_block, c->stream); }
     { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_WCSPH, c->pass_block, c->stream); }
     std::swap(c->pos, c->pos2);
     std::swap(c->vel, c->vel2);
     c->lists_valid = false;
     cube_correct(c); /* WCSPHSolver.cpp:51-60 */
+    if (c->P.pcib) { /* WCSPHSolver.cpp:62-72 */
+        Phase ph(c, SPH_PROF_FORCES, 1);
+        launch_pcib_correct(c->P, arrays(c), true, c->stream);
+    }
     emit(c, true); /* WCSPHSolver.cpp:75: emission, then t += dt */
     return check_launch(c, "wcsph step");
 }
@@ -515,6 +549,10 @@ int step_dfsph(sph_ctx* c)
                        : launch_dfsph_solve(c->P, A, false, solve_grid(c, false), c->solver_occ, c->solver_tpp, c->stream);
     }
     if (e != 0) return fail(c, SPH_ERR_CUDA, std::string("dfsph density solver launch: ") + cudaGetErrorString((cudaError_t)e));
+    if (c->P.pcib) { /* DFSPHSolver.cpp:60-70 */
+        Phase ph(c, SPH_PROF_DENSITY_SOLVE, 1);
+        launch_pcib_correct(c->P, A, false, c->stream);
+    }
     emit(c, false); /* DFSPHSolver.cpp:72: after the position update, before the neighbour search */
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     A = arrays(c);
@@ -633,13 +671,15 @@ int eager_step(sph_ctx* c)
 
 Buffers get_buffers(const sph_ctx* c)
 {
-    return {c->pos, c->pos2, c->vel, c->vel2, c->orig, c->orig2, c->kws, c->kws2, c->kvws, c->kvws2, c->lists_valid};
+    return {c->pos, c->pos2, c->vel, c->vel2, c->orig, c->orig2, c->kws, c->kws2, c->kvws, c->kvws2, c->normal,
+            c->normal2, c->lists_valid};
 }
 
 void set_buffers(sph_ctx* c, const Buffers& b)
 {
     c->pos = b.pos; c->pos2 = b.pos2; c->vel = b.vel; c->vel2 = b.vel2; c->orig = b.orig; c->orig2 = b.orig2;
     c->kws = b.kws; c->kws2 = b.kws2; c->kvws = b.kvws; c->kvws2 = b.kvws2; c->lists_valid = b.lists_valid;
+    c->normal = b.normal; c->normal2 = b.normal2;
 }
 
 /* nsteps (1 or 2) steps as one CUDA graph, captured on first use for the
@@ -728,8 +768,12 @@ int sph_create(const sph_scene_desc* desc, sph_ctx** out)
     *out = nullptr;
     if (desc->simulation_method < SPH_WCSPH || desc->simulation_method > SPH_DFSPH)
         return fail(nullptr, SPH_ERR_ARG, "simulation_method must be 0, 1 or 2");
-    if (desc->boundary_method != SPH_BOUNDARY_AKINCI && desc->boundary_method != SPH_BOUNDARY_CUBE)
-        return fail(nullptr, SPH_ERR_ARG, "boundary methods 2 (Akinci) and 0 (cube) are implemented");
+    if (desc->boundary_method < SPH_BOUNDARY_CUBE || desc->boundary_method > SPH_BOUNDARY_AKINCI)
+        return fail(nullptr, SPH_ERR_ARG, "boundary_method must be 0 (cube), 1 (PCISPH) or 2 (Akinci)");
+    if (desc->boundary_method == SPH_BOUNDARY_PCISPH && desc->adhesion_method == SPH_ADHESION_AKINCI &&
+        desc->adhesion != 0.0f)
+        /* AdhesionForce reads Akinci volumes (AdhesionForce.cpp:22-29) */
+        return fail(nullptr, SPH_ERR_ARG, "adhesion needs Akinci boundary particles (boundary method 2)");
     if (!(desc->particle_radius > 0.0f) || !(desc->density0 > 0.0f) || !(desc->time_step > 0.0f) || !(desc->fps > 0.0f))
         return fail(nullptr, SPH_ERR_ARG, "particle_radius, density0, time_step and fps must be positive");
     if (desc->simulation_method == SPH_WCSPH && !(desc->gamma != 0.0f))
@@ -775,6 +819,20 @@ int sph_set_boundary(sph_ctx* c, unsigned n, const float* xyz)
     if (n > 0 && !xyz) return fail(c, SPH_ERR_ARG, "null positions");
     c->nb = n;
     c->h_bound.assign(xyz, xyz + 3ull * n);
+    return SPH_OK;
+}
+
+int sph_set_boundary_normals(sph_ctx* c, unsigned n, const float* normals, float normal_fct, float tangential_fct)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (c->initialized) return fail(c, SPH_ERR_STATE, "sph_set_boundary_normals after sph_init");
+    if (c->desc.boundary_method != SPH_BOUNDARY_PCISPH)
+        return fail(c, SPH_ERR_ARG, "boundary normals need boundary_method SPH_BOUNDARY_PCISPH");
+    if (n != c->nb) return fail(c, SPH_ERR_ARG, "one normal per boundary particle (call sph_set_boundary first)");
+    if (n > 0 && !normals) return fail(c, SPH_ERR_ARG, "null normals");
+    c->h_bnormal.assign(normals, normals + 3ull * n);
+    c->pcib_nf = normal_fct;
+    c->pcib_tf = tangential_fct;
     return SPH_OK;
 }
 
@@ -834,6 +892,13 @@ int sph_init(sph_ctx* c)
     }
     if (c->desc.boundary_method == SPH_BOUNDARY_CUBE && c->nb > 0)
         return fail(c, SPH_ERR_ARG, "the cube boundary method has no boundary particles");
+    if (c->P.pcib) {
+        if (c->nscenes) return fail(c, SPH_ERR_ARG, "the PCISPH boundary method applies to single scenes");
+        if (c->h_bnormal.size() != 3ull * c->nb)
+            return fail(c, SPH_ERR_ARG, "PCISPH boundary particles need their normals (sph_set_boundary_normals)");
+        P.pcib_nf = c->pcib_nf;
+        P.pcib_tf = c->pcib_tf;
+    }
     /* emitters: their particles are allocated inactive after the blocks */
     c->n_init = c->nf;
     std::vector<float> groups;
@@ -964,6 +1029,11 @@ int sph_init(sph_ctx* c)
     ALLOC(bpos, nb); ALLOC(bvol, nb); ALLOC(borig, nb);
     ALLOC(cnt_f, nf); ALLOC(cnt_b, nf);
     ALLOC(st, 1);
+    if (P.pcib) {
+        ALLOC(bnormal, nb); ALLOC(bdens, nb); ALLOC(bpress, nb); ALLOC(bdp, nb);
+        ALLOC(predv, nf); ALLOC(normal2, nf);
+        ALLOC(cell_entry, (size_t)P.ncells);
+    }
 #undef ALLOC
     c->pos_base = c->pos;
     c->orig_base = c->orig;
@@ -1028,16 +1098,29 @@ int sph_init(sph_ctx* c)
         float4* braw = c->braw;
         unsigned* bid = c->bid;
         CUDA_TRY(c, cudaMemcpyAsync(stage, c->h_bound.data(), 3 * nb * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-        launch_pack_v3((int)nb, stage, braw, 0.0f, c->stream);
+        /* w: the particle's density weight, rho0 V_b once the volumes are
+           known (Akinci) or the boundary mass m_b = rho0 (2r)^3 (PCISPH,
+           SPHSimulation.cpp:435-437), which equals the fluid mass */
+        launch_pack_v3((int)nb, stage, braw, P.pcib ? P.mass : 0.0f, c->stream);
         launch_iota((int)nb, bid, c->stream);
         GatherSet g{};
         g.orig_out = c->borig;
         g.v4_in[0] = braw;
         g.v4_out[0] = c->bpos;
+        float4* nraw = nullptr;
+        if (P.pcib) {
+            if ((rc = dalloc(c, &nraw, nb)) != SPH_OK) return rc;
+            CUDA_TRY(c, cudaStreamSynchronize(c->stream)); /* the stage buffer is reused */
+            CUDA_TRY(c, cudaMemcpyAsync(stage, c->h_bnormal.data(), 3 * nb * sizeof(float), cudaMemcpyHostToDevice,
+                                        c->stream));
+            launch_pack_v3((int)nb, stage, nraw, 0.0f, c->stream);
+            g.v4_in[1] = nraw;
+            g.v4_out[1] = c->bnormal;
+        }
         const SceneRef bref{c->d_scenes, c->d_bscene_of};
         launch_sort(P, bref, (int)nb, braw, c->cell_count, c->bcell_start, c->block_sums, c->cell_of, c->slot,
                     c->tmp_key, c->tmp_src, bid, g, c->stream);
-        launch_boundary_volume(P, bref, c->bpos, c->bcell_start, c->bvol, c->stream);
+        if (!P.pcib) launch_boundary_volume(P, bref, c->bpos, c->bcell_start, c->bvol, c->stream);
     } else {
         CUDA_TRY(c, cudaMemsetAsync(c->bcell_start, 0, ((size_t)P.ncells + 1) * sizeof(unsigned), c->stream));
     }
@@ -1066,6 +1149,9 @@ int sph_init(sph_ctx* c)
     s0.dt = c->desc.time_step;
     s0.n_active = c->n_init;
     CUDA_TRY(c, cudaMemcpyAsync(c->st, &s0, sizeof s0, cudaMemcpyHostToDevice, c->stream));
+    /* PCISPH boundary method: the boundary's cells hold lists from the first
+       search on (SPHSolver::init inserts the boundary first) */
+    if (P.pcib) launch_mark_entries(P, c->bpos, (int)nb, nullptr, c->cell_entry, c->st, false, c->stream);
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     if (c->desc.simulation_method == SPH_DFSPH) {
         /* DFSPHSolver::init: densities and alpha at the initial positions */
@@ -1222,10 +1308,31 @@ int sph_set_state(sph_ctx* c, const float* xyz, const float* v)
     return check_launch(c, "set_state");
 }
 
+int sph_get_boundary_state(sph_ctx* c, float* density, float* pressure)
+{
+    if (!c) return SPH_ERR_ARG;
+    if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_get_boundary_state before sph_init");
+    if (!c->P.pcib) return fail(c, SPH_ERR_ARG, "boundary densities exist for the PCISPH boundary method only");
+    if (c->nb == 0) return SPH_OK;
+    float* tmp = nullptr;
+    CUDA_TRY(c, cudaMallocAsync((void**)&tmp, c->nb * sizeof(float), c->stream));
+    for (int k = 0; k < 2; ++k) {
+        float* out = k == 0 ? density : pressure;
+        if (!out) continue;
+        launch_unsort_f((int)c->nb, c->borig, k == 0 ? c->bdens : c->bpress, tmp, c->stream);
+        CUDA_TRY(c, cudaMemcpyAsync(out, tmp, c->nb * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    }
+    cudaFreeAsync(tmp, c->stream);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_launch(c, "get_boundary_state");
+}
+
 int sph_get_boundary_volume(sph_ctx* c, float* vol)
 {
     if (!c || !vol) return SPH_ERR_ARG;
     if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_get_boundary_volume before sph_init");
+    if (c->P.pcib) return fail(c, SPH_ERR_ARG, "boundary volumes exist for the Akinci boundary method only");
     if (c->nb == 0) return SPH_OK;
     float* tmp = nullptr;
     CUDA_TRY(c, cudaMallocAsync((void**)&tmp, c->nb * sizeof(float), c->stream));
@@ -1323,6 +1430,9 @@ int sph_compute_phase(sph_ctx* c, int phase, float* out)
     DeviceArrays A = arrays(c);
     const bool eos = phase == SPH_PHASE_PRESSURE || phase == SPH_PHASE_PRESSURE_ACC;
     launch_density(c->P, A, phase == SPH_PHASE_ALPHA || c->desc.simulation_method == SPH_DFSPH, eos, c->pass_block, c->stream);
+    /* PCISPH boundary method: SPHSolver::computeDensities covers the
+       boundary particles too (SPHSolver.cpp:126-137), WCSPH their pressures */
+    if (c->P.pcib) launch_boundary_density(c->P, A, c->stream);
     const size_t nf = c->nf;
     float* tmp = nullptr;
     CUDA_TRY(c, cudaMallocAsync((void**)&tmp, 3 * nf * sizeof(float), c->stream));
@@ -1520,6 +1630,9 @@ int sph_set_option(sph_ctx* c, int option, int value)
         if (value != 0 && value != 1) return fail(c, SPH_ERR_ARG, "cell order is 0 or 1");
         if (!c->initialized) { c->P.cell_order = value; return SPH_OK; }
         if (value == c->P.cell_order) return SPH_OK;
+        if (c->P.pcib)
+            /* the per-cell search record is indexed by the cell order */
+            return fail(c, SPH_ERR_ARG, "with the PCISPH boundary method the cell order is set before sph_init");
         return apply_cell_order(c, value);
     case SPH_OPT_SOLVER_OCCUPANCY:
         if (value != 4 && value != 8) return fail(c, SPH_ERR_ARG, "solver occupancy is 4 or 8");
@@ -1559,6 +1672,9 @@ int sph_autotune(sph_ctx* c, int trial_steps, const char* cache_path, int* confi
     if (!c) return SPH_ERR_ARG;
     if (!c->initialized) return fail(c, SPH_ERR_STATE, "sph_autotune before sph_init");
     if (trial_steps < 1) return fail(c, SPH_ERR_ARG, "trial_steps must be positive");
+    if (c->P.pcib)
+        /* trial steps would advance the carried normals and the per-cell search record */
+        return fail(c, SPH_ERR_ARG, "sph_autotune is not available with the PCISPH boundary method");
     const std::string key = tune_key(c);
     int best[SPH_TUNE_COUNT] = {c->P.cell_order, c->solver_occ, c->pass_block, c->solver_tpp};
     int rc;
@@ -1805,6 +1921,8 @@ int adj_supported(sph_ctx* c)
     if (c->nscenes) return fail(c, SPH_ERR_ARG, "the WCSPH adjoint applies to a single scene, not to a batch");
     if (c->desc.simulation_method != SPH_WCSPH) return fail(c, SPH_ERR_ARG, "the adjoint differentiates the WCSPH step only");
     if (c->P.dynamic) return fail(c, SPH_ERR_ARG, "the WCSPH adjoint does not cover emitters");
+    if (c->desc.boundary_method != SPH_BOUNDARY_AKINCI)
+        return fail(c, SPH_ERR_ARG, "the WCSPH adjoint covers Akinci boundaries (boundary method 2) only");
     if (c->P.st_on || c->P.adh_on)
         return fail(c, SPH_ERR_ARG, "the WCSPH adjoint covers neither surface tension nor adhesion");
     if (c->P.visc_method != -1 && c->P.visc_method != SPH_VISCOSITY_ARTIFICIAL)

@@ -61,6 +61,12 @@ struct SimParams {
     unsigned capF, capB;       /* neighbour-list capacity per particle   */
     int cell_order;            /* 0: 4^3 bricks, Morton inside; 1: linear, x fastest */
     int dynamic;               /* emitters: passes cover DevState::n_active particles, nf is the capacity */
+    /* PCISPH boundary method (boundaryMethod 1): mass boundary particles */
+    int pcib;                  /* 1: boundary particles carry normals, densities and pressures */
+    float pcib_nf, pcib_tf;    /* normalFct, tangFct of the boundary object                     */
+    float rest_r;              /* collision distance 0.5 h (PCISPHBoundaryObject.cpp:222)        */
+    float poly6_c;             /* Poly6 315 / (64 pi h^9)                 (Poly6.h:25)            */
+    float spiky_g;             /* Spiky gradient 45 / (pi h^6)            (Spiky.h:25)            */
 };
 
 /* Device-resident solver state; read by the host after a step. */
@@ -79,6 +85,7 @@ struct DevState {
     unsigned bar_count, bar_gen;
     float last_vmax;
     unsigned n_active;          /* active fluid particles (emitters append to them) */
+    unsigned ns_epoch;          /* neighbour searches so far (PCISPH boundary cell entries) */
 };
 
 /* Fluid particles a pass covers: all nf, or with emitters the active prefix
@@ -479,6 +486,55 @@ __device__ __forceinline__ bool grid_barrier(DevState* st)
     }
     __syncthreads();
     return s_ok != 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* PCISPH boundary method helpers, in the reference's float operation order. */
+
+/* glm::length: sqrt((x x + y y) + z z) */
+__device__ __forceinline__ float glm_length(float x, float y, float z)
+{
+    return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
+}
+
+/* Poly6::W (Poly6.h:29-42): |r| squared after the square root, as written */
+__device__ __forceinline__ float poly6_W(float rx, float ry, float rz, const SimParams& P)
+{
+    const float m = glm_length(rx, ry, rz);
+    const float m2 = __fmul_rn(m, m);
+    if (!(m2 <= P.h2)) return 0.0f;
+    const float d = __fsub_rn(P.h2, m2);
+    return __fmul_rn(__fmul_rn(__fmul_rn(P.poly6_c, d), d), d);
+}
+
+/* Spiky::gradW (Spiky.h:44-55): (-c (h - |r|)^2 / |r|) r */
+__device__ __forceinline__ void spiky_gradW(float rx, float ry, float rz, const SimParams& P, float& gx, float& gy,
+                                            float& gz)
+{
+    const float m = glm_length(rx, ry, rz);
+    if (m != 0.0f && m <= P.h) {
+        const float d = __fsub_rn(P.h, m);
+        const float s = __fdiv_rn(__fmul_rn(__fmul_rn(-P.spiky_g, d), d), m);
+        gx = __fmul_rn(s, rx);
+        gy = __fmul_rn(s, ry);
+        gz = __fmul_rn(s, rz);
+    } else {
+        gx = gy = gz = 0.0f;
+    }
+}
+
+/* Whether the reference's hash table held a candidate list for cell c at
+   the last neighbour search. Its table keeps every cell ever touched (by an
+   insertion or by a lookup, HashTable.cpp:88-96) and computes lists for all
+   of them at each search (:23-86); a lookup of a cell first touched since
+   then finds empty lists. entry[c] is the search that first listed c (0:
+   never touched); a lookup of an untouched cell marks it for the next one. */
+__device__ __forceinline__ bool cell_listed(unsigned* entry, unsigned c, unsigned epoch)
+{
+    const unsigned e = entry[c];
+    if (e != 0u) return e <= epoch;
+    atomicCAS(&entry[c], 0u, epoch + 1u);
+    return false;
 }
 
 } // namespace sph

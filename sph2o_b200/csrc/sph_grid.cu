@@ -149,6 +149,7 @@ __global__ void __launch_bounds__(256) k_ns_rank_gather(int n, const unsigned* _
     if (g.cell_out) g.cell_out[dst] = c;
     if (g.v4_in[0]) g.v4_out[0][dst] = g.v4_in[0][src];
     if (g.v4_in[1]) g.v4_out[1][dst] = g.v4_in[1][src];
+    if (g.v4_in[2]) g.v4_out[2][dst] = g.v4_in[2][src];
     if (g.f_in[0]) g.f_out[0][dst] = g.f_in[0][src];
     if (g.f_in[1]) g.f_out[1][dst] = g.f_in[1][src];
 }
@@ -331,6 +332,26 @@ void launch_pack_v3(int n, const float* in3, float4* out, float w, cudaStream_t 
 void launch_iota(int n, unsigned* out, cudaStream_t s)
 {
     if (n > 0) k_iota<<<blocks_for(n, 256), 256, 0, s>>>(n, out);
+}
+
+/* Cells of n particles listed by the search now completing: entry = the
+   completed searches + 1 where still 0 (single-scene grids). */
+__global__ void __launch_bounds__(256) k_mark_entries(SimParams P, const float4* __restrict__ pos, int n,
+                                                      const unsigned* n_dev, unsigned* entry, const DevState* st)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (n_dev ? (int)*n_dev : n)) return;
+    const unsigned c = cell_index(pos[i], P.h, grid_single(P));
+    if (entry[c] == 0u) atomicCAS(&entry[c], 0u, st->ns_epoch + 1u);
+}
+
+__global__ void k_epoch_advance(DevState* st) { st->ns_epoch += 1u; }
+
+void launch_mark_entries(const SimParams& P, const float4* pos, int n, const unsigned* n_dev, unsigned* entry,
+                         DevState* st, bool advance, cudaStream_t s)
+{
+    if (n > 0) k_mark_entries<<<(n + 255) / 256, 256, 0, s>>>(P, pos, n, n_dev, entry, st);
+    if (advance) k_epoch_advance<<<1, 1, 0, s>>>(st);
 }
 
 } // namespace sph

@@ -21,8 +21,8 @@ struct GatherSet {
     const unsigned* n_dev;
     unsigned* orig_out;
     unsigned* cell_out;
-    const float4* v4_in[2];
-    float4* v4_out[2];
+    const float4* v4_in[3];
+    float4* v4_out[3];
     const float* f_in[2];
     float* f_out[2];
 };
@@ -59,6 +59,15 @@ struct DeviceArrays {
     unsigned* any_active; /* batch: per-iteration "some scene still iterates" flags */
     int nscenes;
     unsigned accum_stride;/* batch: doubles per scene in accum */
+    /* PCISPH boundary method (SimParams::pcib): boundary normals, densities,
+       pressures and p / rho^2 in boundary sorted order, predicted velocities,
+       and the per-cell search that first listed each cell */
+    const float4* bnormal;
+    float* bdens;
+    float* bpress;
+    float* bdp;
+    float4* predv;
+    unsigned* cell_entry;
 };
 
 /* sph_grid.cu */
@@ -99,6 +108,18 @@ int launch_dfsph_solve_batch(const SimParams& P, const DeviceArrays& A, bool div
 int launch_barrier_timeout_probe(DevState* st, cudaStream_t s);
 /* cube boundaries: clamp the active particles into each box in order */
 void launch_cube_correct(const SimParams& P, const DeviceArrays& A, const CubeBox* cubes, int ncubes, cudaStream_t s);
+/* PCISPH boundary method: mark the cells of n particles as listed by the
+   search now completing, then count it (two launches) */
+void launch_mark_entries(const SimParams& P, const float4* pos, int n, const unsigned* n_dev, unsigned* entry,
+                         DevState* st, bool advance, cudaStream_t s);
+/* boundary densities with the cubic spline at the current fluid positions,
+   the Tait pressure and p / rho^2 (WCSPH, SPHSolver.cpp:91-124,
+   WCSPHSolver.cpp:97-114) */
+void launch_boundary_density(const SimParams& P, const DeviceArrays& A, cudaStream_t s);
+/* collision correction of positions (and, for WCSPH, velocities) after the
+   position update (PCISPHBoundaryObject.cpp:218-388); wcsph selects the
+   velocity pass */
+void launch_pcib_correct(const SimParams& P, const DeviceArrays& A, bool wcsph, cudaStream_t s);
 /* emission of the nemit emitters' due groups (one block); advance: then t += dt */
 void launch_emit(const SimParams& P, const DeviceArrays& A, EmitterState* E, const float4* group, int nemit,
                  bool advance, cudaStream_t s);

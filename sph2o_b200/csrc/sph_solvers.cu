@@ -79,6 +79,101 @@ __device__ __forceinline__ void for_fluid_neighbors(const DeviceArrays& A, int i
 }
 
 /* ---------------------------------------------------------------------- */
+/* PCISPH boundary method (PCISPHBoundaryObject.cpp:218-447)                 */
+
+/* Collision sums over the boundary candidates of x's cell: particles within
+   rest_r of x (test position) weigh w = max(0, (rest_r - |y - x_b|) / rest_r)
+   with y the weight position (x itself, or the predicted position), and
+   contribute w, w (rest_r - |y - x_b|) and w n_b. */
+__device__ __forceinline__ void pcib_collide(const SimParams& P, const DeviceArrays& A, float4 x, float4 y,
+                                             float& wsum, float& w2sum, float3& avg)
+{
+    wsum = 0.0f;
+    w2sum = 0.0f;
+    avg = make_float3(0.0f, 0.0f, 0.0f);
+    for_cells27(x, P.h, grid_single(P), [&](unsigned c) {
+        const unsigned e = A.bcell_start[c + 1];
+        for (unsigned q = A.bcell_start[c]; q < e; ++q) {
+            const float4 xb = A.bpos[q];
+            if (!(glm_length(__fsub_rn(x.x, xb.x), __fsub_rn(x.y, xb.y), __fsub_rn(x.z, xb.z)) < P.rest_r)) continue;
+            const float l = glm_length(__fsub_rn(y.x, xb.x), __fsub_rn(y.y, xb.y), __fsub_rn(y.z, xb.z));
+            const float gap = __fsub_rn(P.rest_r, l);
+            const float w = fmaxf(0.0f, __fdiv_rn(gap, P.rest_r));
+            wsum = __fadd_rn(wsum, w);
+            w2sum = __fadd_rn(w2sum, __fmul_rn(w, gap));
+            const float4 nb = A.bnormal[q];
+            avg.x = __fadd_rn(avg.x, __fmul_rn(w, nb.x));
+            avg.y = __fadd_rn(avg.y, __fmul_rn(w, nb.y));
+            avg.z = __fadd_rn(avg.z, __fmul_rn(w, nb.z));
+        }
+    });
+}
+
+/* n = normalize(avg) (NaN for a zero sum, as glm computes it); when some
+   weight is positive the point moves by (w2sum / wsum) n. */
+__device__ __forceinline__ float4 pcib_push(float4 p, float wsum, float w2sum, float3 avg, float4& n)
+{
+    const float inv = __fdiv_rn(1.0f, __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(avg.x, avg.x), __fmul_rn(avg.y, avg.y)),
+                                                          __fmul_rn(avg.z, avg.z))));
+    n = make_float4(__fmul_rn(avg.x, inv), __fmul_rn(avg.y, inv), __fmul_rn(avg.z, inv), 0.0f);
+    if (wsum > 0.0f) {
+        const float s = __fmul_rn(__fdiv_rn(1.0f, wsum), w2sum);
+        p.x = __fadd_rn(p.x, __fmul_rn(s, n.x));
+        p.y = __fadd_rn(p.y, __fmul_rn(s, n.y));
+        p.z = __fadd_rn(p.z, __fmul_rn(s, n.z));
+    }
+    return p;
+}
+
+/* correctVelocities: where |n| > 0, v_out = tf (u - (u.n) n) - nf (u.n) n
+   for the reference velocity u */
+__device__ __forceinline__ void pcib_velocity(const SimParams& P, float4 n, float4 u, float4& v_out)
+{
+    if (!(glm_length(n.x, n.y, n.z) > 0.0f)) return;
+    const float d = __fadd_rn(__fadd_rn(__fmul_rn(u.x, n.x), __fmul_rn(u.y, n.y)), __fmul_rn(u.z, n.z));
+    const float nx = __fmul_rn(d, n.x), ny = __fmul_rn(d, n.y), nz = __fmul_rn(d, n.z);
+    v_out.x = __fsub_rn(__fmul_rn(P.pcib_tf, __fsub_rn(u.x, nx)), __fmul_rn(P.pcib_nf, nx));
+    v_out.y = __fsub_rn(__fmul_rn(P.pcib_tf, __fsub_rn(u.y, ny)), __fmul_rn(P.pcib_nf, ny));
+    v_out.z = __fsub_rn(__fmul_rn(P.pcib_tf, __fsub_rn(u.z, nz)), __fmul_rn(P.pcib_nf, nz));
+}
+
+/* Density of boundary particle q: fluid candidates of its 27 cells first,
+   then boundary candidates, each term m W(x_q - x_j) added in turn. POLY6:
+   PCISPHSolver::predictBoundaryDensities (PCISPHSolver.cpp:211-244) at the
+   predicted fluid positions; else SPHSolver::computeBoundaryDensities
+   (SPHSolver.cpp:91-124) with the cubic spline at the current ones. */
+template <bool POLY6>
+__device__ __forceinline__ float boundary_density(const SimParams& P, const DeviceArrays& A, unsigned q)
+{
+    const float4 xq = A.bpos[q];
+    const Grid g = grid_single(P);
+    float rho = 0.0f;
+    for_cells27(xq, P.h, g, [&](unsigned c) {
+        const unsigned e = A.cell_start[c + 1];
+        for (unsigned j = A.cell_start[c]; j < e; ++j) {
+            const float4 xj = POLY6 ? A.predr[j] : A.pos[j];
+            const float s2 = dist2_exact(xq, xj);
+            if (!(s2 <= P.h2_guard)) continue;
+            const float w = POLY6 ? poly6_W(__fsub_rn(xq.x, xj.x), __fsub_rn(xq.y, xj.y), __fsub_rn(xq.z, xj.z), P)
+                                  : cs_W_exact(s2, P);
+            rho = __fadd_rn(rho, __fmul_rn(P.mass, w));
+        }
+    });
+    for_cells27(xq, P.h, g, [&](unsigned c) {
+        const unsigned e = A.bcell_start[c + 1];
+        for (unsigned b = A.bcell_start[c]; b < e; ++b) {
+            const float4 xb = A.bpos[b];
+            const float s2 = dist2_exact(xq, xb);
+            if (!(s2 <= P.h2_guard)) continue;
+            const float w = POLY6 ? poly6_W(__fsub_rn(xq.x, xb.x), __fsub_rn(xq.y, xb.y), __fsub_rn(xq.z, xb.z), P)
+                                  : cs_W_exact(s2, P);
+            rho = __fadd_rn(rho, __fmul_rn(xb.w, w));
+        }
+    });
+    return rho;
+}
+
+/* ---------------------------------------------------------------------- */
 
 template <bool ALPHA, bool EOS>
 __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
@@ -203,12 +298,15 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
         if (pressure || bvisc || (np && P.adh_on)) {
             float bvx = 0.0f, bvy = 0.0f, bvz = 0.0f;
             for (unsigned kk = 0; kk < nB; ++kk) {
-                const float4 xb = A.bpos[list_at(A.nbr_b, kk, nf, i)];
+                const unsigned bq = list_at(A.nbr_b, kk, nf, i);
+                const float4 xb = A.bpos[bq];
                 const Pair p = make_pair(xi, xb);
                 const float psi = xb.w;
                 const float f = cs_gradf(p.rl, p.inv_rl, P);
                 if (pressure) {
-                    const float c = psi * (dpi + dpb) * f;
+                    /* Akinci: rho0 V_b (p_i / rho_i^2 + p_i / rho0^2); PCISPH boundary
+                       particles: m_b (p_i / rho_i^2 + p_b / rho_b^2) (WCSPHSolver.cpp:160-184) */
+                    const float c = psi * (dpi + (P.pcib ? A.bdp[bq] : dpb)) * f;
                     ax -= c * p.rx; ay -= c * p.ry; az -= c * p.rz;
                 }
                 if (bvisc) {
@@ -525,6 +623,10 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
             v.x = __fadd_rn(v.x, __fmul_rn(__fadd_rn(a.x, P.gx), dt));
             v.y = __fadd_rn(v.y, __fmul_rn(__fadd_rn(a.y, P.gy), dt));
             v.z = __fadd_rn(v.z, __fmul_rn(__fadd_rn(a.z, P.gz), dt));
+            /* PCISPH boundary method: PCISPHBoundaryObject::correctVelocities
+               with the normals left by the last collision pass (or by the
+               surface-tension pass of this step, which shares the array) */
+            if (P.pcib) pcib_velocity(P, A.normal[i], v, v);
             A.vel[i] = v;
             A.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
@@ -807,11 +909,13 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
     const int nthr = gridDim.x * blockDim.x;
     const float dt = st->dt;
 
-    /* PCISPHSolver::initPressure */
+    /* PCISPHSolver::initPressure (boundary pressures too with PCISPH boundary particles) */
     for (int i = tid; i < nfi; i += nthr) {
         A.press[i] = 0.0f;
         A.pacc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
+    if (P.pcib)
+        for (int q = tid; q < P.nb; q += nthr) A.bpress[q] = 0.0f;
     unsigned it = 0;
     /* the first test uses the residual left by the previous step (PCISPHSolver.cpp:374) */
     double avg = st->pcisph_avg;
@@ -823,8 +927,21 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
             const float vx = __fadd_rn(v.x, __fmul_rn(__fadd_rn(__fadd_rn(a.x, pa.x), P.gx), dt));
             const float vy = __fadd_rn(v.y, __fmul_rn(__fadd_rn(__fadd_rn(a.y, pa.y), P.gy), dt));
             const float vz = __fadd_rn(v.z, __fmul_rn(__fadd_rn(__fadd_rn(a.z, pa.z), P.gz), dt));
-            A.predr[i] = make_float4(__fadd_rn(x.x, __fmul_rn(vx, dt)), __fadd_rn(x.y, __fmul_rn(vy, dt)),
-                                     __fadd_rn(x.z, __fmul_rn(vz, dt)), 0.0f);
+            float4 pr = make_float4(__fadd_rn(x.x, __fmul_rn(vx, dt)), __fadd_rn(x.y, __fmul_rn(vy, dt)),
+                                    __fadd_rn(x.z, __fmul_rn(vz, dt)), 0.0f);
+            if (P.pcib) {
+                /* PCISPHBoundaryObject::correctPredPositions (:390-438): tested at the
+                   current position (whose cell holds lists), weighted at the
+                   predicted one, which moves */
+                A.predv[i] = make_float4(vx, vy, vz, 0.0f);
+                float wsum, w2sum;
+                float3 avg;
+                pcib_collide(P, A, x, pr, wsum, w2sum, avg);
+                float4 n;
+                pr = pcib_push(pr, wsum, w2sum, avg, n);
+                A.normal[i] = n;
+            }
+            A.predr[i] = pr;
         }
         if (!grid_barrier(st)) return;
         /* predictFluidDensities over the start-of-step candidates of the 27
@@ -858,6 +975,15 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
             A.press[i] = __fadd_rn(A.press[i], __fmul_rn(P.pcisph_delta, err));
             local += (double)(err / P.rho0);
         }
+        if (P.pcib)
+            /* predictBoundaryDensities (Poly6) and their pressure update with
+               the fluid's scaling factor (PCISPHSolver.cpp:211-244, 279-297) */
+            for (int q = tid; q < P.nb; q += nthr) {
+                const float rb = boundary_density<true>(P, A, (unsigned)q);
+                A.bdens[q] = rb;
+                const float err = fmaxf(0.0f, __fsub_rn(rb, P.rho0));
+                A.bpress[q] = __fadd_rn(A.bpress[q], __fmul_rn(P.pcisph_delta, err));
+            }
         const double bs = block_sum(local, s_red);
         if (threadIdx.x == 0) atomicAdd(&A.accum[it], bs);
         if (!grid_barrier(st)) return;
@@ -883,10 +1009,18 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
                 az = __fsub_rn(az, __fmul_rn(c, gz));
             }
             for (unsigned kk = 0; kk < nB; ++kk) {
-                const float4 xb = A.bpos[list_at(A.nbr_b, kk, nf, i)];
-                float gx, gy, gz;
-                cs_gradW_exact(__fsub_rn(xi.x, xb.x), __fsub_rn(xi.y, xb.y), __fsub_rn(xi.z, xb.z), P, gx, gy, gz);
-                const float c = __fmul_rn(xb.w, dpi);
+                const unsigned bq = list_at(A.nbr_b, kk, nf, i);
+                const float4 xb = A.bpos[bq];
+                float gx, gy, gz, c;
+                if (P.pcib) {
+                    /* m_b (p_i / rho_i^2 + p_b / rho_b^2) Spiky::gradW (PCISPHSolver.cpp:336-347) */
+                    spiky_gradW(__fsub_rn(xi.x, xb.x), __fsub_rn(xi.y, xb.y), __fsub_rn(xi.z, xb.z), P, gx, gy, gz);
+                    const float rb = A.bdens[bq];
+                    c = __fmul_rn(xb.w, __fadd_rn(dpi, __fdiv_rn(A.bpress[bq], __fmul_rn(rb, rb))));
+                } else {
+                    cs_gradW_exact(__fsub_rn(xi.x, xb.x), __fsub_rn(xi.y, xb.y), __fsub_rn(xi.z, xb.z), P, gx, gy, gz);
+                    c = __fmul_rn(xb.w, dpi);
+                }
                 ax = __fsub_rn(ax, __fmul_rn(c, gx));
                 ay = __fsub_rn(ay, __fmul_rn(c, gy));
                 az = __fsub_rn(az, __fmul_rn(c, gz));
@@ -909,6 +1043,19 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
         v.z = __fadd_rn(v.z, __fmul_rn(azz, dt));
         x.x = __fadd_rn(x.x, __fmul_rn(v.x, dt)); x.y = __fadd_rn(x.y, __fmul_rn(v.y, dt));
         x.z = __fadd_rn(x.z, __fmul_rn(v.z, dt));
+        if (P.pcib) {
+            /* correctPositions (PCISPH branch, :226-262): candidates of the new
+               cell if the last search listed it, weights at the predicted
+               position; then correctVelocities from the predicted velocity */
+            float wsum = 0.0f, w2sum = 0.0f;
+            float3 avg = make_float3(0.0f, 0.0f, 0.0f);
+            if (cell_listed(A.cell_entry, cell_index(x, P.h, grid_single(P)), st->ns_epoch))
+                pcib_collide(P, A, x, A.predr[i], wsum, w2sum, avg);
+            float4 n;
+            x = pcib_push(x, wsum, w2sum, avg, n);
+            A.normal[i] = n;
+            pcib_velocity(P, n, A.predv[i], v);
+        }
         A.vel[i] = v;
         A.pos[i] = x;
         A.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -926,6 +1073,60 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
             st->steps += 1u;
         }
     }
+}
+
+/* ---------------------------------------------------------------------- */
+/* PCISPH boundary method passes outside the persistent solvers             */
+
+/* SPHSolver::computeBoundaryDensities + WCSPHSolver::computeBoundaryPressures:
+   rho_b, p_b = max(0, k rho0 / gamma ((rho_b / rho0)^gamma - 1)), p_b / rho_b^2 */
+__global__ void __launch_bounds__(256) k_boundary_density(SimParams P, DeviceArrays A)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.nb) return;
+    const float rho = boundary_density<false>(P, A, (unsigned)q);
+    const float p = tait_pressure(rho, P, P.kr_g);
+    A.bdens[q] = rho;
+    A.bpress[q] = p;
+    A.bdp[q] = __fdiv_rn(p, __fmul_rn(rho, rho));
+}
+
+void launch_boundary_density(const SimParams& P, const DeviceArrays& A, cudaStream_t s)
+{
+    if (P.nb > 0) k_boundary_density<<<(P.nb + 255) / 256, 256, 0, s>>>(P, A);
+}
+
+/* PCISPHBoundaryObject::correctPositions (WCSPH / DFSPH branch, :264-300)
+   at the updated positions, and for WCSPH correctVelocities (:338-358) with
+   the new normals */
+template <bool WCSPH>
+__global__ void __launch_bounds__(256) k_pcib_correct(SimParams P, DeviceArrays A)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= active_n(P, A.st)) return;
+    float4 x = A.pos[i];
+    float wsum = 0.0f, w2sum = 0.0f;
+    float3 avg = make_float3(0.0f, 0.0f, 0.0f);
+    if (cell_listed(A.cell_entry, cell_index(x, P.h, grid_single(P)), A.st->ns_epoch))
+        pcib_collide(P, A, x, x, wsum, w2sum, avg);
+    float4 n;
+    x = pcib_push(x, wsum, w2sum, avg, n);
+    A.pos[i] = x;
+    A.normal[i] = n;
+    if (!isfinite(x.x) || !isfinite(x.y) || !isfinite(x.z)) atomicOr(&A.st->err, ERRBIT_NAN);
+    if (WCSPH) {
+        float4 v = A.vel[i];
+        pcib_velocity(P, n, v, v);
+        A.vel[i] = v;
+    }
+}
+
+void launch_pcib_correct(const SimParams& P, const DeviceArrays& A, bool wcsph, cudaStream_t s)
+{
+    const int grid = (P.nf + 255) / 256;
+    if (grid == 0) return;
+    if (wcsph) k_pcib_correct<true><<<grid, 256, 0, s>>>(P, A);
+    else k_pcib_correct<false><<<grid, 256, 0, s>>>(P, A);
 }
 
 /* ---------------------------------------------------------------------- */

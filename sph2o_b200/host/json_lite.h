@@ -44,6 +44,12 @@ public:
         if (kind_ == Bool) return b_ ? 1.0 : 0.0;
         throw JsonError(std::string("expected a number for ") + what);
     }
+    bool as_bool(const char* what = "value") const
+    {
+        if (kind_ == Bool) return b_;
+        if (kind_ == Number) return num_ != 0.0;
+        throw JsonError(std::string("expected true or false for ") + what);
+    }
     const std::string& as_string(const char* what = "value") const
     {
         if (kind_ != String) throw JsonError(std::string("expected a string for ") + what);

@@ -33,8 +33,13 @@
  * directory, as the reference does) and, failing that, relative to the
  * directory of the scene file.
  *
- * Not supported (rejected with SPH_ERR_ARG): more than one fluid model, the
- * PCISPH boundary method (1).
+ * With boundaryMethod 1 (PCISPH boundary particles) the boxes and spheres
+ * are sampled with PCISPHBoundaryObject's samplers, each point with its
+ * normal, and the object's "normalFct"/"tangFct" are read
+ * (PCISPHBoundaryObject.cpp:6-213, SceneLoader.cpp:168-195).
+ *
+ * Not supported (rejected with SPH_ERR_ARG): more than one fluid model;
+ * more than one boundary object with boundaryMethod 1.
  */
 #include "../../include/sph2o_cuda.h"
 #include "geometry.h"
@@ -59,6 +64,9 @@ struct sph_scene {
     std::vector<sph_emitter_desc> emitters;
     struct Cube { float mn[3], mx[3]; };
     std::vector<Cube> cubes;      /* boundary method 0: first box of each boundary object */
+    /* boundary method 1: per-particle normals and the object's velocity factors */
+    std::vector<float> boundary_normal; /* nb*3 */
+    float normal_fct = 0.0f, tangential_fct = 0.0f;
     std::string path;
 };
 
@@ -118,13 +126,18 @@ void sample_cube(V3 lo, V3 hi, float radius, std::vector<float>& out)
 
 /* AkinciBoundaryObject::sampleSphere (AkinciBoundaryObject.cpp:125-153):
    equal-area points with 1.5x overlap; the trigonometry runs in double
-   exactly where the reference's unqualified calls do. */
-void sample_sphere(V3 c, float radius, float particle_radius, std::vector<float>& out)
+   exactly where the reference's unqualified calls do. float_count: the
+   point count formed in float, as PCISPHBoundaryObject::sampleSphere
+   (PCISPHBoundaryObject.cpp:185-213) forms it; the rest is the same. */
+void sample_sphere(V3 c, float radius, float particle_radius, std::vector<float>& out, bool float_count = false)
 {
     const float separation = 1.5f;
-    const unsigned num_parts = (unsigned)::floor(4.0 * M_PI * (double)radius * (double)radius /
-                                                 (M_PI * (double)particle_radius * (double)particle_radius) *
-                                                 (double)separation);
+    const unsigned num_parts =
+        float_count ? (unsigned)::floor((double)((float)(4.0 * M_PI) * radius * radius /
+                                                 ((float)M_PI * particle_radius * particle_radius) * separation))
+                    : (unsigned)::floor(4.0 * M_PI * (double)radius * (double)radius /
+                                        (M_PI * (double)particle_radius * (double)particle_radius) *
+                                        (double)separation);
     if (num_parts == 0) return;
     const float a = (float)(4.0 * M_PI) / (float)num_parts;
     const float d = (float)::sqrt((double)a);
@@ -144,6 +157,95 @@ void sample_sphere(V3 c, float radius, float particle_radius, std::vector<float>
             out.push_back(radius * z + c.z);
         }
     }
+}
+
+/* glm::normalize in float: v * (1 / sqrt((x x + y y) + z z)) */
+V3 normalized(V3 v)
+{
+    const float inv = 1.0f / std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+    return {v.x * inv, v.y * inv, v.z * inv};
+}
+V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+V3 scale(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+V3 div3(V3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+
+/* A box side as PCISPHBoundaryObject::sampleCube measures it: its
+   unqualified abs takes an int there (PCISPHBoundaryObject.cpp:61-63), so
+   the float difference is truncated to a whole number first. A side that
+   truncates to 0 would give the reference 0/0 spacings (NaN particles):
+   refused here. */
+float pcisph_side(float lo, float hi, const char* axis)
+{
+    const float d = lo - hi;
+    if (!(std::fabs(d) < 2147483648.0f)) throw std::invalid_argument("PCISPH boundary box too large");
+    const int t = std::abs((int)d);
+    if (t == 0)
+        throw std::invalid_argument(std::string("PCISPH boundary box side along ") + axis +
+                                    " is shorter than 1: SPH2O truncates these sides to whole numbers");
+    return (float)t;
+}
+
+/* PCISPHBoundaryObject::sampleCube (PCISPHBoundaryObject.cpp:52-183): a
+   hollow box at ceil(l / 0.45h) intervals per axis, each point with the
+   normal of its face, edge (normalised mean of two face normals) or corner
+   (of three), times inv (1 for an inverted box, the container, else -1). */
+void sample_cube_pcisph(V3 lo, V3 hi, float h, float inv, std::vector<float>& pts, std::vector<float>& nrm)
+{
+    const float lx = pcisph_side(lo.x, hi.x, "x"), ly = pcisph_side(lo.y, hi.y, "y"), lz = pcisph_side(lo.z, hi.z, "z");
+    const float sp = 0.45f * h;
+    const unsigned nx = (unsigned)::ceil((double)(lx / sp)), ny = (unsigned)::ceil((double)(ly / sp)),
+                   nz = (unsigned)::ceil((double)(lz / sp));
+    const float dx = lx / (float)nx, dy = ly / (float)ny, dz = lz / (float)nz;
+    const V3 L{1, 0, 0}, R{-1, 0, 0}, T{0, -1, 0}, B{0, 1, 0}, F{0, 0, -1}, K{0, 0, 1}; /* K: behind */
+    auto edge = [](V3 a, V3 b) { return normalized(scale(add(a, b), 0.5f)); };
+    auto corner = [](V3 a, V3 b, V3 c) { return normalized(div3(add(add(a, b), c), 3.0f)); };
+    const V3 LB = edge(L, B), KB = edge(K, B), FB = edge(F, B), RB = edge(R, B);
+    const V3 LT = edge(L, T), KT = edge(K, T), FT = edge(F, T), RT = edge(R, T);
+    const V3 LK = edge(L, K), RK = edge(R, K), RF = edge(R, F), LF = edge(L, F);
+    const V3 LKB = corner(L, K, B), RKB = corner(R, K, B), LFB = corner(L, F, B), RFB = corner(R, F, B);
+    const V3 LKT = corner(L, K, T), RKT = corner(R, K, T), LFT = corner(L, F, T), RFT = corner(R, F, T);
+    for (unsigned i = 0; i <= nx; i++)
+        for (unsigned j = 0; j <= ny; j++)
+            for (unsigned k = 0; k <= nz; k++) {
+                const bool i0 = i == 0, iN = i == nx, im = i > 0 && i < nx;
+                const bool j0 = j == 0, jN = j == ny, jm = j > 0 && j < ny;
+                const bool k0 = k == 0, kN = k == nz, km = k > 0 && k < nz;
+                if (!(i0 || iN || j0 || jN || k0 || kN)) continue;
+                pts.push_back((float)i * dx + lo.x);
+                pts.push_back((float)j * dy + lo.y);
+                pts.push_back((float)k * dz + lo.z);
+                /* the reference's if-chain, first match wins */
+                V3 n;
+                if (i0 && j0 && k0) n = LKB;
+                else if (iN && j0 && k0) n = RKB;
+                else if (i0 && j0 && kN) n = LFB;
+                else if (iN && j0 && kN) n = RFB;
+                else if (i0 && jN && k0) n = LKT;
+                else if (iN && jN && k0) n = RKT;
+                else if (i0 && jN && kN) n = LFT;
+                else if (iN && jN && kN) n = RFT;
+                else if (i0 && j0 && km) n = LB;
+                else if (im && j0 && k0) n = KB;
+                else if (im && j0 && kN) n = FB;
+                else if (iN && j0 && km) n = RB;
+                else if (i0 && jN && km) n = LT;
+                else if (im && jN && k0) n = KT;
+                else if (im && jN && kN) n = FT;
+                else if (iN && jN && km) n = RT;
+                else if (i0 && jm && k0) n = LK;
+                else if (iN && jm && k0) n = RK;
+                else if (iN && jm && kN) n = RF;
+                else if (i0 && jm && kN) n = LF;
+                else if (i0 && jm && km) n = L;
+                else if (iN && jm && km) n = R;
+                else if (im && jN && km) n = T;
+                else if (im && j0 && km) n = B;
+                else if (im && jm && kN) n = F;
+                else n = K; /* im && jm && k0 */
+                nrm.push_back(inv * n.x);
+                nrm.push_back(inv * n.y);
+                nrm.push_back(inv * n.z);
+            }
 }
 
 unsigned uint_field(const sphjson::Value& cfg, const char* key)
@@ -209,8 +311,8 @@ sph_scene* build_scene(const std::string& text, const std::string& path)
     } else {
         throw sphjson::JsonError("simulationMethod must be 0 (WCSPH), 1 (PCISPH) or 2 (DFSPH)");
     }
-    if (d.boundary_method != SPH_BOUNDARY_AKINCI && d.boundary_method != SPH_BOUNDARY_CUBE)
-        throw std::invalid_argument("boundaryMethod 2 (Akinci) and 0 (cube) are implemented");
+    if (d.boundary_method < SPH_BOUNDARY_CUBE || d.boundary_method > SPH_BOUNDARY_AKINCI)
+        throw std::invalid_argument("boundaryMethod must be 0 (cube), 1 (PCISPH) or 2 (Akinci)");
 
     /* SceneLoader::readFluidInfo (SceneLoader.cpp:80-146) */
     const sphjson::Value& fl = root.get("Fluid");
@@ -278,6 +380,45 @@ sph_scene* build_scene(const std::string& text, const std::string& path)
                 const V3 mn = vec3(boxes->at(0).get("min"), "box.min"), mx = vec3(boxes->at(0).get("max"), "box.max");
                 scene->cubes.push_back({{mn.x, mn.y, mn.z}, {mx.x, mx.y, mx.z}});
             }
+        return scene.release();
+    }
+    /* SceneLoader::readBoundaryInfo with the PCISPH method's keys
+       (SceneLoader.cpp:168-195) + importScene (:428-453): boxes, then
+       spheres, per object; "geometry" entries are not read for this method */
+    if (d.boundary_method == SPH_BOUNDARY_PCISPH) {
+        if (const sphjson::Value* bnd = root.find("Boundary")) {
+            if (bnd->size() > 1)
+                throw std::invalid_argument("the PCISPH boundary method takes one boundary object (SPH2O indexes an "
+                                            "object's arrays with the candidates of all objects)");
+            const float h = 4.0f * d.particle_radius;
+            for (size_t i = 0; i < bnd->size(); ++i) {
+                const sphjson::Value& b = bnd->at(i);
+                scene->normal_fct = num(b.get("normalFct"), "normalFct");
+                scene->tangential_fct = num(b.get("tangFct"), "tangFct");
+                if (const sphjson::Value* boxes = b.find("box"))
+                    for (size_t j = 0; j < boxes->size(); ++j) {
+                        const sphjson::Value& bx = boxes->at(j);
+                        const float inv = bx.get("inverted").as_bool("box.inverted") ? 1.0f : -1.0f;
+                        sample_cube_pcisph(vec3(bx.get("min"), "box.min"), vec3(bx.get("max"), "box.max"), h, inv,
+                                           scene->boundary, scene->boundary_normal);
+                    }
+                if (const sphjson::Value* sph = b.find("sphere"))
+                    for (size_t j = 0; j < sph->size(); ++j) {
+                        const sphjson::Value& sv = sph->at(j);
+                        const float inv = sv.get("inverted").as_bool("sphere.inverted") ? 1.0f : -1.0f;
+                        const V3 c = vec3(sv.get("pos"), "sphere.pos");
+                        const size_t first = scene->boundary.size();
+                        sample_sphere(c, num(sv.get("radius"), "sphere.radius"), d.particle_radius, scene->boundary,
+                                      true);
+                        /* n = inv (centre - point) (PCISPHBoundaryObject.cpp:40) */
+                        for (size_t q = first; q < scene->boundary.size(); q += 3) {
+                            scene->boundary_normal.push_back(inv * (c.x - scene->boundary[q]));
+                            scene->boundary_normal.push_back(inv * (c.y - scene->boundary[q + 1]));
+                            scene->boundary_normal.push_back(inv * (c.z - scene->boundary[q + 2]));
+                        }
+                    }
+            }
+        }
         return scene.release();
     }
     /* SceneLoader::readBoundaryInfo (SceneLoader.cpp:148-209) + importScene (:407-426) */
@@ -424,6 +565,15 @@ int sph_scene_get_emitter(const sph_scene* s, unsigned k, sph_emitter_desc* out)
 }
 unsigned sph_scene_num_boundary(const sph_scene* s) { return s ? (unsigned)(s->boundary.size() / 3) : 0u; }
 
+int sph_scene_get_boundary_normals(const sph_scene* s, float* xyz, float* normal_fct, float* tangential_fct)
+{
+    if (!s || s->desc.boundary_method != SPH_BOUNDARY_PCISPH) return SPH_ERR_ARG;
+    if (xyz) std::memcpy(xyz, s->boundary_normal.data(), s->boundary_normal.size() * sizeof(float));
+    if (normal_fct) *normal_fct = s->normal_fct;
+    if (tangential_fct) *tangential_fct = s->tangential_fct;
+    return SPH_OK;
+}
+
 int sph_scene_get_fluid(const sph_scene* s, float* xyz, float* v)
 {
     if (!s) return SPH_ERR_ARG;
@@ -502,6 +652,10 @@ int sph_create_from_scene(const sph_scene* s, sph_ctx** out)
     if ((rc = sph_set_fluid(ctx, sph_scene_num_fluid(s), s->fluid.data(), s->fluid_v.data())) != SPH_OK ||
         (rc = sph_set_boundary(ctx, sph_scene_num_boundary(s), s->boundary.data())) != SPH_OK)
         return rc; /* the context stays valid; sph_last_error(ctx) explains */
+    if (s->desc.boundary_method == SPH_BOUNDARY_PCISPH &&
+        (rc = sph_set_boundary_normals(ctx, sph_scene_num_boundary(s), s->boundary_normal.data(), s->normal_fct,
+                                       s->tangential_fct)) != SPH_OK)
+        return rc;
     for (const sph_scene::Cube& b : s->cubes)
         if ((rc = sph_add_cube_boundary(ctx, b.mn, b.mx, 0.0f, 0.0f)) != SPH_OK) return rc;
     for (const sph_emitter_desc& e : s->emitters)

@@ -326,6 +326,41 @@ def geometry_scenes():
     return {"geometry_dfsph_cup": df, "geometry_wcsph_quirks": wc}
 
 
+def with_pcisph_boundary(scene_dict, normal_fct=0.5, tangential_fct=0.9):
+    """The scene with the PCISPH boundary method (boundaryMethod 1): every
+    boundary object gets "normalFct"/"tangFct" and every box and sphere an
+    "inverted" flag (SceneLoader.cpp:168-195): boxes are containers (True),
+    spheres obstacles (False)."""
+    scene_dict["Configuration"]["boundaryMethod"] = BOUNDARY_PCISPH
+    for b in scene_dict["Boundary"]:
+        b["normalFct"] = f32(normal_fct)
+        b["tangFct"] = f32(tangential_fct)
+        for box in b.get("box", []):
+            box["inverted"] = True
+        for sph in b.get("sphere", []):
+            sph["inverted"] = False
+    return scene_dict
+
+
+def pcisph_boundary_scenes():
+    """Small scenes with PCISPH boundary particles (mass particles sampled at
+    0.45 h with per-particle normals, densities and pressures, and collision
+    correction of positions and velocities), one per solver, in a 1 m tank
+    (SPH2O's sampler for this method truncates box lengths to whole numbers),
+    with a sphere obstacle in the WCSPH and DFSPH scenes."""
+    r = 0.025
+    tank = ((0, 0, 0), (1, 1, 1))
+    blk = lambda n: block(n, r, (4 * r,) * 3)
+    sphere = [((0.8, 0.3, 0.15), 0.12)]  # clear of the blocks by more than h
+    wc = with_pcisph_boundary(scene(method=WCSPH, radius=r, blocks=[blk((10, 8, 8))], tank=tank, spheres=sphere,
+                                    time_step=2e-4, seed=61), 0.5, 0.9)
+    pc = with_pcisph_boundary(scene(method=PCISPH, radius=r, blocks=[blk((8, 8, 10))], tank=tank, eta=0.01,
+                                    time_step=5e-4, seed=62), 0.3, 1.0)
+    df = with_pcisph_boundary(scene(method=DFSPH, radius=r, blocks=[blk((8, 8, 8))], tank=tank, spheres=sphere,
+                                    seed=63), 0.5, 0.8)
+    return {"pcib_wcsph_sphere": wc, "pcib_pcisph": pc, "pcib_dfsph_sphere": df}
+
+
 def resolve_geometry_paths(scene_dict, directory):
     """Copy of the scene with every relative geometry path joined to `directory`."""
     import copy

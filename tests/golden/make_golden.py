@@ -51,7 +51,8 @@ from sph2o_b200 import scenes as S  # noqa: E402
 
 NSTEPS = 20
 # emitter scenes run long enough for several emissions
-STEPS = {"emitter_wcsph_square": 120, "emitter_dfsph_circle": 120, "cube_dfsph_floor": 120}
+STEPS = {"emitter_wcsph_square": 120, "emitter_dfsph_circle": 120, "cube_dfsph_floor": 120,
+         "pcib_wcsph_sphere": 120, "pcib_pcisph": 60, "pcib_dfsph_sphere": 60}
 REF32 = os.path.join(ROOT, "oracle", "_ref", "sph2o_ref_f32")
 REF64 = os.path.join(ROOT, "oracle", "_ref", "sph2o_ref_f64")
 
@@ -61,6 +62,7 @@ def golden_scenes():
         **S.emitter_scenes(),
         **S.cube_scenes(),
         **S.geometry_scenes(),
+        **S.pcisph_boundary_scenes(),
         "dfsph_st_sphere": S.small(method=S.DFSPH, surface_tension=0.05, sphere=True),
         "wcsph_artificial": S.small(method=S.WCSPH, n=(12, 10, 10)),
         "pcisph_artificial": S.small(method=S.PCISPH, n=(10, 10, 12), eta=0.01, time_step=5e-4),
@@ -95,6 +97,9 @@ def make(name, scene, td):
         g[k] = nb[k]
     ph = run(REF32, path, "phases", os.path.join(td, "ph.sphd"))
     g["bvol"] = ph.get("bvol", np.zeros(0, np.float32))  # absent without Akinci boundary particles
+    for k in ("bnormal", "bdensity", "bpressure"):  # PCISPH boundary particles
+        if k in ph:
+            g[k] = ph[k]
     g["density"] = ph["density"]
     g["a_np"] = ph["a_nonpressure"]
     for k in ("alpha", "pressure", "a_pressure"):

@@ -92,8 +92,16 @@ def test_call_order_errors():
     L.sph_destroy(h)
     bad = SceneDesc()
     C.memmove(C.byref(bad), C.byref(d), C.sizeof(d))
-    bad.boundary_method = 1  # PCISPH boundary particles: not implemented
+    bad.boundary_method = 3  # no such method
     assert L.sph_create(C.byref(bad), C.byref(h)) == -1
+    bad.boundary_method = 1  # PCISPH boundary particles need their normals before init
+    assert L.sph_create(C.byref(bad), C.byref(h)) == SPH_OK
+    x = np.zeros((8, 3), np.float32)
+    x[:, 0] = np.arange(8) * 0.05
+    assert L.sph_set_fluid(h, 8, x.ctypes.data_as(C.POINTER(C.c_float)), None) == SPH_OK
+    assert L.sph_set_boundary(h, 8, (x + np.float32(1.0)).ctypes.data_as(C.POINTER(C.c_float))) == SPH_OK
+    assert L.sph_init(h) == -1
+    L.sph_destroy(h)
 
 
 def test_outside_grid_particles_still_found():

@@ -10,11 +10,11 @@ reference the same way."""
 import numpy as np
 import pytest
 
-from conftest import golden_names, load_golden, rel_err
+from conftest import load_golden, oracle_golden_names, rel_err
 from oracle.oracle import Oracle
 from sph2o_b200.api import Scene
 
-NAMES = golden_names()
+NAMES = oracle_golden_names()
 
 
 def make(g, fp64=False):

@@ -24,6 +24,42 @@ def test_particles_bit_exact(name):
     assert not v.any()
 
 
+@pytest.mark.parametrize("name", [n for n in golden_names() if n.startswith("pcib_")])
+def test_pcisph_boundary_normals_bit_exact(name):
+    """PCISPHBoundaryObject::sampleCube / sampleSphere: positions and normals
+    bit for bit, and the object's velocity factors."""
+    g = load_golden(name)
+    sc = Scene.from_dict(g["scene"])
+    nrm, nf, tf = sc.boundary_normals()
+    assert np.array_equal(nrm.view(np.uint32), g["bnormal"].view(np.uint32))
+    b = g["scene"]["Boundary"][0]
+    assert nf == np.float32(b["normalFct"]) and tf == np.float32(b["tangFct"])
+
+
+@pytest.mark.parametrize("mutate,code", [
+    # SPH2O truncates PCISPH box sides to whole numbers: a 0.6 side would be 0
+    (lambda d: d["Boundary"][0]["box"][0].__setitem__("max", [1.0, 0.6, 1.0]), -1),
+    (lambda d: d["Boundary"].append(copy.deepcopy(d["Boundary"][0])), -1),
+    (lambda d: d["Boundary"][0]["box"][0].pop("inverted"), -8),
+    (lambda d: d["Boundary"][0].pop("tangFct"), -8),
+])
+def test_bad_pcisph_boundary_scenes_rejected(mutate, code):
+    d = S.pcisph_boundary_scenes()["pcib_pcisph"]
+    mutate(d)
+    with pytest.raises(SphError) as e:
+        Scene.from_dict(d)
+    assert e.value.code == code
+
+
+def test_pcisph_boundary_ignores_geometry_entries():
+    """importScene's PCISPH branch adds boxes and spheres only
+    (SPHSimulation.cpp:428-453): geometry entries are not even opened."""
+    d = S.pcisph_boundary_scenes()["pcib_pcisph"]
+    n = Scene.from_dict(d).boundary().shape[0]
+    d["Boundary"][0]["geometry"] = [{"path": "missing.obj", "spacing": 1.0}]
+    assert Scene.from_dict(d).boundary().shape[0] == n
+
+
 def test_desc_fields():
     sc = Scene.from_dict(S.dam_break_dfsph_125k())
     d = sc.desc()
@@ -45,7 +81,7 @@ def test_missing_sphere_geometry_keys_tolerated():
 @pytest.mark.parametrize("mutate,code", [
     (lambda d: d["Configuration"].pop("timeStep"), -8),
     (lambda d: d["Fluid"]["FluidModel"].append(copy.deepcopy(d["Fluid"]["FluidModel"][0])), -1),
-    (lambda d: d["Configuration"].__setitem__("boundaryMethod", 1), -1),
+    (lambda d: d["Configuration"].__setitem__("boundaryMethod", 3), -1),
     (lambda d: d["Fluid"]["FluidModel"][0].__setitem__("emitters", [{"type": 0}]), -8),
     (lambda d: d["Boundary"][0].__setitem__("geometry", [{"path": "missing.obj", "spacing": 1.0}]), -8),
     (lambda d: d["Boundary"][0].__setitem__("geometry", [{"spacing": 1.0}]), -8),
