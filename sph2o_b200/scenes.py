@@ -358,7 +358,22 @@ def pcisph_boundary_scenes():
                                     time_step=5e-4, seed=62), 0.3, 1.0)
     df = with_pcisph_boundary(scene(method=DFSPH, radius=r, blocks=[blk((8, 8, 8))], tank=tank, spheres=sphere,
                                     seed=63), 0.5, 0.8)
-    return {"pcib_wcsph_sphere": wc, "pcib_pcisph": pc, "pcib_dfsph_sphere": df}
+    # a block against the far x wall (whose particles sit in the next cell
+    # row, x = 1.0): the fluid spreads along the wall into cells no particle
+    # has visited, which hold no candidate lists until the next search
+    fw = with_pcisph_boundary(scene(method=WCSPH, radius=r, blocks=[block((5, 4, 8), r, (0.72, 0.4, 0.03))], tank=tank,
+                                    time_step=2e-4, seed=64), 0.4, 0.95)
+    # two lone particles pressed against the far x wall and driven along it
+    # (gravity 20 along x, 40 along y), at the heights of wall particle rows
+    # (z = 16 and 9 spacings of 1/23): when they cross y = 0.6 they enter
+    # cells no particle has visited, which hold no candidate lists until the
+    # next search, so that step goes uncorrected though they touch the wall
+    ws = with_pcisph_boundary(scene(method=WCSPH, radius=r,
+                                    blocks=[block((1, 1, 1), r, (0.94, 0.52, 16 / 23 - r)),
+                                            block((1, 1, 1), r, (0.94, 0.52, 9 / 23 - r))], tank=tank,
+                                    gravity=(20.0, 40.0, 0.0), time_step=2e-4, seed=65), 0.4, 1.0)
+    return {"pcib_wcsph_sphere": wc, "pcib_pcisph": pc, "pcib_dfsph_sphere": df, "pcib_wcsph_farwall": fw,
+            "pcib_wcsph_wallslide": ws}
 
 
 def resolve_geometry_paths(scene_dict, directory):

@@ -52,7 +52,8 @@ from sph2o_b200 import scenes as S  # noqa: E402
 NSTEPS = 20
 # emitter scenes run long enough for several emissions
 STEPS = {"emitter_wcsph_square": 120, "emitter_dfsph_circle": 120, "cube_dfsph_floor": 120,
-         "pcib_wcsph_sphere": 120, "pcib_pcisph": 60, "pcib_dfsph_sphere": 60}
+         "pcib_wcsph_sphere": 120, "pcib_pcisph": 60, "pcib_dfsph_sphere": 60, "pcib_wcsph_farwall": 400,
+         "pcib_wcsph_wallslide": 400}
 REF32 = os.path.join(ROOT, "oracle", "_ref", "sph2o_ref_f32")
 REF64 = os.path.join(ROOT, "oracle", "_ref", "sph2o_ref_f64")
 

@@ -78,3 +78,19 @@ def test_adhesion_rejected():
     with pytest.raises(SphError) as e:
         Simulation.from_scene(Scene.from_dict(d))
     assert e.value.code == -1
+
+
+def test_unlisted_cells_skip_the_collision_pass():
+    """Two lone particles slide along the far x wall into cells no particle
+    has visited (pcib_wcsph_wallslide). SPH2O's hash table holds no candidate
+    lists for such a cell until the next search, so the collision pass skips
+    them for that step. The GPU run ends where the FP32 reference ends
+    (measured: identical); a run that treats every cell as listed ends
+    7.2e-7 m away."""
+    g = load_golden("pcib_wcsph_wallslide")
+    sim = Simulation.from_scene(Scene.from_dict(g["scene"]))
+    for _ in range(g["trace_f32"].shape[0]):
+        sim.step(1)
+    x, _, _ = sim.state()
+    sim.close()
+    assert np.max(np.abs(x.astype(np.float64) - g["final_pos_f32"])) <= 1e-7
