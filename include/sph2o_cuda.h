@@ -221,11 +221,8 @@ enum sph_option {
     SPH_OPT_CELL_ORDER = 1,       /* 0 (default): 4x4x4 cell bricks, Morton inside; 1: linear, x fastest */
     SPH_OPT_SOLVER_OCCUPANCY = 2, /* DFSPH persistent solver blocks per SM: 8 (default) or 4 */
     SPH_OPT_PASS_BLOCK = 3,       /* threads per block of the particle-pass kernels: 256 (default) or 128 */
-    SPH_OPT_SOLVER_LANES = 4,     /* lanes sharing one particle's neighbour list in the persistent DFSPH
+    SPH_OPT_SOLVER_LANES = 4      /* lanes sharing one particle's neighbour list in the persistent DFSPH
                                      solver: 1, 2 (default) or 4 */
-    SPH_OPT_PCISPH_MARGIN = 5     /* PCISPH: margin of the extended candidate lists in percent of h
-                                     (0 = scan the 27 cells in every iteration; default 25); before
-                                     sph_init */
 };
 /* Number of values sph_autotune chooses (options 1..4 in order). */
 #define SPH_TUNE_COUNT 4

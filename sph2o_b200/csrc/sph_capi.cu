@@ -117,9 +117,6 @@ struct sph_ctx {
     float4 *bnormal = nullptr, *normal2 = nullptr, *predv = nullptr;
     float *bdens = nullptr, *bpress = nullptr, *bdp = nullptr;
     unsigned* cell_entry = nullptr;
-    /* PCISPH extended candidate lists (margin in percent of h) */
-    int pcisph_margin = 25;
-    ExtLists ext{};
     /* autotune snapshot */
     float4 *snap_pos = nullptr, *snap_vel = nullptr;
     unsigned* snap_orig = nullptr;
@@ -350,7 +347,6 @@ DeviceArrays arrays(sph_ctx* c)
     A.accum = c->accum; A.st = c->st;
     A.bnormal = c->bnormal; A.bdens = c->bdens; A.bpress = c->bpress; A.bdp = c->bdp;
     A.predv = c->predv; A.cell_entry = c->cell_entry;
-    A.ext = c->ext;
     if (c->nscenes) {
         A.sref.scenes = c->d_scenes;
         A.sref.scene_of = c->d_scene_of;
@@ -454,12 +450,10 @@ int neighbor_search(sph_ctx* c)
         std::swap(c->kvws, c->kvws2);
         if (c->P.pcib) std::swap(c->normal, c->normal2);
     }
-    if (c->P.ext_on)
-        CUDA_TRY(c, cudaMemsetAsync(&c->st->ext_overflow, 0, sizeof(unsigned), c->stream));
     {
         Phase ph(c, SPH_PROF_LISTS, 1);
         launch_build_lists(c->P, SceneRef{c->d_scenes, c->d_scene_of}, c->pos, c->cell_start, c->bpos, c->bcell_start, c->nbr_f, c->cnt_f, c->nbr_b,
-                           c->cnt_b, c->st, c->stream, c->P.ext_on ? c->ext : ExtLists{});
+                           c->cnt_b, c->st, c->stream);
     }
     if (c->P.pcib) {
         /* the fluid's cells get candidate lists at this search */
@@ -1045,20 +1039,6 @@ int sph_init(sph_ctx* c)
     c->orig_base = c->orig;
     c->kws_base = c->kws;
     if ((rc = alloc_lists(c)) != SPH_OK) return rc;
-    if (c->desc.simulation_method == SPH_PCISPH && !c->nscenes && c->pcisph_margin > 0) {
-        /* capacity scaled with the volume of the wider sphere */
-        const double grow = std::pow(1.0 + c->pcisph_margin / 100.0, 3.0);
-        const double m = P.h * (c->pcisph_margin / 100.0);
-        P.capFE = (unsigned)std::ceil(P.capF * grow / 32.0) * 32u;
-        P.capBE = (unsigned)std::ceil(P.capB * grow / 32.0) * 32u;
-        P.ext_r2 = (float)(((double)P.h + m) * ((double)P.h + m) * (1.0 + 1.0e-5));
-        P.ext_disp = (float)(0.45 * m);
-        P.ext_on = 1;
-        if ((rc = dalloc(c, &c->ext.nbr_f, (size_t)P.capFE * nf)) != SPH_OK) return rc;
-        if ((rc = dalloc(c, &c->ext.cnt_f, nf)) != SPH_OK) return rc;
-        if ((rc = dalloc(c, &c->ext.nbr_b, (size_t)P.capBE * nf)) != SPH_OK) return rc;
-        if ((rc = dalloc(c, &c->ext.cnt_b, nf)) != SPH_OK) return rc;
-    }
     c->accum_len = 2 * ((size_t)P.max_it + 2) * std::max(1u, c->nscenes);
     if ((rc = dalloc(c, &c->accum, c->accum_len)) != SPH_OK) return rc;
     if (c->nscenes) {
@@ -1669,11 +1649,6 @@ int sph_set_option(sph_ctx* c, int option, int value)
         c->solver_tpp = value;
         drop_graphs(c);
         return SPH_OK;
-    case SPH_OPT_PCISPH_MARGIN:
-        if (value < 0 || value > 100) return fail(c, SPH_ERR_ARG, "the PCISPH list margin is 0..100 percent of h");
-        if (c->initialized) return fail(c, SPH_ERR_STATE, "the PCISPH list margin is set before sph_init");
-        c->pcisph_margin = value;
-        return SPH_OK;
     default:
         return fail(c, SPH_ERR_ARG, "unknown option");
     }
@@ -1688,7 +1663,6 @@ int sph_get_option(const sph_ctx* c, int option, int* value)
     case SPH_OPT_SOLVER_OCCUPANCY: *value = c->solver_occ; return SPH_OK;
     case SPH_OPT_PASS_BLOCK: *value = c->pass_block; return SPH_OK;
     case SPH_OPT_SOLVER_LANES: *value = c->solver_tpp; return SPH_OK;
-    case SPH_OPT_PCISPH_MARGIN: *value = c->pcisph_margin; return SPH_OK;
     default: return SPH_ERR_ARG;
     }
 }

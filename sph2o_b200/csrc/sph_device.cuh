@@ -67,14 +67,6 @@ struct SimParams {
     float rest_r;              /* collision distance 0.5 h (PCISPHBoundaryObject.cpp:222)        */
     float poly6_c;             /* Poly6 315 / (64 pi h^9)                 (Poly6.h:25)            */
     float spiky_g;             /* Spiky gradient 45 / (pi h^6)            (Spiky.h:25)            */
-    /* PCISPH: lists of the 27-cell candidates within h + margin, used for
-       the predicted densities while every predicted displacement stays
-       within ext_disp (0.45 margin), so that no candidate left out can come
-       within h */
-    int ext_on;
-    float ext_r2;              /* (h + margin)^2 (1 + 1e-5)                                    */
-    float ext_disp;            /* 0.45 margin                                                  */
-    unsigned capFE, capBE;     /* extended list capacities                                     */
 };
 
 /* Device-resident solver state; read by the host after a step. */
@@ -94,7 +86,6 @@ struct DevState {
     float last_vmax;
     unsigned n_active;          /* active fluid particles (emitters append to them) */
     unsigned ns_epoch;          /* neighbour searches so far (PCISPH boundary cell entries) */
-    unsigned ext_overflow;      /* PCISPH extended lists over capacity at the last search */
 };
 
 /* Fluid particles a pass covers: all nf, or with emitters the active prefix

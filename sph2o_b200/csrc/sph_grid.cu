@@ -154,17 +154,14 @@ __global__ void __launch_bounds__(256) k_ns_rank_gather(int n, const unsigned* _
     if (g.f_in[1]) g.f_out[1][dst] = g.f_in[1][src];
 }
 
-/* Neighbour lists in the reference's candidate order, filtered at |r| <= h.
-   EXT: also the PCISPH extended lists (the same candidates within h +
-   margin, same order); over capacity they are flagged unusable. */
-template <bool EXT>
+/* Neighbour lists in the reference's candidate order, filtered at |r| <= h. */
 __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S, const float4* __restrict__ pos,
                                                         const unsigned* __restrict__ cell_start,
                                                         const float4* __restrict__ bpos,
                                                         const unsigned* __restrict__ bcell_start,
                                                         unsigned* __restrict__ nbr_f, unsigned* __restrict__ cnt_f,
                                                         unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b,
-                                                        ExtLists X, DevState* st)
+                                                        DevState* st)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= active_n(P, st)) return;
@@ -173,7 +170,7 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
     /* a cheap float test settles clear cases; candidates within a relative
        1e-5 band of h take the exact IEEE test that defines the set */
     const float lo2 = P.h2 * (1.0f - 1.0e-5f), hi2 = P.h2 * (1.0f + 1.0e-5f);
-    unsigned nF = 0, nB = 0, nFE = 0, nBE = 0;
+    unsigned nF = 0, nB = 0;
     for_cells27(xi, P.h, grid_for(P, S, (unsigned)i), [&](unsigned c) {
         const unsigned s = cell_start[c], e = cell_start[c + 1];
         for (unsigned q = s; q < e; ++q) {
@@ -183,10 +180,6 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
             if (d2 < lo2 || (d2 <= hi2 && within_h_exact(xi, xq, P.h))) {
                 if (nF < P.capF) __stcs(nbr_f + (size_t)nF * nf + i, q);
                 ++nF;
-            }
-            if (EXT && d2 <= P.ext_r2) {
-                if (nFE < P.capFE) __stcs(X.nbr_f + (size_t)nFE * nf + i, q);
-                ++nFE;
             }
         }
         if (P.nb > 0) {
@@ -199,10 +192,6 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
                     if (nB < P.capB) __stcs(nbr_b + (size_t)nB * nf + i, q);
                     ++nB;
                 }
-                if (EXT && d2 <= P.ext_r2) {
-                    if (nBE < P.capBE) __stcs(X.nbr_b + (size_t)nBE * nf + i, q);
-                    ++nBE;
-                }
             }
         }
     });
@@ -211,11 +200,6 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
     if (nF > P.capF || nB > P.capB) {
         atomicAdd(&st->overflow, 1u);
         atomicOr(&st->err, ERRBIT_OVERFLOW);
-    }
-    if (EXT) {
-        X.cnt_f[i] = min(nFE, P.capFE);
-        X.cnt_b[i] = min(nBE, P.capBE);
-        if (nFE > P.capFE || nBE > P.capBE) st->ext_overflow = 1u;
     }
 }
 
@@ -314,15 +298,11 @@ void launch_sort(const SimParams& P, const SceneRef& S, int n, const float4* pos
 void launch_build_lists(const SimParams& P, const SceneRef& S, const float4* pos, const unsigned* cell_start,
                         const float4* bpos,
                         const unsigned* bcell_start, unsigned* nbr_f, unsigned* cnt_f, unsigned* nbr_b,
-                        unsigned* cnt_b, DevState* st, cudaStream_t s, const ExtLists& X)
+                        unsigned* cnt_b, DevState* st, cudaStream_t s)
 {
     if (P.nf <= 0) return;
-    if (X.nbr_f)
-        k_ns_build_lists<true><<<blocks_for(P.nf, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
-                                                                      cnt_f, nbr_b, cnt_b, X, st);
-    else
-        k_ns_build_lists<false><<<blocks_for(P.nf, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
-                                                                       cnt_f, nbr_b, cnt_b, X, st);
+    k_ns_build_lists<<<blocks_for(P.nf, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f,
+                                                            nbr_b, cnt_b, st);
 }
 
 void launch_boundary_volume(const SimParams& P, const SceneRef& S, float4* bpos, const unsigned* bcell_start,

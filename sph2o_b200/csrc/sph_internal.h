@@ -27,14 +27,6 @@ struct GatherSet {
     float* f_out[2];
 };
 
-/* PCISPH extended lists (column-major like the exact ones; all NULL: none) */
-struct ExtLists {
-    unsigned* nbr_f;
-    unsigned* cnt_f;
-    unsigned* nbr_b;
-    unsigned* cnt_b;
-};
-
 /* Device pointers of one scene, handed to the solver launchers. */
 struct DeviceArrays {
     float4* pos;
@@ -76,7 +68,6 @@ struct DeviceArrays {
     float* bdp;
     float4* predv;
     unsigned* cell_entry;
-    ExtLists ext;         /* PCISPH extended lists (nbr_f NULL: none) */
 };
 
 /* sph_grid.cu */
@@ -87,7 +78,7 @@ void launch_sort(const SimParams& P, const SceneRef& S, int n, const float4* pos
 void launch_build_lists(const SimParams& P, const SceneRef& S, const float4* pos, const unsigned* cell_start,
                         const float4* bpos,
                         const unsigned* bcell_start, unsigned* nbr_f, unsigned* cnt_f, unsigned* nbr_b,
-                        unsigned* cnt_b, DevState* st, cudaStream_t s, const ExtLists& X = ExtLists{});
+                        unsigned* cnt_b, DevState* st, cudaStream_t s);
 void launch_boundary_volume(const SimParams& P, const SceneRef& S, float4* bpos, const unsigned* bcell_start,
                             float* bvol, cudaStream_t s);
 void launch_unsort_v4(int n, const unsigned* orig, const float4* in, float* out3, cudaStream_t s);

@@ -919,11 +919,7 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
     unsigned it = 0;
     /* the first test uses the residual left by the previous step (PCISPHSolver.cpp:374) */
     double avg = st->pcisph_avg;
-    /* per-iteration maximum predicted displacement (float bits), in the
-       second half of the residual accumulators, which PCISPH leaves unused */
-    unsigned* disp_max = reinterpret_cast<unsigned*>(A.accum + (P.max_it + 2));
     while ((avg > (double)P.eta || it < P.min_it) && it < P.max_it) {
-        float disp2 = 0.0f;
         /* predictVelocityAndPosition */
         for (int i = tid; i < nfi; i += nthr) {
             const float4 a = A.acc[i], pa = A.pacc[i], v = A.vel[i], x = A.pos[i];
@@ -946,21 +942,8 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
                 A.normal[i] = n;
             }
             A.predr[i] = pr;
-            if (P.ext_on) {
-                const float dx = pr.x - x.x, dy = pr.y - x.y, dz = pr.z - x.z;
-                disp2 = fmaxf(disp2, dx * dx + dy * dy + dz * dz);
-            }
-        }
-        if (P.ext_on) {
-            const float wm = warp_max(disp2);
-            if ((threadIdx.x & 31) == 0 && wm > 0.0f) atomicMax(&disp_max[2 * it], __float_as_uint(wm));
         }
         if (!grid_barrier(st)) return;
-        /* the extended lists hold every candidate that can come within h
-           while each particle moved at most ext_disp (2 ext_disp + h below
-           the list radius); otherwise this iteration scans the 27 cells */
-        const bool use_ext = P.ext_on && st->ext_overflow == 0u &&
-                             sqrtf(__uint_as_float(*(volatile unsigned*)&disp_max[2 * it])) <= P.ext_disp;
         /* predictFluidDensities over the start-of-step candidates of the 27
            cells around the particle's current cell, then updatePressure */
         double local = 0.0;
@@ -971,37 +954,22 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
                candidates: the reference's summation order (PCISPHSolver.cpp:180-206) */
             const Grid g = grid_for(P, A.sref, (unsigned)i);
             float rho = 0.0f;
-            if (use_ext) {
-                /* the same candidates in the same order, less those that
-                   cannot be within h: the same sum, bit for bit */
-                const unsigned nFE = A.ext.cnt_f[i], nBE = A.ext.cnt_b[i];
-                for (unsigned kk = 0; kk < nFE; ++kk) {
-                    const float s2 = dist2_exact(pi, A.predr[list_at(A.ext.nbr_f, kk, nf, i)]);
+            for_cells27(xi, P.h, g, [&](unsigned c) {
+                const unsigned e = A.cell_start[c + 1];
+                for (unsigned q = A.cell_start[c]; q < e; ++q) {
+                    const float s2 = dist2_exact(pi, A.predr[q]);
                     if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(s2, P)));
                 }
-                for (unsigned kk = 0; kk < nBE; ++kk) {
-                    const float4 xb = A.bpos[list_at(A.ext.nbr_b, kk, nf, i)];
-                    const float s2 = dist2_exact(pi, xb);
-                    if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(s2, P)));
-                }
-            } else {
+            });
+            if (P.nb > 0)
                 for_cells27(xi, P.h, g, [&](unsigned c) {
-                    const unsigned e = A.cell_start[c + 1];
-                    for (unsigned q = A.cell_start[c]; q < e; ++q) {
-                        const float s2 = dist2_exact(pi, A.predr[q]);
-                        if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(s2, P)));
+                    const unsigned e = A.bcell_start[c + 1];
+                    for (unsigned q = A.bcell_start[c]; q < e; ++q) {
+                        const float4 xb = A.bpos[q];
+                        const float s2 = dist2_exact(pi, xb);
+                        if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(s2, P)));
                     }
                 });
-                if (P.nb > 0)
-                    for_cells27(xi, P.h, g, [&](unsigned c) {
-                        const unsigned e = A.bcell_start[c + 1];
-                        for (unsigned q = A.bcell_start[c]; q < e; ++q) {
-                            const float4 xb = A.bpos[q];
-                            const float s2 = dist2_exact(pi, xb);
-                            if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(s2, P)));
-                        }
-                    });
-            }
             A.rho[i] = rho;
             const float err = fmaxf(0.0f, __fsub_rn(rho, P.rho0));
             A.press[i] = __fadd_rn(A.press[i], __fmul_rn(P.pcisph_delta, err));

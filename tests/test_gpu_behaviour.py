@@ -9,7 +9,6 @@ import pytest
 
 from conftest import load_golden
 from sph2o_b200 import scenes as S
-from sph2o_b200 import api as api_mod
 from sph2o_b200.api import SPH_OK, Scene, SceneDesc, Simulation, SphError, lib
 
 pytestmark = pytest.mark.gpu
@@ -117,20 +116,3 @@ def test_outside_grid_particles_still_found():
     fo, fi, bo, bi = sim.neighbors()
     assert set(fi[fo[0]:fo[1]].tolist()) == {0, 1}
     sim.close()
-
-
-@pytest.mark.parametrize("name,margin", [("pcisph_artificial", 25), ("pcisph_artificial", 1), ("pcib_pcisph", 25)])
-def test_pcisph_extended_lists_equal_cell_scan(name, margin):
-    """PCISPH predicted densities over the extended candidate lists (or, when
-    a displacement leaves the margin, over the 27-cell scan) are the sums of
-    the scan bit for bit: margin 25 % (lists used), 1 % (mostly the scan)
-    and 0 (the scan only) end in identical states."""
-    g = load_golden(name)
-    runs = []
-    for m in (0, margin):
-        sim = Simulation.from_scene(Scene.from_dict(g["scene"]), options={api_mod.OPT_PCISPH_MARGIN: m})
-        sim.step(15)
-        runs.append(sim.state())
-        sim.close()
-    for a, b in zip(*runs):
-        assert np.array_equal(a, b)
