@@ -33,6 +33,8 @@ def lib():
         L.sph_oracle_destroy.argtypes = [P]
         L.sph_oracle_wcsph_adjoint.argtypes = [P, C.c_double, C.c_double, C.c_uint, D, D, C.c_uint, D, C.c_int, D,
                                                D, D, D, D, D, D]
+        L.sph_oracle_set_boundary_normals.argtypes = [P, C.c_uint, F, C.c_float, C.c_float]
+        L.sph_oracle_boundary_state.argtypes = [P, D, D]
         L.sph_oracle_sample_mesh.argtypes = [F, C.c_uint, U, C.c_uint, C.c_float, F, F, F, C.c_size_t,
                                              C.POINTER(C.c_size_t)]
         _lib = L
@@ -54,7 +56,7 @@ def _u(a):
 class Oracle:
     """CPU restatement of the reference; fp64=False reproduces its FP32 build."""
 
-    def __init__(self, desc, fluid, boundary, vel=None, fp64=False, cubes=()):
+    def __init__(self, desc, fluid, boundary, vel=None, fp64=False, cubes=(), boundary_normals=None):
         L = lib()
         self.h = L.sph_oracle_create(C.addressof(desc), 1 if fp64 else 0)
         x = np.ascontiguousarray(fluid, np.float32)
@@ -63,6 +65,10 @@ class Oracle:
         self.nf, self.nb = x.shape[0], b.shape[0]
         L.sph_oracle_set_fluid(self.h, self.nf, _f(x), _f(v))
         L.sph_oracle_set_boundary(self.h, self.nb, _f(b))
+        if boundary_normals is not None:
+            nrm, nfct, tfct = boundary_normals
+            nrm = np.ascontiguousarray(nrm, np.float32).reshape(-1, 3)
+            L.sph_oracle_set_boundary_normals(self.h, nrm.shape[0], _f(nrm), float(nfct), float(tfct))
         for mn, mx, nfct, tfct in cubes:
             L.sph_oracle_add_cube(self.h, _f(np.ascontiguousarray(mn, np.float32)),
                                   _f(np.ascontiguousarray(mx, np.float32)), float(nfct), float(tfct))
@@ -84,6 +90,13 @@ class Oracle:
         out = np.zeros(self.nb)
         lib().sph_oracle_get_boundary_volume(self.h, _d(out))
         return out
+
+    def boundary_state(self):
+        """(densities, pressures) of PCISPH boundary particles, last computed."""
+        d = np.zeros(self.nb)
+        p = np.zeros(self.nb)
+        lib().sph_oracle_boundary_state(self.h, _d(d), _d(p))
+        return d, p
 
     def phase(self, phase):
         vec = phase in (2, 4)

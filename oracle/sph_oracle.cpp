@@ -54,8 +54,18 @@ template <typename R> struct Oracle {
     std::vector<R> bvol;
     struct Cube { V3<R> mn, mx; R nf, tf; };
     std::vector<Cube> cubes;
-    struct Cell { std::vector<uint32_t> f, b; };
+    /* PCISPH boundary method: normals, velocity factors, boundary densities
+       and pressures, predicted velocities, kernel constants */
+    bool pcib = false;
+    std::vector<V3<R>> bn, predv;
+    std::vector<R> bdens, bpress;
+    R pnf = 0, ptf = 0, rest = 0, h2 = 0, poly6c = 0, spikyg = 0;
+    /* since: the neighbour search that first gave the cell candidate lists
+       (HashTable keeps every cell ever touched; a cell first touched by a
+       lookup gets lists at the next search); nsc: searches so far */
+    struct Cell { std::vector<uint32_t> f, b; unsigned since = 0; };
     std::unordered_map<uint64_t, Cell> cells;
+    unsigned nsc = 0;
 
     /* ---- smoothing kernels ---------------------------------------------- */
     /* CubicSpline::W (CubicSpline.h:27-45) */
@@ -121,6 +131,27 @@ template <typename R> struct Oracle {
         const R m = length(rv);
         return m <= h ? lapl * (h - m) : (R)0;
     }
+    /* Poly6::W (Poly6.h:29-42) */
+    R poly6W(const V3<R>& rv) const
+    {
+        const R m = length(rv);
+        const R m2 = m * m;
+        if (m2 <= h2) {
+            const R diff = h2 - m2;
+            return poly6c * diff * diff * diff;
+        }
+        return 0;
+    }
+    /* Spiky::gradW (Spiky.h:44-55) */
+    V3<R> spikyGrad(const V3<R>& rv) const
+    {
+        const R m = length(rv);
+        if (m != 0 && m <= h) {
+            const R diff = h - m;
+            return (-spikyg * diff * diff / m) * rv;
+        }
+        return V3<R>();
+    }
 
     /* ---- set-up (SPHSimulation::importScene/init, SPHSimulation.cpp:117-155, 201-208) */
     void setup(const sph_scene_desc& desc)
@@ -140,6 +171,11 @@ template <typename R> struct Oracle {
         coh1 = (R)(32.0 / M_PI) / h9;
         coh2 = h6 / (R)64;
         lapl = (R)45 / ((R)M_PI * h6);
+        h2 = h * h;
+        poly6c = (R)315 / ((R)(64.0 * M_PI) * h9);
+        spikyg = (R)45 / ((R)M_PI * h6);
+        rest = (R)0.5 * h;
+        pcib = d.boundary_method == SPH_BOUNDARY_PCISPH;
         g = V3<R>((R)d.gravity[0], (R)d.gravity[1], (R)d.gravity[2]);
         dt = (R)d.time_step;
         const R fps_ts = (R)1 / (R)d.fps;
@@ -164,16 +200,21 @@ template <typename R> struct Oracle {
         for (size_t i = 0; i < bx.size(); ++i) {
             int64_t c[3];
             cell_of(bx[i], c);
-            cells[key(c[0], c[1], c[2])].b.push_back((uint32_t)i);
+            Cell& cell = cells[key(c[0], c[1], c[2])];
+            if (cell.since == 0) cell.since = nsc + 1;
+            cell.b.push_back((uint32_t)i);
         }
     }
     void insert_fluid()
     {
         for (auto& kvp : cells) kvp.second.f.clear();
+        ++nsc;
         for (size_t i = 0; i < x.size(); ++i) {
             int64_t c[3];
             cell_of(x[i], c);
-            cells[key(c[0], c[1], c[2])].f.push_back((uint32_t)i);
+            Cell& cell = cells[key(c[0], c[1], c[2])];
+            if (cell.since == 0) cell.since = nsc;
+            cell.f.push_back((uint32_t)i);
         }
     }
     /* the 27 cells of p's cell in x-major offset order (HashTable.cpp:59-65):
@@ -206,7 +247,23 @@ template <typename R> struct Oracle {
             bvol[i] = (R)1 / delta_;
         }
     }
-    R psi(uint32_t b) const { return rho0 * bvol[b]; }
+    /* a boundary particle's density weight: rho0 V_b (Akinci) or its mass
+       rho0 (2r)^3 (PCISPH method, SPHSimulation.cpp:435-437) */
+    R psi(uint32_t b) const { return pcib ? mass : rho0 * bvol[b]; }
+
+    /* whether p's cell held candidate lists at the last search; a lookup of
+       an untouched cell creates its entry (HashTable's operator[]) */
+    bool listed(const V3<R>& p)
+    {
+        int64_t c[3];
+        cell_of(p, c);
+        auto it = cells.find(key(c[0], c[1], c[2]));
+        if (it == cells.end()) {
+            cells[key(c[0], c[1], c[2])].since = nsc + 1;
+            return false;
+        }
+        return it->second.since <= nsc;
+    }
 
     /* SPHSolver::computeFluidDensities (SPHSolver.cpp:42-89), Akinci branch */
     void densities()
@@ -243,7 +300,7 @@ template <typename R> struct Oracle {
     {
         const size_t n = x.size();
         const R h2 = h * h;
-        const R visc_c = (R)d.viscosity, bvisc = (R)d.boundary_viscosity;
+        const R visc_c = (R)d.viscosity, bvisc = pcib ? (R)0 : (R)d.boundary_viscosity; /* an Akinci-only term */
         if (visc && d.viscosity_method == SPH_VISCOSITY_ARTIFICIAL) {
             /* ArtificialViscosity::step (ArtificialViscosity.cpp:6-54) */
             for (size_t i = 0; i < n; ++i) {
@@ -354,8 +411,13 @@ template <typename R> struct Oracle {
                            },
                            [](uint32_t) {});
             const R dpb = press[i] / (rho0 * rho0);
-            for_candidates(x[i], [](uint32_t) {},
-                           [&](uint32_t b) { a[i] -= psi(b) * (dpi + dpb) * gradW(x[i] - bx[b]); });
+            if (pcib) /* WCSPHSolver.cpp:160-171 */
+                for_candidates(x[i], [](uint32_t) {}, [&](uint32_t b) {
+                    a[i] -= mass * (dpi + bpress[b] / (bdens[b] * bdens[b])) * gradW(x[i] - bx[b]);
+                });
+            else
+                for_candidates(x[i], [](uint32_t) {},
+                               [&](uint32_t b) { a[i] -= psi(b) * (dpi + dpb) * gradW(x[i] - bx[b]); });
         }
     }
     /* SPHSolver::integrate (SPHSolver.cpp:139-168) */
@@ -393,15 +455,95 @@ template <typename R> struct Oracle {
             }
     }
 
+    /* ---- PCISPH boundary method (PCISPHBoundaryObject.cpp:218-447) ---- */
+    /* boundary densities: SPHSolver::computeBoundaryDensities (cubic spline,
+       SPHSolver.cpp:91-124) or PCISPHSolver::predictBoundaryDensities (Poly6
+       at the predicted fluid positions, PCISPHSolver.cpp:211-244) */
+    void boundary_densities(bool poly6, const std::vector<V3<R>>& fx)
+    {
+        for (size_t b = 0; b < bx.size(); ++b) {
+            R dens = 0;
+            for_candidates(bx[b],
+                           [&](uint32_t j) { dens += mass * (poly6 ? poly6W(bx[b] - fx[j]) : W(bx[b] - fx[j])); },
+                           [&](uint32_t q) { dens += mass * (poly6 ? poly6W(bx[b] - bx[q]) : W(bx[b] - bx[q])); });
+            bdens[b] = dens;
+        }
+    }
+    /* WCSPHSolver::computeBoundaryPressures (WCSPHSolver.cpp:97-114) */
+    void boundary_pressures()
+    {
+        const R k = (R)d.stiffness, gm = (R)d.gamma;
+        for (size_t b = 0; b < bx.size(); ++b)
+            bpress[b] = std::max((R)0, k * rho0 / gm * (std::pow(bdens[b] / rho0, gm) - (R)1));
+    }
+    /* collision sums of point p (test) weighted at q (correctPositions /
+       correctPredPositions): writes the normal (glm::normalize of the
+       weighted sum, NaN when it is zero) and returns whether to push, with
+       the push length (1 / wsum) w2sum */
+    bool collide(size_t i, const V3<R>& p, const V3<R>& q, bool lookup, R& s)
+    {
+        V3<R> avg;
+        R wsum = 0, w2sum = 0;
+        if (!lookup || listed(p))
+            for_candidates(p, [](uint32_t) {}, [&](uint32_t b) {
+                if (length(p - bx[b]) < rest) {
+                    const R l = length(q - bx[b]);
+                    const R w = std::max((R)0, (rest - l) / rest);
+                    wsum += w;
+                    w2sum += w * (rest - l);
+                    avg += w * bn[b];
+                }
+            });
+        nrm[i] = avg * ((R)1 / std::sqrt(dot(avg, avg)));
+        s = (R)1 / wsum * w2sum;
+        return wsum > 0;
+    }
+    /* correctPositions at the updated positions, weighted there (WCSPH,
+       DFSPH) or at the predicted positions (PCISPH) */
+    void pcib_positions(bool pred)
+    {
+        for (size_t i = 0; i < x.size(); ++i) {
+            R sc;
+            if (collide(i, x[i], pred ? predr[i] : x[i], true, sc)) x[i] += sc * nrm[i];
+        }
+    }
+    /* correctPredPositions: tested at the current position, weighted at and
+       moving the predicted one */
+    void pcib_pred_positions()
+    {
+        for (size_t i = 0; i < x.size(); ++i) {
+            R sc;
+            if (collide(i, x[i], predr[i], false, sc)) predr[i] += sc * nrm[i];
+        }
+    }
+    /* correctVelocities from u = v (WCSPH, DFSPH) or the predicted velocity (PCISPH) */
+    void pcib_velocities(bool pred)
+    {
+        for (size_t i = 0; i < x.size(); ++i) {
+            const V3<R>& n = nrm[i];
+            if (!(length(n) > 0)) continue;
+            const V3<R> u = pred ? predv[i] : v[i];
+            const V3<R> nv = dot(u, n) * n;
+            const V3<R> tv = u - nv;
+            v[i] = ptf * tv - pnf * nv;
+        }
+    }
+
     void wcsph_step()
     {
         insert_fluid();
         densities();
+        if (pcib) boundary_densities(false, x);
         wcsph_pressures();
+        if (pcib) boundary_pressures();
         wcsph_pressure_force();
         nonpressure();
         integrate();
         cube_correct();
+        if (pcib) { /* WCSPHSolver.cpp:62-72 */
+            pcib_positions(false);
+            pcib_velocities(false);
+        }
         time += dt;
     }
 
@@ -431,13 +573,16 @@ template <typename R> struct Oracle {
         nonpressure();
         const size_t n = x.size();
         for (size_t i = 0; i < n; ++i) { press[i] = 0; pacc[i] = V3<R>(); }
+        if (pcib) std::fill(bpress.begin(), bpress.end(), (R)0);
         unsigned it = 0;
         while ((pci_avg > (R)d.eta || it < d.min_iterations) && it < d.max_iterations) {
             for (size_t i = 0; i < n; ++i) {
                 const V3<R> acc = a[i] + pacc[i] + g;
                 const V3<R> pv = v[i] + acc * dt;
+                predv[i] = pv;
                 predr[i] = x[i] + pv * dt;
             }
+            if (pcib) pcib_pred_positions();
             /* predicted densities over the start-of-step candidates of x_i's cell */
             for (size_t i = 0; i < n; ++i) {
                 R dens = 0;
@@ -452,6 +597,10 @@ template <typename R> struct Oracle {
                 avg += err / rho0;
             }
             pci_avg = avg / (R)n;
+            if (pcib) { /* predictBoundaryDensities + the boundary part of updatePressure */
+                boundary_densities(true, predr);
+                for (size_t b = 0; b < bx.size(); ++b) bpress[b] += delta * std::max((R)0, bdens[b] - rho0);
+            }
             for (size_t i = 0; i < n; ++i) {
                 V3<R> pa;
                 const R dpi = press[i] / (rho[i] * rho[i]);
@@ -459,7 +608,12 @@ template <typename R> struct Oracle {
                                [&](uint32_t j) {
                                    pa -= mass * (dpi + press[j] / (rho[j] * rho[j])) * gradW(x[i] - x[j]);
                                },
-                               [&](uint32_t b) { pa -= psi(b) * dpi * gradW(x[i] - bx[b]); });
+                               [&](uint32_t b) {
+                                   if (pcib) /* PCISPHSolver.cpp:336-347 */
+                                       pa -= mass * (dpi + bpress[b] / (bdens[b] * bdens[b])) * spikyGrad(x[i] - bx[b]);
+                                   else
+                                       pa -= psi(b) * dpi * gradW(x[i] - bx[b]);
+                               });
                 pacc[i] = pa;
             }
             ++it;
@@ -473,6 +627,10 @@ template <typename R> struct Oracle {
             a[i] = V3<R>();
         }
         cube_correct();
+        if (pcib) { /* PCISPHSolver.cpp:64-74 */
+            pcib_positions(true);
+            pcib_velocities(true);
+        }
         time += dt;
     }
 
@@ -560,6 +718,7 @@ template <typename R> struct Oracle {
         nonpressure();
         update_time_step();
         for (size_t i = 0; i < n; ++i) { v[i] += (a[i] + g) * dt; a[i] = V3<R>(); }
+        if (pcib) pcib_velocities(false); /* DFSPHSolver.cpp:46-52 */
         const R ts2 = dt * dt;
         /* densityWarmStart (:851-955) */
         predict_densities();
@@ -582,6 +741,7 @@ template <typename R> struct Oracle {
         its = it;
         avg_dens = avg;
         for (size_t i = 0; i < n; ++i) x[i] += v[i] * dt;  /* updatePositions (:204-224) */
+        if (pcib) pcib_positions(false);                   /* :60-70 */
         insert_fluid();
         densities();
         compute_alpha();
@@ -614,13 +774,15 @@ template <typename R> struct Oracle {
         v.resize(n); a.assign(n, V3<R>()); nrm.assign(n, V3<R>()); predr.assign(n, V3<R>()); pacc.assign(n, V3<R>());
         rho.assign(n, 0); alpha.assign(n, 0); press.assign(n, 0); kk.assign(n, 0); kv.assign(n, 0);
         kws.assign(n, 0); kvws.assign(n, 0); pred.assign(n, 0); div.assign(n, 0);
+        predv.assign(n, V3<R>());
+        bdens.assign(bx.size(), 0); bpress.assign(bx.size(), 0);
     }
 
     void init()
     {
         resize(x.size());
         insert_boundary();
-        boundary_volumes();
+        if (!pcib) boundary_volumes();
         if (d.simulation_method == SPH_PCISPH) pcisph_scaling();
         insert_fluid();
         if (d.simulation_method == SPH_DFSPH) {
@@ -686,6 +848,36 @@ int sph_oracle_set_boundary(sph_oracle* o, unsigned n, const float* xyz)
     };
     fill(o->f);
     fill(o->dd);
+    return SPH_OK;
+}
+
+int sph_oracle_set_boundary_normals(sph_oracle* o, unsigned n, const float* nxyz, float normal_fct,
+                                    float tangential_fct)
+{
+    if (!o || (n && !nxyz)) return SPH_ERR_ARG;
+    auto fill = [&](auto& S) {
+        using R = std::remove_reference_t<decltype(S.r)>;
+        S.bn.resize(n);
+        for (unsigned i = 0; i < n; ++i) S.bn[i] = {(R)nxyz[3 * i], (R)nxyz[3 * i + 1], (R)nxyz[3 * i + 2]};
+        S.pnf = (R)normal_fct;
+        S.ptf = (R)tangential_fct;
+    };
+    fill(o->f);
+    fill(o->dd);
+    return SPH_OK;
+}
+
+int sph_oracle_boundary_state(sph_oracle* o, double* dens, double* press)
+{
+    if (!o) return SPH_ERR_ARG;
+    auto get = [&](auto& S) {
+        for (size_t b = 0; b < S.bdens.size(); ++b) {
+            if (dens) dens[b] = S.bdens[b];
+            if (press) press[b] = S.bpress[b];
+        }
+    };
+    if (o->fp64) get(o->dd);
+    else get(o->f);
     return SPH_OK;
 }
 
@@ -759,6 +951,10 @@ int sph_oracle_phase(sph_oracle* o, int phase, double* out)
         using R = std::remove_reference_t<decltype(S.r)>;
         S.insert_fluid();
         S.densities();
+        if (S.pcib) { /* computeDensities covers the boundary particles; WCSPH their pressures */
+            S.boundary_densities(false, S.x);
+            if (S.d.simulation_method == SPH_WCSPH) S.boundary_pressures();
+        }
         const size_t n = S.x.size();
         switch (phase) {
         case SPH_PHASE_DENSITY: for (size_t i = 0; i < n; ++i) out[i] = S.rho[i]; break;

@@ -26,6 +26,12 @@ typedef struct sph_oracle sph_oracle;
 sph_oracle* sph_oracle_create(const sph_scene_desc* desc, int fp64);
 int sph_oracle_set_fluid(sph_oracle* o, unsigned n, const float* xyz, const float* v);
 int sph_oracle_set_boundary(sph_oracle* o, unsigned n, const float* xyz);
+/* PCISPH boundary method: normals of the boundary particles (same order) and
+   the object's normalFct / tangFct */
+int sph_oracle_set_boundary_normals(sph_oracle* o, unsigned n, const float* nxyz, float normal_fct,
+                                    float tangential_fct);
+/* PCISPH boundary method: the last computed boundary densities / pressures */
+int sph_oracle_boundary_state(sph_oracle* o, double* dens, double* press);
 /* cube boundary (boundary method 0), applied after integration in order */
 int sph_oracle_add_cube(sph_oracle* o, const float* mn, const float* mx, float normal_fct, float tangential_fct);
 int sph_oracle_init(sph_oracle* o);

@@ -41,12 +41,6 @@ def golden_names():
     return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("emitter_"))
 
 
-def oracle_golden_names():
-    """Golden scenes the CPU oracle restates (not the PCISPH boundary method,
-    whose parity is pinned on the reference's fixtures directly)."""
-    return [n for n in golden_names() if not n.startswith("pcib_")]
-
-
 def emitter_golden_names():
     return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("emitter_"))
 

@@ -10,11 +10,11 @@ reference the same way."""
 import numpy as np
 import pytest
 
-from conftest import load_golden, oracle_golden_names, rel_err
+from conftest import golden_names, load_golden, rel_err
 from oracle.oracle import Oracle
 from sph2o_b200.api import Scene
 
-NAMES = oracle_golden_names()
+NAMES = golden_names()
 
 
 def make(g, fp64=False):
@@ -22,20 +22,26 @@ def make(g, fp64=False):
     # geometries (sampled on the GPU) are left out of this parse
     scene = {**g["scene"], "Boundary": [{**b, "geometry": []} for b in g["scene"].get("Boundary", [])]}
     sc = Scene.from_dict(scene)
-    return Oracle(sc.desc(), g["init_pos"], g["bpos"], fp64=fp64, cubes=sc.cube_boundaries())
+    return Oracle(sc.desc(), g["init_pos"], g["bpos"], fp64=fp64, cubes=sc.cube_boundaries(),
+                  boundary_normals=sc.boundary_normals())
 
 
 @pytest.mark.parametrize("name", NAMES)
 def test_phases_bit_exact(name):
     g = load_golden(name)
     o = make(g)
-    assert np.array_equal(o.boundary_volume().astype(np.float32), g["bvol"])
+    if "bnormal" not in g:
+        assert np.array_equal(o.boundary_volume().astype(np.float32), g["bvol"])
     assert np.array_equal(o.phase(0).astype(np.float32), g["density"])
+    if "bdensity" in g:  # PCISPH boundary particles: densities (and WCSPH pressures)
+        assert np.array_equal(o.boundary_state()[0].astype(np.float32), g["bdensity"])
     if "alpha" in g:
         assert np.array_equal(o.phase(1).astype(np.float32), g["alpha"])
     assert np.array_equal(o.phase(2).astype(np.float32), g["a_np"])
     if "pressure" in g:
         assert np.array_equal(o.phase(3).astype(np.float32), g["pressure"])
+        if "bpressure" in g:
+            assert np.array_equal(o.boundary_state()[1].astype(np.float32), g["bpressure"])
         assert np.array_equal(o.phase(4).astype(np.float32), g["a_pressure"])
     fo, fi, bo, bi = o.neighbors()
     assert np.array_equal(fo, g["nbr_f_offsets"]) and np.array_equal(fi, g["nbr_f"])
@@ -74,3 +80,17 @@ def test_trace_fp64(name):
     long_trace = ref.shape[0] > 20
     assert rel_err(x, g["final_pos_f64"]) <= (1e-5 if long_trace else 1e-9)
     assert rel_err(v, g["final_vel_f64"]) <= (1e-4 if long_trace else 1e-6)
+
+
+@pytest.mark.parametrize("name", [n for n in NAMES if n.startswith("pcib_")])
+def test_pcisph_boundary_trajectory_bit_exact(name):
+    """PCISPH boundary method: the FP32 restatement ends exactly where the
+    reference's FP32 build ends (60-400 steps), the collision passes'
+    skipped lookups of cells first touched since the last search included
+    (pcib_wcsph_wallslide)."""
+    g = load_golden(name)
+    o = make(g)
+    o.step(g["trace_f32"].shape[0])
+    x, v, _ = o.state()
+    assert np.array_equal(x.astype(np.float32), g["final_pos_f32"])
+    assert np.array_equal(v.astype(np.float32), g["final_vel_f32"])
