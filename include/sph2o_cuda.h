@@ -221,8 +221,12 @@ enum sph_option {
     SPH_OPT_CELL_ORDER = 1,       /* 0 (default): 4x4x4 cell bricks, Morton inside; 1: linear, x fastest */
     SPH_OPT_SOLVER_OCCUPANCY = 2, /* DFSPH persistent solver blocks per SM: 8 (default) or 4 */
     SPH_OPT_PASS_BLOCK = 3,       /* threads per block of the particle-pass kernels: 256 (default) or 128 */
-    SPH_OPT_SOLVER_LANES = 4      /* lanes sharing one particle's neighbour list in the persistent DFSPH
+    SPH_OPT_SOLVER_LANES = 4,     /* lanes sharing one particle's neighbour list in the persistent DFSPH
                                      solver: 1, 2 (default) or 4 */
+    SPH_OPT_POSITION_RESIDUAL = 5 /* 1: every position keeps the rounding residual of its integration
+                                     (float pair, error-free sums), so long runs of small steps keep about
+                                     twice float precision; 0 (default): FP32 positions rounded as the
+                                     reference rounds them. Single scenes, set before sph_init. */
 };
 /* Number of values sph_autotune chooses (options 1..4 in order). */
 #define SPH_TUNE_COUNT 4

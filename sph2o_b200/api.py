@@ -27,7 +27,7 @@ STATUS = {
     -7: "SPH_ERR_NO_DEVICE", -8: "SPH_ERR_IO", -9: "SPH_ERR_CAPACITY",
 }
 PHASE_DENSITY, PHASE_ALPHA, PHASE_NONPRESSURE_ACC, PHASE_PRESSURE, PHASE_PRESSURE_ACC = range(5)
-OPT_CUDA_GRAPHS, OPT_CELL_ORDER, OPT_SOLVER_OCCUPANCY, OPT_PASS_BLOCK, OPT_SOLVER_LANES = range(5)
+OPT_CUDA_GRAPHS, OPT_CELL_ORDER, OPT_SOLVER_OCCUPANCY, OPT_PASS_BLOCK, OPT_SOLVER_LANES, OPT_POSITION_RESIDUAL = range(6)
 TUNE_COUNT = 4
 PROF_NAMES = ["sort", "lists", "density", "normals", "forces", "density_solve", "divergence_solve",
               "pressure_solve"]
@@ -308,9 +308,11 @@ class Scene:
 class Simulation:
     """One GPU simulation context (sph_ctx)."""
 
-    def __init__(self, desc: SceneDesc, fluid, boundary, vel=None, emitters=(), cubes=(), boundary_normals=None):
+    def __init__(self, desc: SceneDesc, fluid, boundary, vel=None, emitters=(), cubes=(), boundary_normals=None,
+                 options=None):
         """boundary_normals: (normals (nb, 3), normal_fct, tangential_fct) for
-        the PCISPH boundary method (boundary_method 1)."""
+        the PCISPH boundary method (boundary_method 1); options: {option:
+        value} set before sph_init (e.g. OPT_POSITION_RESIDUAL)."""
         L = lib()
         h = C.c_void_p()
         rc = L.sph_create(C.byref(desc), C.byref(h))
@@ -333,14 +335,16 @@ class Simulation:
             self._check(L.sph_add_cube_boundary(h, _fptr(mn), _fptr(mx), float(nfct), float(tfct)))
         for e in emitters:
             self._check(L.sph_add_emitter(h, C.byref(e)))
+        for opt, val in (options or {}).items():
+            self._check(L.sph_set_option(h, int(opt), int(val)))
         self._check(L.sph_init(h))
         self.nf, self.nb = L.sph_num_fluid(h), b.shape[0]
 
     @classmethod
-    def from_scene(cls, scene: Scene, vel=None):
+    def from_scene(cls, scene: Scene, vel=None, options=None):
         x, v = scene.fluid()
         return cls(scene.desc(), x, scene.boundary(), v if vel is None else vel, emitters=scene.emitters(),
-                   cubes=scene.cube_boundaries(), boundary_normals=scene.boundary_normals())
+                   cubes=scene.cube_boundaries(), boundary_normals=scene.boundary_normals(), options=options)
 
     def num_active(self):
         n = C.c_uint()

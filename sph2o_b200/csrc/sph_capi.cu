@@ -41,6 +41,7 @@ struct Buffers {
     unsigned *orig, *orig2;
     float *kws, *kws2, *kvws, *kvws2;
     float4 *normal, *normal2;
+    float4 *plo, *plo2;
     bool lists_valid;
 };
 
@@ -117,6 +118,10 @@ struct sph_ctx {
     float4 *bnormal = nullptr, *normal2 = nullptr, *predv = nullptr;
     float *bdens = nullptr, *bpress = nullptr, *bdp = nullptr;
     unsigned* cell_entry = nullptr;
+    /* position residuals (SPH_OPT_POSITION_RESIDUAL): current / spare */
+    int pos_lo = 0;
+    float4 *plo = nullptr, *plo2 = nullptr;
+    float4* snap_plo = nullptr;
     /* autotune snapshot */
     float4 *snap_pos = nullptr, *snap_vel = nullptr;
     unsigned* snap_orig = nullptr;
@@ -347,6 +352,8 @@ DeviceArrays arrays(sph_ctx* c)
     A.accum = c->accum; A.st = c->st;
     A.bnormal = c->bnormal; A.bdens = c->bdens; A.bpress = c->bpress; A.bdp = c->bdp;
     A.predv = c->predv; A.cell_entry = c->cell_entry;
+    A.plo = c->P.pos_lo ? c->plo : nullptr;
+    A.plo_alt = c->P.pos_lo ? c->plo2 : nullptr;
     if (c->nscenes) {
         A.sref.scenes = c->d_scenes;
         A.sref.scene_of = c->d_scene_of;
@@ -430,6 +437,7 @@ int neighbor_search(sph_ctx* c)
     g.cell_out = c->cell_sorted;
     g.v4_in[0] = c->pos; g.v4_out[0] = c->pos2;
     g.v4_in[1] = c->vel; g.v4_out[1] = c->vel2;
+    if (c->P.pos_lo) { g.v4_in[3] = c->plo; g.v4_out[3] = c->plo2; }
     if (c->desc.simulation_method == SPH_DFSPH) {
         g.f_in[0] = c->kws; g.f_out[0] = c->kws2;
         g.f_in[1] = c->kvws; g.f_out[1] = c->kvws2;
@@ -445,6 +453,7 @@ int neighbor_search(sph_ctx* c)
     std::swap(c->pos, c->pos2);
     std::swap(c->vel, c->vel2);
     std::swap(c->orig, c->orig2);
+    if (c->P.pos_lo) std::swap(c->plo, c->plo2);
     if (c->desc.simulation_method == SPH_DFSPH) {
         std::swap(c->kws, c->kws2);
         std::swap(c->kvws, c->kvws2);
@@ -500,6 +509,7 @@ int step_wcsph(sph_ctx* c)
     { Phase ph(c, SPH_PROF_FORCES, 1); launch_forces(c->P, A, FORCE_WCSPH, c->pass_block, c->stream); }
     std::swap(c->pos, c->pos2);
     std::swap(c->vel, c->vel2);
+    if (c->P.pos_lo) std::swap(c->plo, c->plo2);
     c->lists_valid = false;
     cube_correct(c); /* WCSPHSolver.cpp:51-60 */
     if (c->P.pcib) { /* WCSPHSolver.cpp:62-72 */
@@ -672,7 +682,7 @@ int eager_step(sph_ctx* c)
 Buffers get_buffers(const sph_ctx* c)
 {
     return {c->pos, c->pos2, c->vel, c->vel2, c->orig, c->orig2, c->kws, c->kws2, c->kvws, c->kvws2, c->normal,
-            c->normal2, c->lists_valid};
+            c->normal2, c->plo, c->plo2, c->lists_valid};
 }
 
 void set_buffers(sph_ctx* c, const Buffers& b)
@@ -680,6 +690,7 @@ void set_buffers(sph_ctx* c, const Buffers& b)
     c->pos = b.pos; c->pos2 = b.pos2; c->vel = b.vel; c->vel2 = b.vel2; c->orig = b.orig; c->orig2 = b.orig2;
     c->kws = b.kws; c->kws2 = b.kws2; c->kvws = b.kvws; c->kvws2 = b.kvws2; c->lists_valid = b.lists_valid;
     c->normal = b.normal; c->normal2 = b.normal2;
+    c->plo = b.plo; c->plo2 = b.plo2;
 }
 
 /* nsteps (1 or 2) steps as one CUDA graph, captured on first use for the
@@ -1039,6 +1050,12 @@ int sph_init(sph_ctx* c)
     c->orig_base = c->orig;
     c->kws_base = c->kws;
     if ((rc = alloc_lists(c)) != SPH_OK) return rc;
+    if (c->pos_lo) {
+        if (c->nscenes) return fail(c, SPH_ERR_ARG, "position residuals apply to single scenes, not to batches");
+        if ((rc = dalloc(c, &c->plo, nf)) != SPH_OK) return rc;
+        if ((rc = dalloc(c, &c->plo2, nf)) != SPH_OK) return rc;
+        P.pos_lo = 1;
+    }
     c->accum_len = 2 * ((size_t)P.max_it + 2) * std::max(1u, c->nscenes);
     if ((rc = dalloc(c, &c->accum, c->accum_len)) != SPH_OK) return rc;
     if (c->nscenes) {
@@ -1290,6 +1307,8 @@ int sph_set_state(sph_ctx* c, const float* xyz, const float* v)
     if (xyz) {
         CUDA_TRY(c, cudaMemcpyAsync(tmp, xyz, 3 * nf * sizeof(float), cudaMemcpyHostToDevice, c->stream));
         launch_sort_v3((int)na, c->orig, tmp, c->pos, c->stream);
+        /* the given positions are exact: no residual */
+        if (c->P.pos_lo) CUDA_TRY(c, cudaMemsetAsync(c->plo, 0, nf * sizeof(float4), c->stream));
     }
     if (v) {
         CUDA_TRY(c, cudaMemcpyAsync(tmp, v, 3 * nf * sizeof(float), cudaMemcpyHostToDevice, c->stream));
@@ -1539,6 +1558,10 @@ int snapshot(sph_ctx* c, bool save)
     if ((rc = cp(c->st, c->snap_st, sizeof(DevState))) != SPH_OK) return rc;
     if (c->nscenes && (rc = cp(c->d_sst, c->snap_sst, c->nscenes * sizeof(SceneState))) != SPH_OK) return rc;
     if (c->d_emit && (rc = cp(c->d_emit, c->snap_emit, c->emitters.size() * sizeof(EmitterState))) != SPH_OK) return rc;
+    if (c->P.pos_lo) {
+        if (!c->snap_plo && (rc = dalloc(c, &c->snap_plo, nf)) != SPH_OK) return rc;
+        if ((rc = cp(c->plo, c->snap_plo, nf * sizeof(float4))) != SPH_OK) return rc;
+    }
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return SPH_OK;
 }
@@ -1649,6 +1672,11 @@ int sph_set_option(sph_ctx* c, int option, int value)
         c->solver_tpp = value;
         drop_graphs(c);
         return SPH_OK;
+    case SPH_OPT_POSITION_RESIDUAL:
+        if (value != 0 && value != 1) return fail(c, SPH_ERR_ARG, "the position residual option is 0 or 1");
+        if (c->initialized) return fail(c, SPH_ERR_STATE, "position residuals are chosen before sph_init");
+        c->pos_lo = value;
+        return SPH_OK;
     default:
         return fail(c, SPH_ERR_ARG, "unknown option");
     }
@@ -1663,6 +1691,7 @@ int sph_get_option(const sph_ctx* c, int option, int* value)
     case SPH_OPT_SOLVER_OCCUPANCY: *value = c->solver_occ; return SPH_OK;
     case SPH_OPT_PASS_BLOCK: *value = c->pass_block; return SPH_OK;
     case SPH_OPT_SOLVER_LANES: *value = c->solver_tpp; return SPH_OK;
+    case SPH_OPT_POSITION_RESIDUAL: *value = c->pos_lo; return SPH_OK;
     default: return SPH_ERR_ARG;
     }
 }
@@ -1923,6 +1952,7 @@ int adj_supported(sph_ctx* c)
     if (c->P.dynamic) return fail(c, SPH_ERR_ARG, "the WCSPH adjoint does not cover emitters");
     if (c->desc.boundary_method != SPH_BOUNDARY_AKINCI)
         return fail(c, SPH_ERR_ARG, "the WCSPH adjoint covers Akinci boundaries (boundary method 2) only");
+    if (c->P.pos_lo) return fail(c, SPH_ERR_ARG, "the WCSPH adjoint differentiates FP32 positions (no residuals)");
     if (c->P.st_on || c->P.adh_on)
         return fail(c, SPH_ERR_ARG, "the WCSPH adjoint covers neither surface tension nor adhesion");
     if (c->P.visc_method != -1 && c->P.visc_method != SPH_VISCOSITY_ARTIFICIAL)

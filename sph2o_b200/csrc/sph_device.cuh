@@ -67,6 +67,9 @@ struct SimParams {
     float rest_r;              /* collision distance 0.5 h (PCISPHBoundaryObject.cpp:222)        */
     float poly6_c;             /* Poly6 315 / (64 pi h^9)                 (Poly6.h:25)            */
     float spiky_g;             /* Spiky gradient 45 / (pi h^6)            (Spiky.h:25)            */
+    /* 1: positions carry their rounding residual (DeviceArrays::plo) and
+       integrate as float pairs; 0: plain FP32 as the reference rounds */
+    int pos_lo;
 };
 
 /* Device-resident solver state; read by the host after a step. */
@@ -100,6 +103,21 @@ __device__ __forceinline__ int active_n(const SimParams& P, const DevState* st)
 __device__ __forceinline__ double advance_time(double t, float dt)
 {
     return (double)__fadd_rn((float)t, dt);
+}
+
+/* x + d for one position coordinate. With the residual on, lo holds what
+   the float x has lost of the exact sum of all the steps so far; the pair is
+   advanced with an error-free float sum (Knuth's TwoSum), so a long run of
+   steps much smaller than x's spacing is integrated to about twice float
+   precision while every pass keeps reading the float x. */
+__device__ __forceinline__ float pos_add(float x, float& lo, float d, int on)
+{
+    if (!on) return __fadd_rn(x, d);
+    const float t = __fadd_rn(lo, d);
+    const float s = __fadd_rn(x, t);
+    const float bp = __fsub_rn(s, x);
+    lo = __fadd_rn(__fsub_rn(x, __fsub_rn(s, bp)), __fsub_rn(t, bp));
+    return s;
 }
 
 /* A cube boundary (CubeBoundaryObject.h:6-27): box and velocity factors. */

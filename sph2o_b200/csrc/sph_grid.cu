@@ -150,6 +150,7 @@ __global__ void __launch_bounds__(256) k_ns_rank_gather(int n, const unsigned* _
     if (g.v4_in[0]) g.v4_out[0][dst] = g.v4_in[0][src];
     if (g.v4_in[1]) g.v4_out[1][dst] = g.v4_in[1][src];
     if (g.v4_in[2]) g.v4_out[2][dst] = g.v4_in[2][src];
+    if (g.v4_in[3]) g.v4_out[3][dst] = g.v4_in[3][src];
     if (g.f_in[0]) g.f_out[0][dst] = g.f_in[0][src];
     if (g.f_in[1]) g.f_out[1][dst] = g.f_in[1][src];
 }

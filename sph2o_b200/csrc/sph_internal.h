@@ -21,8 +21,8 @@ struct GatherSet {
     const unsigned* n_dev;
     unsigned* orig_out;
     unsigned* cell_out;
-    const float4* v4_in[3];
-    float4* v4_out[3];
+    const float4* v4_in[4];
+    float4* v4_out[4];
     const float* f_in[2];
     float* f_out[2];
 };
@@ -68,6 +68,10 @@ struct DeviceArrays {
     float* bdp;
     float4* predv;
     unsigned* cell_entry;
+    /* position residuals (SimParams::pos_lo; NULL when off) and the WCSPH
+       integration target */
+    float4* plo;
+    float4* plo_alt;
 };
 
 /* sph_grid.cu */

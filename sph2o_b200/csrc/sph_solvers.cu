@@ -340,10 +340,13 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
             ax = __fadd_rn(ax, P.gx); ay = __fadd_rn(ay, P.gy); az = __fadd_rn(az, P.gz);
             const float nvx = __fadd_rn(vi.x, __fmul_rn(ax, dt)), nvy = __fadd_rn(vi.y, __fmul_rn(ay, dt)),
                         nvz = __fadd_rn(vi.z, __fmul_rn(az, dt));
-            const float px = __fadd_rn(xi.x, __fmul_rn(nvx, dt)), py = __fadd_rn(xi.y, __fmul_rn(nvy, dt)),
-                        pz = __fadd_rn(xi.z, __fmul_rn(nvz, dt));
+            float4 lo = P.pos_lo ? A.plo[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const float px = pos_add(xi.x, lo.x, __fmul_rn(nvx, dt), P.pos_lo),
+                        py = pos_add(xi.y, lo.y, __fmul_rn(nvy, dt), P.pos_lo),
+                        pz = pos_add(xi.z, lo.z, __fmul_rn(nvz, dt), P.pos_lo);
             A.vel_alt[i] = make_float4(nvx, nvy, nvz, 0.0f);
             A.pos_alt[i] = make_float4(px, py, pz, 0.0f);
+            if (P.pos_lo) A.plo_alt[i] = lo;
             if (!isfinite(px) || !isfinite(py) || !isfinite(pz)) atomicOr(&A.st->err, ERRBIT_NAN);
         }
         if (A.sst) {
@@ -694,10 +697,12 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
         for (int i = tid; i < nfi; i += nthr) {
             const float4 v = A.vel[i];
             float4 x = A.pos[i];
-            x.x = __fadd_rn(x.x, __fmul_rn(v.x, dt));
-            x.y = __fadd_rn(x.y, __fmul_rn(v.y, dt));
-            x.z = __fadd_rn(x.z, __fmul_rn(v.z, dt));
+            float4 lo = P.pos_lo ? A.plo[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            x.x = pos_add(x.x, lo.x, __fmul_rn(v.x, dt), P.pos_lo);
+            x.y = pos_add(x.y, lo.y, __fmul_rn(v.y, dt), P.pos_lo);
+            x.z = pos_add(x.z, lo.z, __fmul_rn(v.z, dt), P.pos_lo);
             A.pos[i] = x;
+            if (P.pos_lo) A.plo[i] = lo;
             bad |= !isfinite(x.x) || !isfinite(x.y) || !isfinite(x.z);
         }
         if (bad) atomicOr(&st->err, ERRBIT_NAN);
@@ -1041,8 +1046,11 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
         const float azz = __fadd_rn(a.z, __fadd_rn(P.gz, pa.z));
         v.x = __fadd_rn(v.x, __fmul_rn(axx, dt)); v.y = __fadd_rn(v.y, __fmul_rn(ayy, dt));
         v.z = __fadd_rn(v.z, __fmul_rn(azz, dt));
-        x.x = __fadd_rn(x.x, __fmul_rn(v.x, dt)); x.y = __fadd_rn(x.y, __fmul_rn(v.y, dt));
-        x.z = __fadd_rn(x.z, __fmul_rn(v.z, dt));
+        float4 lo = P.pos_lo ? A.plo[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        x.x = pos_add(x.x, lo.x, __fmul_rn(v.x, dt), P.pos_lo);
+        x.y = pos_add(x.y, lo.y, __fmul_rn(v.y, dt), P.pos_lo);
+        x.z = pos_add(x.z, lo.z, __fmul_rn(v.z, dt), P.pos_lo);
+        if (P.pos_lo) A.plo[i] = lo;
         if (P.pcib) {
             /* correctPositions (PCISPH branch, :226-262): candidates of the new
                cell if the last search listed it, weights at the predicted
@@ -1155,7 +1163,8 @@ __global__ void __launch_bounds__(256) k_cube_correct(SimParams P, DeviceArrays 
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= active_n(P, A.st)) return;
-    float4 x = A.pos[i], v = A.vel[i];
+    const float4 x0 = A.pos[i];
+    float4 x = x0, v = A.vel[i];
     for (int c = 0; c < ncubes; ++c) {
         const CubeBox b = cubes[c];
         cube_axis(x.x, v.x, v.y, v.z, b.minx, b.maxx, b.normal_fct, b.tangential_fct);
@@ -1164,6 +1173,14 @@ __global__ void __launch_bounds__(256) k_cube_correct(SimParams P, DeviceArrays 
     }
     A.pos[i] = x;
     A.vel[i] = v;
+    if (P.pos_lo && (x.x != x0.x || x.y != x0.y || x.z != x0.z)) {
+        /* a clamped coordinate sits exactly on the face */
+        float4 lo = A.plo[i];
+        if (x.x != x0.x) lo.x = 0.0f;
+        if (x.y != x0.y) lo.y = 0.0f;
+        if (x.z != x0.z) lo.z = 0.0f;
+        A.plo[i] = lo;
+    }
 }
 
 void launch_cube_correct(const SimParams& P, const DeviceArrays& A, const CubeBox* cubes, int ncubes, cudaStream_t s)
@@ -1234,6 +1251,7 @@ __global__ void __launch_bounds__(256) k_emit(SimParams P, DeviceArrays A, Emitt
                 quat_rotate(em, px, py, pz, rx, ry, rz);
                 const unsigned slot = s_n + k;
                 A.pos[slot] = make_float4(__fadd_rn(rx, em.px), __fadd_rn(ry, em.py), __fadd_rn(rz, em.pz), 0.0f);
+                if (P.pos_lo) A.plo[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 A.vel[slot] = make_float4(rvx, rvy, rvz, 0.0f);
                 A.acc[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 A.orig_w[slot] = slot;
