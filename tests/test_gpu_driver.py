@@ -80,3 +80,48 @@ def test_bad_scene_fails_cleanly(tmp_path):
     p.write_text('{"Configuration": {}}')
     r = subprocess.run([DRIVER, "-c", str(p), "-g", "false"], capture_output=True, text=True, timeout=60)
     assert r.returncode != 0 and "Cannot import scene" in r.stderr
+
+
+def last_frame_matches_api(tmp_path, scene_dict, api_scene):
+    """Runs the driver on scene_dict (written beside its OBJ meshes) and
+    checks its last frame against the API stepped to the same time."""
+    out, summary = run("-c", tmp_path / "scene.json", "-g", "false", "-o", "true")
+    frames = sorted(f for f in os.listdir(tmp_path) if f.startswith("scene_") and f.endswith(".json"))
+    assert len(frames) == summary["frames"] >= 2
+    last = json.loads((tmp_path / frames[-1]).read_text())
+    sim = Simulation.from_scene(Scene.from_dict(api_scene))
+    for _ in range(summary["steps"]):
+        sim.step(1)
+        t, _ = sim.time()
+        if abs(t - last["time"]) < 1e-12:
+            break
+    assert abs(t - last["time"]) < 1e-12
+    x, v, _ = sim.state()
+    sim.close()
+    assert np.array_equal(np.asarray(last["positions"], np.float32), x)
+    assert np.array_equal(np.asarray(last["velocities"], np.float32), v)
+
+
+def test_driver_geometry_scene_relative_mesh_path(tmp_path):
+    """An OBJ geometry given by a path relative to the scene file."""
+    import shutil
+
+    from conftest import GOLDEN, load_golden
+
+    g = load_golden("geometry_dfsph_cup")
+    sc = json.loads(json.dumps(g["scene"]))
+    sc["Configuration"]["endTime"] = 0.004
+    sc["Configuration"]["fps"] = 1000.0
+    api_scene = json.loads(json.dumps(sc))
+    sc["Boundary"][0]["geometry"][0]["path"] = "cup.obj"
+    shutil.copy(os.path.join(GOLDEN, "cup.obj"), tmp_path / "cup.obj")
+    (tmp_path / "scene.json").write_text(json.dumps(sc))
+    last_frame_matches_api(tmp_path, sc, api_scene)
+
+
+def test_driver_pcisph_boundary_scene(tmp_path):
+    sc = S.pcisph_boundary_scenes()["pcib_wcsph_sphere"]
+    sc["Configuration"]["endTime"] = 0.004
+    sc["Configuration"]["fps"] = 1000.0
+    (tmp_path / "scene.json").write_text(json.dumps(sc))
+    last_frame_matches_api(tmp_path, sc, sc)
