@@ -72,6 +72,9 @@ struct DeviceArrays {
        integration target */
     float4* plo;
     float4* plo_alt;
+    /* DFSPH: divergence error of the density pass (NULL: the divergence
+       solver computes its warm-start residual itself) */
+    float* divres;
 };
 
 /* sph_grid.cu */

@@ -175,23 +175,34 @@ __device__ __forceinline__ float boundary_density(const SimParams& P, const Devi
 
 /* ---------------------------------------------------------------------- */
 
-template <bool ALPHA, bool EOS>
+/* DIVRES: also the divergence error of the current velocities
+   (DFSPHSolver::computeDivergenceError, DFSPHSolver.cpp:538-621), which the
+   divergence solver's warm start reads (A.divres) instead of spending a
+   neighbour pass on it: the velocities do not change between this pass
+   and that solver. */
+template <bool ALPHA, bool EOS, bool DIVRES = false>
 __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= active_n(P, A.st)) return;
     const size_t nf = (size_t)P.nf;
     const float4 xi = A.pos[i];
-    float rho = 0.0f, sgx = 0.0f, sgy = 0.0f, sgz = 0.0f, ssq = 0.0f;
+    const float4 vi = DIVRES ? A.vel[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float rho = 0.0f, sgx = 0.0f, sgy = 0.0f, sgz = 0.0f, ssq = 0.0f, div = 0.0f;
     const unsigned nF = A.cnt_f[i];
-    for_fluid_neighbors<2>(A, i, nf, nF, [&](unsigned, const float4& xj) {
+    for_fluid_neighbors<2>(A, i, nf, nF, [&](unsigned j, const float4& xj) {
         rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(dist2_exact(xi, xj), P)));
         if (ALPHA) {
             const Pair p = make_pair(xi, xj);
-            const float f = P.mass * cs_gradf(p.rl, p.inv_rl, P);
+            const float fg = cs_gradf(p.rl, p.inv_rl, P);
+            const float f = P.mass * fg;
             const float gx = f * p.rx, gy = f * p.ry, gz = f * p.rz;
             sgx += gx; sgy += gy; sgz += gz;
             ssq += (gx * gx + gy * gy) + gz * gz;
+            if (DIVRES) {
+                const float4 vj = A.vel[j];
+                div += P.mass * (fg * (((vi.x - vj.x) * p.rx + (vi.y - vj.y) * p.ry) + (vi.z - vj.z) * p.rz));
+            }
         }
     });
     const unsigned nB = A.cnt_b[i];
@@ -200,8 +211,10 @@ __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
         rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(dist2_exact(xi, xb), P)));
         if (ALPHA) {
             const Pair p = make_pair(xi, xb);
-            const float f = xb.w * cs_gradf(p.rl, p.inv_rl, P);
+            const float fg = cs_gradf(p.rl, p.inv_rl, P);
+            const float f = xb.w * fg;
             sgx += f * p.rx; sgy += f * p.ry; sgz += f * p.rz;
+            if (DIVRES) div += xb.w * (fg * ((vi.x * p.rx + vi.y * p.ry) + vi.z * p.rz));
         }
     }
     A.rho[i] = rho;
@@ -210,6 +223,8 @@ __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
         A.alpha[i] = denom > P.eps ? rho / denom : 0.0f;
     }
     if (EOS) A.press[i] = tait_pressure(rho, P, P.kr_g);
+    /* fewer than 20 neighbours within h: no correction (DFSPHSolver.cpp:608-611) */
+    if (DIVRES) A.divres[i] = (nF + nB < 20u) ? 0.0f : fmaxf(div, 0.0f);
 }
 
 __global__ void __launch_bounds__(256, 8) k_normals(SimParams P, DeviceArrays A)
@@ -643,7 +658,9 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
     /* warm start: residual at the current velocities, keep the previous
        step's accumulated k only where the residual is positive */
     for_particles<TPP>(nfi, [&](int i, int sub, bool valid) {
-        const float r = dfsph_residual_lanes<DIV, TPP, U>(P, A, i, sub, valid, nf, dt);
+        /* the divergence error may come from the density pass (A.divres) */
+        const float r = (DIV && A.divres) ? (valid ? A.divres[i] : 0.0f)
+                                          : dfsph_residual_lanes<DIV, TPP, U>(P, A, i, sub, valid, nf, dt);
         if (valid && sub == 0) {
             if (DIV) kws[i] = r > 0.0f ? kws[i] / dt : 0.0f;
             else kws[i] = r > P.rho0 ? kws[i] / ts2 : 0.0f;
@@ -1304,6 +1321,7 @@ void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool 
     if (P.nf <= 0) return;
     const int g = blocks_for(P.nf, block);
     if (alpha && eos) k_density<true, true><<<g, block, 0, s>>>(P, A);
+    else if (alpha && A.divres) k_density<true, false, true><<<g, block, 0, s>>>(P, A);
     else if (alpha) k_density<true, false><<<g, block, 0, s>>>(P, A);
     else if (eos) k_density<false, true><<<g, block, 0, s>>>(P, A);
     else k_density<false, false><<<g, block, 0, s>>>(P, A);
