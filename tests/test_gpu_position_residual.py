@@ -58,3 +58,24 @@ def test_option_is_set_before_init_and_for_single_scenes():
     with pytest.raises(SphError):  # the adjoint differentiates FP32 positions
         sim.wcsph_forward(2, x)
     sim.close()
+
+
+@pytest.mark.parametrize("name", ["emitter_wcsph_square", "emitter_dfsph_circle", "cube_wcsph_outside",
+                                  "pcib_dfsph_sphere"])
+def test_residual_with_emitters_cubes_and_pcisph_boundaries(name):
+    """Emitted particles start without a residual, cube clamps zero the
+    clamped coordinates', PCISPH-boundary pushes leave it: the runs stay
+    finite, emit the same particles and end within the reference's own
+    FP32-to-FP64 spread of the plain run."""
+    g = load_golden(name)
+    runs = []
+    for residual in (0, 1):
+        sim = Simulation.from_scene(Scene.from_dict(g["scene"]), options={api.OPT_POSITION_RESIDUAL: residual})
+        sim.step(g["trace_f32"].shape[0])
+        runs.append((sim.state(), sim.num_active()))
+        sim.close()
+    (x0, v0, _), n0 = runs[0]
+    (x1, v1, _), n1 = runs[1]
+    assert n0 == n1 and np.all(np.isfinite(x1[:n1])) and np.all(np.isfinite(v1[:n1]))
+    spread = float(np.abs(g["final_pos_f32"] - g["final_pos_f64"]).max())
+    assert float(np.abs(x1[:n1] - x0[:n0]).max()) <= 2.0 * spread + 1e-6
