@@ -122,7 +122,7 @@ struct sph_ctx {
     int pos_lo = 0;
     float4 *plo = nullptr, *plo2 = nullptr;
     float4* snap_plo = nullptr;
-    float* divres = nullptr;  /* single DFSPH scene: divergence error of the density pass */
+    float* divres = nullptr;  /* DFSPH: divergence error of the density pass */
     /* autotune snapshot */
     float4 *snap_pos = nullptr, *snap_vel = nullptr;
     unsigned* snap_orig = nullptr;
@@ -1052,8 +1052,7 @@ int sph_init(sph_ctx* c)
     c->orig_base = c->orig;
     c->kws_base = c->kws;
     if ((rc = alloc_lists(c)) != SPH_OK) return rc;
-    if (c->desc.simulation_method == SPH_DFSPH && !c->nscenes && (rc = dalloc(c, &c->divres, nf)) != SPH_OK)
-        return rc;
+    if (c->desc.simulation_method == SPH_DFSPH && (rc = dalloc(c, &c->divres, nf)) != SPH_OK) return rc;
     if (c->pos_lo) {
         if (c->nscenes) return fail(c, SPH_ERR_ARG, "position residuals apply to single scenes, not to batches");
         if ((rc = dalloc(c, &c->plo, nf)) != SPH_OK) return rc;

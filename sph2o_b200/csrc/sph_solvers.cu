@@ -815,7 +815,8 @@ __global__ void __launch_bounds__(kSolverBlock, 8) k_dfsph_solve_batch(SimParams
     float* kws = DIV ? A.kvws : A.kws;
     for (int i = tid; i < nfi; i += nthr) {
         const float dt = sst[so[i]].dt_next;
-        const float r = dfsph_residual<DIV>(P, A, i, nf, dt);
+        /* the divergence error may come from the density pass (A.divres) */
+        const float r = (DIV && A.divres) ? A.divres[i] : dfsph_residual<DIV>(P, A, i, nf, dt);
         if (DIV) kws[i] = r > 0.0f ? kws[i] / dt : 0.0f;
         else kws[i] = r > P.rho0 ? kws[i] / (dt * dt) : 0.0f;
     }
