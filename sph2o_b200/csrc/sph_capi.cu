@@ -261,6 +261,7 @@ void derive_params(sph_ctx* c)
     P.gamma = d.gamma;
     P.kr_g = d.gamma != 0.0f ? d.stiffness * d.density0 / d.gamma : 0.0f;
     P.h2_guard = (float)((double)h * (double)h * (1.0 + 1.0e-5));
+    P.h2_exact = sqrt_le_bound(h);
     P.eta = d.eta;
     P.eta_v = d.eta_v;
     P.cfl = d.cfl_factor;

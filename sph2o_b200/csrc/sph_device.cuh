@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
+
 namespace sph {
 
 /* error bits in DevState::err */
@@ -42,6 +44,7 @@ struct SimParams {
     float stiffness, gamma;
     float kr_g;         /* (stiffness * rho0) / gamma, WCSPHSolver.cpp:93            */
     float h2_guard;     /* h^2 (1 + 1e-5): exact-W candidates above it are 0 anyway  */
+    float h2_exact;     /* sqrt_le_bound(h): s <= h2_exact exactly when sqrt_rn(s) <= h */
     float eta, eta_v, cfl, min_ts, max_ts;
     unsigned min_it, max_it, min_it_v, max_it_v;
     float pcisph_delta;
@@ -380,12 +383,17 @@ __device__ __forceinline__ Grid grid_for(const SimParams& P, const SceneRef& S, 
     return S.scenes ? S.scenes[S.scene_of[slot]].grid : grid_single(P);
 }
 
-/* exact |xi - xj| <= h test of the reference (glm::length: sqrt((dx dx + dy dy) + dz dz)) */
-__device__ __forceinline__ bool within_h_exact(float4 a, float4 b, float h)
+/* Largest float s with sqrt_rn(s) <= h. The correctly rounded square root
+   is monotonic, so the reference's neighbour test glm::length(r) <= h,
+   sqrt_rn((dx dx + dy dy) + dz dz) <= h, holds exactly when that rounded
+   sum is <= this bound (NaN and infinity fail both forms). The host's
+   sqrtf is the IEEE correctly rounded one, as __fsqrt_rn is. */
+static inline float sqrt_le_bound(float h)
 {
-    const float dx = __fsub_rn(a.x, b.x), dy = __fsub_rn(a.y, b.y), dz = __fsub_rn(a.z, b.z);
-    const float s = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-    return __fsqrt_rn(s) <= h;
+    float s = h * h;
+    while (s > 0.0f && std::sqrt(s) > h) s = std::nextafter(s, 0.0f);
+    while (std::sqrt(std::nextafter(s, INFINITY)) <= h) s = std::nextafter(s, INFINITY);
+    return s;
 }
 
 /* Entry kk of sorted particle i's neighbour list (column-major). The lists

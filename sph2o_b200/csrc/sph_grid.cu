@@ -168,17 +168,13 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
     if (i >= active_n(P, st)) return;
     const float4 xi = pos[i];
     const size_t nf = (size_t)P.nf;
-    /* a cheap float test settles clear cases; candidates within a relative
-       1e-5 band of h take the exact IEEE test that defines the set */
-    const float lo2 = P.h2 * (1.0f - 1.0e-5f), hi2 = P.h2 * (1.0f + 1.0e-5f);
+    /* |r| <= h as the reference rounds it, without the square root */
+    const float s2max = P.h2_exact;
     unsigned nF = 0, nB = 0;
     for_cells27(xi, P.h, grid_for(P, S, (unsigned)i), [&](unsigned c) {
         const unsigned s = cell_start[c], e = cell_start[c + 1];
         for (unsigned q = s; q < e; ++q) {
-            const float4 xq = pos[q];
-            const float dx = xi.x - xq.x, dy = xi.y - xq.y, dz = xi.z - xq.z;
-            const float d2 = dx * dx + dy * dy + dz * dz;
-            if (d2 < lo2 || (d2 <= hi2 && within_h_exact(xi, xq, P.h))) {
+            if (dist2_exact(xi, pos[q]) <= s2max) {
                 if (nF < P.capF) __stcs(nbr_f + (size_t)nF * nf + i, q);
                 ++nF;
             }
@@ -186,10 +182,7 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
         if (P.nb > 0) {
             const unsigned bs = bcell_start[c], be = bcell_start[c + 1];
             for (unsigned q = bs; q < be; ++q) {
-                const float4 xb = bpos[q];
-                const float dx = xi.x - xb.x, dy = xi.y - xb.y, dz = xi.z - xb.z;
-                const float d2 = dx * dx + dy * dy + dz * dz;
-                if (d2 < lo2 || (d2 <= hi2 && within_h_exact(xi, xb, P.h))) {
+                if (dist2_exact(xi, bpos[q]) <= s2max) {
                     if (nB < P.capB) __stcs(nbr_b + (size_t)nB * nf + i, q);
                     ++nB;
                 }

@@ -159,6 +159,7 @@ extern "C" int sph_density_noalloc(float particle_radius, float density0, const 
     P.h = 4.0f * particle_radius;
     P.h2 = P.h * P.h;
     P.h2_guard = (float)((double)P.h * (double)P.h * (1.0 + 1.0e-5));
+    P.h2_exact = sqrt_le_bound(P.h);
     P.inv_h = 1.0f / P.h;
     P.rho0 = density0;
     const float diameter = 2.0f * particle_radius;
