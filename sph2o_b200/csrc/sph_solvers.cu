@@ -558,9 +558,14 @@ __device__ __forceinline__ float lane_group_sum(float v)
 }
 
 /* Calls f(i, sub, valid) for every particle i < n, TPP adjacent lanes per
-   particle (sub = lane index within the group), 32 / TPP particles per warp,
-   warps striding over the grid. The trip count is uniform per warp, so f may
-   use warp shuffles; lanes past the end get valid = false. */
+   particle (sub = lane index within the group), up to 32 / TPP particles per
+   warp and round. In each full round the warps take consecutive groups of
+   32 / TPP particles, so at any moment the whole grid works on one stretch
+   of the cell-ordered arrays (whose state and lists then stay in L2); the
+   particles left over for the last round are spread evenly over all warps,
+   so that no warp sits out the last round while others run a full group.
+   The trip count is uniform per warp, so f may use warp shuffles; lanes
+   without a particle get valid = false. */
 template <int TPP, typename F>
 __device__ __forceinline__ void for_particles(int n, F&& f)
 {
@@ -568,9 +573,15 @@ __device__ __forceinline__ void for_particles(int n, F&& f)
     const int lane = threadIdx.x & 31;
     const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int nw = (int)((gridDim.x * blockDim.x) >> 5);
-    for (int base = gw * PPW; base < n; base += nw * PPW) {
-        const int i = base + lane / TPP;
-        f(i, lane % TPP, i < n);
+    const int per_round = nw * PPW;
+    const int full = n / per_round;
+    for (int r = 0; r < full; ++r) f(r * per_round + gw * PPW + lane / TPP, lane % TPP, true);
+    const int base = full * per_round, rem = n - base;
+    if (rem > 0) {
+        const int lo = base + (int)(((long long)rem * gw) / nw);
+        const int hi = base + (int)(((long long)rem * (gw + 1)) / nw);
+        const int i = lo + lane / TPP;
+        f(i, lane % TPP, i < hi);
     }
 }
 
