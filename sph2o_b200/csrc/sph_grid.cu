@@ -155,7 +155,14 @@ __global__ void __launch_bounds__(256) k_ns_rank_gather(int n, const unsigned* _
     if (g.f_in[1]) g.f_out[1][dst] = g.f_in[1][src];
 }
 
-/* Neighbour lists in the reference's candidate order, filtered at |r| <= h. */
+/* Neighbour lists in the reference's candidate order, filtered at |r| <= h.
+   TPP adjacent lanes share a particle: they test a cell's candidates TPP at
+   a time (lane sub takes q = s + sub, s + sub + TPP, ...), and a ballot over
+   the group ranks the accepted ones, so entries are written in candidate
+   order whatever TPP is. TPP = 1 is one lane per particle (large scenes, where
+   particles already fill the GPU); more lanes shorten each particle's serial
+   candidate walk when there are few particles. */
+template <int TPP>
 __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S, const float4* __restrict__ pos,
                                                         const unsigned* __restrict__ cell_start,
                                                         const float4* __restrict__ bpos,
@@ -164,8 +171,13 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
                                                         unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b,
                                                         DevState* st)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / TPP;
+    /* a group's lanes share i, so a group leaves together */
     if (i >= active_n(P, st)) return;
+    const unsigned lane = threadIdx.x & 31u, sub = lane % TPP;
+    const unsigned gmask = TPP == 32 ? 0xffffffffu : ((1u << TPP) - 1u) << (lane - sub);
+    const unsigned below = (1u << sub) - 1u;
     const float4 xi = pos[i];
     const size_t nf = (size_t)P.nf;
     /* |r| <= h as the reference rounds it, without the square root */
@@ -173,22 +185,49 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
     unsigned nF = 0, nB = 0;
     for_cells27(xi, P.h, grid_for(P, S, (unsigned)i), [&](unsigned c) {
         const unsigned s = cell_start[c], e = cell_start[c + 1];
-        for (unsigned q = s; q < e; ++q) {
-            if (dist2_exact(xi, pos[q]) <= s2max) {
-                if (nF < P.capF) __stcs(nbr_f + (size_t)nF * nf + i, q);
-                ++nF;
+        if (TPP == 1) {
+            for (unsigned q = s; q < e; ++q) {
+                if (dist2_exact(xi, pos[q]) <= s2max) {
+                    if (nF < P.capF) __stcs(nbr_f + (size_t)nF * nf + i, q);
+                    ++nF;
+                }
+            }
+        } else {
+            for (unsigned q0 = s; q0 < e; q0 += TPP) {
+                const unsigned q = q0 + sub;
+                const bool in = q < e && dist2_exact(xi, pos[q]) <= s2max;
+                const unsigned bits = __ballot_sync(gmask, in) >> (lane - sub);
+                if (in) {
+                    const unsigned k = nF + __popc(bits & below);
+                    if (k < P.capF) __stcs(nbr_f + (size_t)k * nf + i, q);
+                }
+                nF += __popc(bits);
             }
         }
         if (P.nb > 0) {
             const unsigned bs = bcell_start[c], be = bcell_start[c + 1];
-            for (unsigned q = bs; q < be; ++q) {
-                if (dist2_exact(xi, bpos[q]) <= s2max) {
-                    if (nB < P.capB) __stcs(nbr_b + (size_t)nB * nf + i, q);
-                    ++nB;
+            if (TPP == 1) {
+                for (unsigned q = bs; q < be; ++q) {
+                    if (dist2_exact(xi, bpos[q]) <= s2max) {
+                        if (nB < P.capB) __stcs(nbr_b + (size_t)nB * nf + i, q);
+                        ++nB;
+                    }
+                }
+            } else {
+                for (unsigned q0 = bs; q0 < be; q0 += TPP) {
+                    const unsigned q = q0 + sub;
+                    const bool in = q < be && dist2_exact(xi, bpos[q]) <= s2max;
+                    const unsigned bits = __ballot_sync(gmask, in) >> (lane - sub);
+                    if (in) {
+                        const unsigned k = nB + __popc(bits & below);
+                        if (k < P.capB) __stcs(nbr_b + (size_t)k * nf + i, q);
+                    }
+                    nB += __popc(bits);
                 }
             }
         }
     });
+    if (sub != 0) return;
     cnt_f[i] = min(nF, P.capF);
     cnt_b[i] = min(nB, P.capB);
     if (nF > P.capF || nB > P.capB) {
@@ -295,8 +334,21 @@ void launch_build_lists(const SimParams& P, const SceneRef& S, const float4* pos
                         unsigned* cnt_b, DevState* st, cudaStream_t s)
 {
     if (P.nf <= 0) return;
-    k_ns_build_lists<<<blocks_for(P.nf, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f,
-                                                            nbr_b, cnt_b, st);
+    /* lanes per particle: enough threads to fill the GPU (148 SMs x 2048) */
+    const int tpp = P.nf >= (1 << 19) ? 1 : P.nf >= (1 << 17) ? 2 : P.nf >= (1 << 15) ? 4 : 8;
+    const long long nt = (long long)P.nf * tpp;
+    if (tpp == 1)
+        k_ns_build_lists<1><<<blocks_for(nt, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
+                                                                 cnt_f, nbr_b, cnt_b, st);
+    else if (tpp == 2)
+        k_ns_build_lists<2><<<blocks_for(nt, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
+                                                                 cnt_f, nbr_b, cnt_b, st);
+    else if (tpp == 4)
+        k_ns_build_lists<4><<<blocks_for(nt, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
+                                                                 cnt_f, nbr_b, cnt_b, st);
+    else
+        k_ns_build_lists<8><<<blocks_for(nt, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
+                                                                 cnt_f, nbr_b, cnt_b, st);
 }
 
 void launch_boundary_volume(const SimParams& P, const SceneRef& S, float4* bpos, const unsigned* bcell_start,
