@@ -68,6 +68,21 @@ __device__ __forceinline__ void pair_of(float4 a, float4 b, float& rx, float& ry
     len_inv(s, rl, inv_rl);
 }
 
+/* Sum over the TPP adjacent lanes of a group (gmask: the group's lanes). */
+template <int TPP>
+__device__ __forceinline__ float group_sum(float v, unsigned gmask)
+{
+    for (int o = TPP / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
+    return v;
+}
+
+template <int TPP>
+__device__ __forceinline__ unsigned group_mask()
+{
+    const unsigned lane = threadIdx.x & 31u;
+    return TPP == 32 ? 0xffffffffu : ((1u << TPP) - 1u) << (lane - lane % TPP);
+}
+
 /* Loss L = (1/N) sum_i |x_i - t_i|^2 of the current (sorted) positions
    against the caller-order target; seeds xbar = 2 (x - t) / N, vbar = 0. */
 __global__ void __launch_bounds__(256) k_adj_seed(int n, const float4* __restrict__ pos,
@@ -108,13 +123,21 @@ __global__ void __launch_bounds__(256) k_adj_load(SimParams P, AdjointArrays J)
     J.Ap[i] = J.press[i] / (r * r);
 }
 
-/* Adjoint of the pressure and viscosity accelerations (and of the EOS). */
+/* Adjoint of the pressure and viscosity accelerations (and of the EOS).
+   TPP adjacent lanes share particle i, each summing the list entries
+   sub, sub + TPP, ...; the group's partial sums are then added by shuffles
+   in a fixed order, so results are reproducible run to run. */
+template <int TPP>
 __global__ void __launch_bounds__(256, 4) k_adj_forces(SimParams P, AdjointArrays J)
 {
     __shared__ double s_red[32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / TPP;
+    const unsigned sub = (unsigned)t % TPP;
     const size_t nf = (size_t)P.nf;
     double kbar = 0.0, nubar = 0.0;
+    float sA = 0.0f, sB = 0.0f, rv = 0.0f, sbv = 0.0f, nup = 0.0f;
+    float xrx = 0.0f, xry = 0.0f, xrz = 0.0f, vrx = 0.0f, vry = 0.0f, vrz = 0.0f;
     if (i < P.nf) {
         const float4 xi = J.pos[i];
         const float4 vi = J.vel[i];
@@ -128,10 +151,8 @@ __global__ void __launch_bounds__(256, 4) k_adj_forces(SimParams P, AdjointArray
         const float nu = P.visc, nub = P.bvisc;
         const float eps_h2 = 0.01f * P.h2;
         const float inv_rho_i = 1.0f / rho_i;
-        float sA = 0.0f, sB = 0.0f, rv = 0.0f, sbv = 0.0f, nup = 0.0f;
-        float xrx = 0.0f, xry = 0.0f, xrz = 0.0f, vrx = 0.0f, vry = 0.0f, vrz = 0.0f;
         const unsigned nF = J.cnt_f[i];
-        for (unsigned kk = 0; kk < nF; ++kk) {
+        for (unsigned kk = sub; kk < nF; kk += TPP) {
             const unsigned j = list_at(J.nbr_f, kk, nf, i);
             const float4 xj = J.pos[j];
             float rx, ry, rz, s, rl, inv_rl, f, g;
@@ -174,7 +195,7 @@ __global__ void __launch_bounds__(256, 4) k_adj_forces(SimParams P, AdjointArray
             }
         }
         const unsigned nB = J.cnt_b[i];
-        for (unsigned kk = 0; kk < nB; ++kk) {
+        for (unsigned kk = sub; kk < nB; kk += TPP) {
             const float4 xb = J.bpos[list_at(J.nbr_b, kk, nf, i)];
             float rx, ry, rz, s, rl, inv_rl, f, g;
             pair_of(xi, xb, rx, ry, rz, s, rl, inv_rl);
@@ -207,6 +228,20 @@ __global__ void __launch_bounds__(256, 4) k_adj_forces(SimParams P, AdjointArray
                 sbv += psi * phi * f * rai;
             }
         }
+        if (TPP > 1) {
+            const unsigned gm = group_mask<TPP>();
+            sA = group_sum<TPP>(sA, gm); sB = group_sum<TPP>(sB, gm);
+            rv = group_sum<TPP>(rv, gm); sbv = group_sum<TPP>(sbv, gm); nup = group_sum<TPP>(nup, gm);
+            xrx = group_sum<TPP>(xrx, gm); xry = group_sum<TPP>(xry, gm); xrz = group_sum<TPP>(xrz, gm);
+            vrx = group_sum<TPP>(vrx, gm); vry = group_sum<TPP>(vry, gm); vrz = group_sum<TPP>(vrz, gm);
+        }
+    }
+    if (i < P.nf && sub == 0) {
+        const float rho_i = J.rho[i], p_i = J.press[i];
+        const float inv_rho_i = 1.0f / rho_i;
+        const float m = P.mass;
+        const bool visc = P.visc_method == 1;
+        const float nu = P.visc, nub = P.bvisc;
         /* EOS: p = max(0, kr_g (ratio^gamma - 1)), kr_g = k rho0 / gamma */
         const float pbar = sA * inv_rho_i * inv_rho_i + sB / (P.rho0 * P.rho0);
         float dpdrho = 0.0f;
@@ -249,16 +284,20 @@ __global__ void __launch_bounds__(256) k_adj_finish(int nblocks, const double* _
 }
 
 /* Adjoint of the density sum; writes the step's input adjoint in caller order. */
+template <int TPP>
 __global__ void __launch_bounds__(256, 6) k_adj_density(SimParams P, AdjointArrays J)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / TPP;
+    const unsigned sub = (unsigned)t % TPP;
+    /* a group's lanes share i, so a group leaves together */
     if (i >= P.nf) return;
     const size_t nf = (size_t)P.nf;
     const float4 xi = J.pos[i];
     const float rbi = J.rhobar[i];
     float sx = 0.0f, sy = 0.0f, sz = 0.0f;
     const unsigned nF = J.cnt_f[i];
-    for (unsigned kk = 0; kk < nF; ++kk) {
+    for (unsigned kk = sub; kk < nF; kk += TPP) {
         const unsigned j = list_at(J.nbr_f, kk, nf, i);
         float rx, ry, rz, s, rl, inv_rl;
         pair_of(xi, J.pos[j], rx, ry, rz, s, rl, inv_rl);
@@ -268,12 +307,17 @@ __global__ void __launch_bounds__(256, 6) k_adj_density(SimParams P, AdjointArra
         sx += c * rx; sy += c * ry; sz += c * rz;
     }
     const unsigned nB = J.cnt_b[i];
-    for (unsigned kk = 0; kk < nB; ++kk) {
+    for (unsigned kk = sub; kk < nB; kk += TPP) {
         const float4 xb = J.bpos[list_at(J.nbr_b, kk, nf, i)];
         float rx, ry, rz, s, rl, inv_rl;
         pair_of(xi, xb, rx, ry, rz, s, rl, inv_rl);
         const float c = xb.w * rbi * cs_gradf(rl, inv_rl, P);
         sx += c * rx; sy += c * ry; sz += c * rz;
+    }
+    if (TPP > 1) {
+        const unsigned gm = group_mask<TPP>();
+        sx = group_sum<TPP>(sx, gm); sy = group_sum<TPP>(sy, gm); sz = group_sum<TPP>(sz, gm);
+        if (sub != 0) return;
     }
     const unsigned o = J.orig[i];
     const float4 xa = J.xacc[i];
@@ -293,7 +337,10 @@ __global__ void k_adj_unpack(int n, const float4* __restrict__ in, float* __rest
 
 static inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
 
-int adjoint_blocks(int n) { return blocks_for(n, 256); }
+/* lanes per particle of the adjoint passes: enough threads to fill the GPU */
+static inline int adjoint_tpp(int n) { return n >= (1 << 19) ? 1 : n >= (1 << 17) ? 2 : n >= (1 << 15) ? 4 : 8; }
+
+int adjoint_blocks(int n) { return blocks_for(n * adjoint_tpp(n), 256); }
 
 void launch_adjoint_seed(int n, const float4* pos, const unsigned* orig, const float* target, float4* xbar,
                          float4* vbar, double* part, cudaStream_t s)
@@ -304,16 +351,20 @@ void launch_adjoint_seed(int n, const float4* pos, const unsigned* orig, const f
 
 void launch_adjoint_finish(int n, const double* part, double* red, cudaStream_t s)
 {
-    k_adj_finish<<<1, 256, 0, s>>>(blocks_for(n, 256), part, red);
+    k_adj_finish<<<1, 256, 0, s>>>(adjoint_blocks(n), part, red);
 }
 
 void launch_adjoint_step(const SimParams& P, const AdjointArrays& J, cudaStream_t s)
 {
     if (P.nf <= 0) return;
-    const int g = blocks_for(P.nf, 256);
-    k_adj_load<<<g, 256, 0, s>>>(P, J);
-    k_adj_forces<<<g, 256, 0, s>>>(P, J);
-    k_adj_density<<<g, 256, 0, s>>>(P, J);
+    k_adj_load<<<blocks_for(P.nf, 256), 256, 0, s>>>(P, J);
+    const int g = adjoint_blocks(P.nf);
+    switch (adjoint_tpp(P.nf)) {
+    case 1: k_adj_forces<1><<<g, 256, 0, s>>>(P, J); k_adj_density<1><<<g, 256, 0, s>>>(P, J); break;
+    case 2: k_adj_forces<2><<<g, 256, 0, s>>>(P, J); k_adj_density<2><<<g, 256, 0, s>>>(P, J); break;
+    case 4: k_adj_forces<4><<<g, 256, 0, s>>>(P, J); k_adj_density<4><<<g, 256, 0, s>>>(P, J); break;
+    default: k_adj_forces<8><<<g, 256, 0, s>>>(P, J); k_adj_density<8><<<g, 256, 0, s>>>(P, J); break;
+    }
 }
 
 void launch_adjoint_unpack(int n, const float4* in, float* out3, cudaStream_t s)
