@@ -57,25 +57,37 @@ __device__ __forceinline__ Pair make_pair(float4 a, float4 b)
 /* Calls f(j, x_j) for the fluid neighbours of sorted particle i in list
    order, issuing the list loads and position gathers of U entries before the
    first of them is used (more loads in flight per thread; same order, so the
-   sums it feeds are unchanged). */
-template <int U, typename F>
-__device__ __forceinline__ void for_fluid_neighbors(const DeviceArrays& A, int i, size_t nf, unsigned n, F&& f)
+   sums it feeds are unchanged). With TPP lanes per particle, lane sub visits
+   the entries sub, sub + TPP, ... */
+template <int U, int TPP = 1, typename F>
+__device__ __forceinline__ void for_fluid_neighbors(const DeviceArrays& A, int i, size_t nf, unsigned n, F&& f,
+                                                    unsigned sub = 0)
 {
-    unsigned kk = 0;
-    for (; kk + U <= n; kk += U) {
+    unsigned kk = sub;
+    for (; kk + (U - 1) * TPP < n; kk += U * TPP) {
         unsigned jj[U];
         float4 xj[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) jj[u] = list_at(A.nbr_f, kk + u, nf, i);
+        for (int u = 0; u < U; ++u) jj[u] = list_at(A.nbr_f, kk + u * TPP, nf, i);
 #pragma unroll
         for (int u = 0; u < U; ++u) xj[u] = A.pos[jj[u]];
 #pragma unroll
         for (int u = 0; u < U; ++u) f(jj[u], xj[u]);
     }
-    for (; kk < n; ++kk) {
+    for (; kk < n; kk += TPP) {
         const unsigned j = list_at(A.nbr_f, kk, nf, i);
         f(j, A.pos[j]);
     }
+}
+
+/* Sum over the TPP adjacent lanes of a particle's lane group. */
+template <int TPP>
+__device__ __forceinline__ float group_sum(float v)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned gmask = TPP == 32 ? 0xffffffffu : ((1u << TPP) - 1u) << (lane - lane % TPP);
+    for (int o = TPP / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
+    return v;
 }
 
 /* ---------------------------------------------------------------------- */
@@ -227,6 +239,47 @@ __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
     if (DIVRES) A.divres[i] = (nF + nB < 20u) ? 0.0f : fmaxf(div, 0.0f);
 }
 
+/* Density (and the Tait pressure when EOS) of small scenes with TPP lanes per
+   particle: in each round the group's lanes evaluate m W for TPP consecutive
+   list entries, and lane 0 adds the TPP terms in list order (shuffled to
+   it), so the sum is the sequential one bit for bit; the terms of entries
+   past the end are +0, which leaves a non-negative sum unchanged. */
+template <bool EOS, int TPP>
+__global__ void __launch_bounds__(256) k_density_lanes(SimParams P, DeviceArrays A)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / TPP;
+    /* a group's lanes share i, so a group leaves together */
+    if (i >= active_n(P, A.st)) return;
+    const unsigned lane = threadIdx.x & 31u, sub = lane % TPP, first = lane - sub;
+    const unsigned gmask = ((1u << TPP) - 1u) << first;
+    const size_t nf = (size_t)P.nf;
+    const float4 xi = A.pos[i];
+    float rho = 0.0f;
+    const unsigned nF = A.cnt_f[i];
+    for (unsigned k0 = 0; k0 < nF; k0 += TPP) {
+        const unsigned kk = k0 + sub;
+        float w = 0.0f;
+        if (kk < nF) w = __fmul_rn(P.mass, cs_W_exact(dist2_exact(xi, A.pos[list_at(A.nbr_f, kk, nf, i)]), P));
+#pragma unroll
+        for (int l = 0; l < TPP; ++l) rho = __fadd_rn(rho, __shfl_sync(gmask, w, first + l));
+    }
+    const unsigned nB = A.cnt_b[i];
+    for (unsigned k0 = 0; k0 < nB; k0 += TPP) {
+        const unsigned kk = k0 + sub;
+        float w = 0.0f;
+        if (kk < nB) {
+            const float4 xb = A.bpos[list_at(A.nbr_b, kk, nf, i)];
+            w = __fmul_rn(xb.w, cs_W_exact(dist2_exact(xi, xb), P));
+        }
+#pragma unroll
+        for (int l = 0; l < TPP; ++l) rho = __fadd_rn(rho, __shfl_sync(gmask, w, first + l));
+    }
+    if (sub != 0) return;
+    A.rho[i] = rho;
+    if (EOS) A.press[i] = tait_pressure(rho, P, P.kr_g);
+}
+
 __global__ void __launch_bounds__(256, 8) k_normals(SimParams P, DeviceArrays A)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -244,11 +297,17 @@ __global__ void __launch_bounds__(256, 8) k_normals(SimParams P, DeviceArrays A)
     A.normal[i] = make_float4(nx * P.h, ny * P.h, nz * P.h, 0.0f);
 }
 
-template <int MODE>
+/* Non-pressure and pressure accelerations (MODE). TPP adjacent lanes share
+   particle i (small scenes), each summing the list entries sub, sub + TPP,
+   ...; the group's sums are combined by shuffles and lane 0 of the group
+   finishes the particle. */
+template <int MODE, int TPP = 1>
 __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
 {
     __shared__ float s_red[32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / TPP;
+    const unsigned sub = (unsigned)t % TPP;
     const bool active = i < active_n(P, A.st);
     const size_t nf = (size_t)P.nf;
     /* per-scene coefficients and time step of a batch */
@@ -272,7 +331,7 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
         const float4 ni = st_on ? A.normal[i] : make_float4(0, 0, 0, 0);
         const float eps_h2 = 0.01f * P.h2;
         float svx = 0.0f, svy = 0.0f, svz = 0.0f; /* standard viscosity sum */
-        for_fluid_neighbors<2>(A, i, nf, nF, [&](unsigned j, const float4& xj) {
+        for_fluid_neighbors<2, TPP>(A, i, nf, nF, [&](unsigned j, const float4& xj) {
             const Pair p = make_pair(xi, xj);
             const float rho_j = A.rho[j];
             const float f = cs_gradf(p.rl, p.inv_rl, P);
@@ -304,7 +363,14 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
                 ay += kij * (-c * p.ry - P.st * (ni.y - nj.y));
                 az += kij * (-c * p.rz - P.st * (ni.z - nj.z));
             }
-        });
+        }, sub);
+        if (TPP > 1) {
+            ax = group_sum<TPP>(ax); ay = group_sum<TPP>(ay); az = group_sum<TPP>(az);
+            svx = group_sum<TPP>(svx); svy = group_sum<TPP>(svy); svz = group_sum<TPP>(svz);
+            /* lane 0 of the group carries the fluid sums on; the boundary sums
+               below are split over the lanes again and combined at the end */
+            if (sub != 0) ax = ay = az = svx = svy = svz = 0.0f;
+        }
         if (vm == 0) {
             const float c = visc_c / rho_i;
             ax += svx * c; ay += svy * c; az += svz * c;
@@ -312,7 +378,7 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
         const bool bvisc = vm >= 0 && bvisc_c != 0.0f;
         if (pressure || bvisc || (np && P.adh_on)) {
             float bvx = 0.0f, bvy = 0.0f, bvz = 0.0f;
-            for (unsigned kk = 0; kk < nB; ++kk) {
+            for (unsigned kk = sub; kk < nB; kk += TPP) {
                 const unsigned bq = list_at(A.nbr_b, kk, nf, i);
                 const float4 xb = A.bpos[bq];
                 const Pair p = make_pair(xi, xb);
@@ -347,10 +413,15 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
                 ax += bvx * c; ay += bvy * c; az += bvz * c;
             }
         }
+        if (TPP > 1) {
+            ax = group_sum<TPP>(ax); ay = group_sum<TPP>(ay); az = group_sum<TPP>(az);
+        }
     }
+    /* from here on, lane 0 of each group stands for its particle */
+    const bool owner = active && sub == 0;
 
     if (MODE == FORCE_WCSPH) {
-        if (active) {
+        if (owner) {
             /* SPHSolver::integrate: a += g; v += a dt; x += v dt (unfused, as the reference rounds) */
             ax = __fadd_rn(ax, P.gx); ay = __fadd_rn(ay, P.gy); az = __fadd_rn(az, P.gz);
             const float nvx = __fadd_rn(vi.x, __fmul_rn(ax, dt)), nvy = __fadd_rn(vi.y, __fmul_rn(ay, dt)),
@@ -365,7 +436,7 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
             if (!isfinite(px) || !isfinite(py) || !isfinite(pz)) atomicOr(&A.st->err, ERRBIT_NAN);
         }
         if (A.sst) {
-            if (active && (unsigned)i == A.sref.scenes[scene].fbegin) {
+            if (owner && (unsigned)i == A.sref.scenes[scene].fbegin) {
                 A.sst[scene].time = advance_time(A.sst[scene].time, dt);
                 A.sst[scene].steps += 1u;
             }
@@ -376,10 +447,10 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
         }
         return;
     }
-    if (active) A.acc[i] = make_float4(ax, ay, az, 0.0f);
+    if (owner) A.acc[i] = make_float4(ax, ay, az, 0.0f);
     if (MODE == FORCE_NP_CFL) {
         float speed = 0.0f;
-        if (active) {
+        if (owner) {
             const float cx = __fadd_rn(vi.x, __fmul_rn(__fadd_rn(ax, P.gx), dt));
             const float cy = __fadd_rn(vi.y, __fmul_rn(__fadd_rn(ay, P.gy), dt));
             const float cz = __fadd_rn(vi.z, __fmul_rn(__fadd_rn(az, P.gz), dt));
@@ -1328,6 +1399,14 @@ int launch_barrier_timeout_probe(DevState* st, cudaStream_t s)
 
 static inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
+/* Lanes per particle for the WCSPH density and force passes: enough threads
+   to fill the GPU (148 SMs x 2048) in small scenes, one lane from 2^19
+   particles on. */
+static int small_scene_lanes(int n)
+{
+    return n >= (1 << 19) ? 1 : n >= (1 << 17) ? 2 : n >= (1 << 15) ? 4 : 8;
+}
+
 void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool eos, int block, cudaStream_t s)
 {
     if (P.nf <= 0) return;
@@ -1335,6 +1414,15 @@ void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool 
     if (alpha && eos) k_density<true, true><<<g, block, 0, s>>>(P, A);
     else if (alpha && A.divres) k_density<true, false, true><<<g, block, 0, s>>>(P, A);
     else if (alpha) k_density<true, false><<<g, block, 0, s>>>(P, A);
+    else if (small_scene_lanes(P.nf) > 1) {
+        const int tpp = small_scene_lanes(P.nf);
+        const int gl = blocks_for((long long)P.nf * tpp, block);
+        void (*k)(SimParams, DeviceArrays) =
+            tpp == 2 ? (eos ? k_density_lanes<true, 2> : k_density_lanes<false, 2>)
+            : tpp == 4 ? (eos ? k_density_lanes<true, 4> : k_density_lanes<false, 4>)
+                       : (eos ? k_density_lanes<true, 8> : k_density_lanes<false, 8>);
+        k<<<gl, block, 0, s>>>(P, A);
+    }
     else if (eos) k_density<false, true><<<g, block, 0, s>>>(P, A);
     else k_density<false, false><<<g, block, 0, s>>>(P, A);
 }
@@ -1351,7 +1439,15 @@ void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, int bloc
     switch (mode) {
     case FORCE_NP: k_forces<FORCE_NP><<<g, block, 0, s>>>(P, A); break;
     case FORCE_NP_CFL: k_forces<FORCE_NP_CFL><<<g, block, 0, s>>>(P, A); break;
-    case FORCE_WCSPH: k_forces<FORCE_WCSPH><<<g, block, 0, s>>>(P, A); break;
+    case FORCE_WCSPH: {
+        const int tpp = small_scene_lanes(P.nf);
+        const int gw = P.nf > 0 ? blocks_for((long long)P.nf * tpp, block) : 1;
+        if (tpp == 1) k_forces<FORCE_WCSPH, 1><<<gw, block, 0, s>>>(P, A);
+        else if (tpp == 2) k_forces<FORCE_WCSPH, 2><<<gw, block, 0, s>>>(P, A);
+        else if (tpp == 4) k_forces<FORCE_WCSPH, 4><<<gw, block, 0, s>>>(P, A);
+        else k_forces<FORCE_WCSPH, 8><<<gw, block, 0, s>>>(P, A);
+        break;
+    }
     default: k_forces<FORCE_PRESSURE><<<g, block, 0, s>>>(P, A); break;
     }
 }
