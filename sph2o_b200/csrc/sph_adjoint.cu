@@ -337,8 +337,9 @@ __global__ void k_adj_unpack(int n, const float4* __restrict__ in, float* __rest
 
 static inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
 
-/* lanes per particle of the adjoint passes: enough threads to fill the GPU */
-static inline int adjoint_tpp(int n) { return n >= (1 << 19) ? 1 : n >= (1 << 17) ? 2 : n >= (1 << 15) ? 4 : 8; }
+/* lanes per particle of the adjoint passes: 4 below 2^16 particles, where
+   one lane per particle leaves most of the GPU idle; one above */
+static inline int adjoint_tpp(int n) { return n < (1 << 16) ? 4 : 1; }
 
 int adjoint_blocks(int n) { return blocks_for(n * adjoint_tpp(n), 256); }
 
@@ -359,11 +360,12 @@ void launch_adjoint_step(const SimParams& P, const AdjointArrays& J, cudaStream_
     if (P.nf <= 0) return;
     k_adj_load<<<blocks_for(P.nf, 256), 256, 0, s>>>(P, J);
     const int g = adjoint_blocks(P.nf);
-    switch (adjoint_tpp(P.nf)) {
-    case 1: k_adj_forces<1><<<g, 256, 0, s>>>(P, J); k_adj_density<1><<<g, 256, 0, s>>>(P, J); break;
-    case 2: k_adj_forces<2><<<g, 256, 0, s>>>(P, J); k_adj_density<2><<<g, 256, 0, s>>>(P, J); break;
-    case 4: k_adj_forces<4><<<g, 256, 0, s>>>(P, J); k_adj_density<4><<<g, 256, 0, s>>>(P, J); break;
-    default: k_adj_forces<8><<<g, 256, 0, s>>>(P, J); k_adj_density<8><<<g, 256, 0, s>>>(P, J); break;
+    if (adjoint_tpp(P.nf) == 1) {
+        k_adj_forces<1><<<g, 256, 0, s>>>(P, J);
+        k_adj_density<1><<<g, 256, 0, s>>>(P, J);
+    } else {
+        k_adj_forces<4><<<g, 256, 0, s>>>(P, J);
+        k_adj_density<4><<<g, 256, 0, s>>>(P, J);
     }
 }
 

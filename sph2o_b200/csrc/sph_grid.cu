@@ -155,14 +155,7 @@ __global__ void __launch_bounds__(256) k_ns_rank_gather(int n, const unsigned* _
     if (g.f_in[1]) g.f_out[1][dst] = g.f_in[1][src];
 }
 
-/* Neighbour lists in the reference's candidate order, filtered at |r| <= h.
-   TPP adjacent lanes share a particle: they test a cell's candidates TPP at
-   a time (lane sub takes q = s + sub, s + sub + TPP, ...), and a ballot over
-   the group ranks the accepted ones, so entries are written in candidate
-   order whatever TPP is. TPP = 1 is one lane per particle (large scenes, where
-   particles already fill the GPU); more lanes shorten each particle's serial
-   candidate walk when there are few particles. */
-template <int TPP>
+/* Neighbour lists in the reference's candidate order, filtered at |r| <= h. */
 __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S, const float4* __restrict__ pos,
                                                         const unsigned* __restrict__ cell_start,
                                                         const float4* __restrict__ bpos,
@@ -171,13 +164,8 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
                                                         unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b,
                                                         DevState* st)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = t / TPP;
-    /* a group's lanes share i, so a group leaves together */
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= active_n(P, st)) return;
-    const unsigned lane = threadIdx.x & 31u, sub = lane % TPP;
-    const unsigned gmask = TPP == 32 ? 0xffffffffu : ((1u << TPP) - 1u) << (lane - sub);
-    const unsigned below = (1u << sub) - 1u;
     const float4 xi = pos[i];
     const size_t nf = (size_t)P.nf;
     /* |r| <= h as the reference rounds it, without the square root */
@@ -185,49 +173,102 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
     unsigned nF = 0, nB = 0;
     for_cells27(xi, P.h, grid_for(P, S, (unsigned)i), [&](unsigned c) {
         const unsigned s = cell_start[c], e = cell_start[c + 1];
-        if (TPP == 1) {
-            for (unsigned q = s; q < e; ++q) {
-                if (dist2_exact(xi, pos[q]) <= s2max) {
-                    if (nF < P.capF) __stcs(nbr_f + (size_t)nF * nf + i, q);
-                    ++nF;
-                }
-            }
-        } else {
-            for (unsigned q0 = s; q0 < e; q0 += TPP) {
-                const unsigned q = q0 + sub;
-                const bool in = q < e && dist2_exact(xi, pos[q]) <= s2max;
-                const unsigned bits = __ballot_sync(gmask, in) >> (lane - sub);
-                if (in) {
-                    const unsigned k = nF + __popc(bits & below);
-                    if (k < P.capF) __stcs(nbr_f + (size_t)k * nf + i, q);
-                }
-                nF += __popc(bits);
+        for (unsigned q = s; q < e; ++q) {
+            if (dist2_exact(xi, pos[q]) <= s2max) {
+                if (nF < P.capF) __stcs(nbr_f + (size_t)nF * nf + i, q);
+                ++nF;
             }
         }
         if (P.nb > 0) {
             const unsigned bs = bcell_start[c], be = bcell_start[c + 1];
-            if (TPP == 1) {
-                for (unsigned q = bs; q < be; ++q) {
-                    if (dist2_exact(xi, bpos[q]) <= s2max) {
-                        if (nB < P.capB) __stcs(nbr_b + (size_t)nB * nf + i, q);
-                        ++nB;
-                    }
-                }
-            } else {
-                for (unsigned q0 = bs; q0 < be; q0 += TPP) {
-                    const unsigned q = q0 + sub;
-                    const bool in = q < be && dist2_exact(xi, bpos[q]) <= s2max;
-                    const unsigned bits = __ballot_sync(gmask, in) >> (lane - sub);
-                    if (in) {
-                        const unsigned k = nB + __popc(bits & below);
-                        if (k < P.capB) __stcs(nbr_b + (size_t)k * nf + i, q);
-                    }
-                    nB += __popc(bits);
+            for (unsigned q = bs; q < be; ++q) {
+                if (dist2_exact(xi, bpos[q]) <= s2max) {
+                    if (nB < P.capB) __stcs(nbr_b + (size_t)nB * nf + i, q);
+                    ++nB;
                 }
             }
         }
     });
-    if (sub != 0) return;
+    cnt_f[i] = min(nF, P.capF);
+    cnt_b[i] = min(nB, P.capB);
+    if (nF > P.capF || nB > P.capB) {
+        atomicAdd(&st->overflow, 1u);
+        atomicOr(&st->err, ERRBIT_OVERFLOW);
+    }
+}
+
+/* The same lists for small scenes, one warp per particle: lane k < 27 loads
+   the range of the particle's k-th cell (the reference's offset order), a
+   warp scan lays the 27 ranges end to end, and the warp then tests the
+   concatenated candidates 32 at a time; a ballot ranks each round's accepted
+   candidates, so entries are written in candidate order. The serial walk of a
+   particle shrinks from ~216 candidates (or 27 cells) to ~7 rounds. */
+__device__ __forceinline__ void warp_candidates(const float4* __restrict__ xs, unsigned s, unsigned e, float4 xi,
+                                                float s2max, unsigned lane, unsigned cap, unsigned* __restrict__ list,
+                                                size_t nf, int i, unsigned& n)
+{
+    const unsigned cnt = e - s;
+    unsigned incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o) incl += v;
+    }
+    const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+    const unsigned excl = incl - cnt;
+    for (unsigned u0 = 0; u0 < total; u0 += 32) {
+        const unsigned u = min(u0 + lane, total - 1u);
+        /* cell of candidate u: the number of lanes whose ranges end at or before u */
+        unsigned k = 0;
+#pragma unroll
+        for (unsigned step = 16; step >= 1; step >>= 1)
+            if (__shfl_sync(0xffffffffu, incl, k + step - 1) <= u) k += step;
+        const unsigned q = __shfl_sync(0xffffffffu, s, k) + (u - __shfl_sync(0xffffffffu, excl, k));
+        const bool in = u0 + lane < total && dist2_exact(xi, xs[q]) <= s2max;
+        const unsigned bits = __ballot_sync(0xffffffffu, in);
+        if (in) {
+            const unsigned r = n + __popc(bits & ((1u << lane) - 1u));
+            if (r < cap) __stcs(list + (size_t)r * nf + i, q);
+        }
+        n += __popc(bits);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_ns_build_lists_warp(SimParams P, SceneRef S,
+                                                             const float4* __restrict__ pos,
+                                                             const unsigned* __restrict__ cell_start,
+                                                             const float4* __restrict__ bpos,
+                                                             const unsigned* __restrict__ bcell_start,
+                                                             unsigned* __restrict__ nbr_f, unsigned* __restrict__ cnt_f,
+                                                             unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b,
+                                                             DevState* st)
+{
+    const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    /* the whole warp shares i and leaves together */
+    if (i >= active_n(P, st)) return;
+    const unsigned lane = threadIdx.x & 31u;
+    const float4 xi = pos[i];
+    const Grid g = grid_for(P, S, (unsigned)i);
+    unsigned s = 0, e = 0, bs = 0, be = 0;
+    if (lane < 27) {
+        const int xx = cell_coord(xi.x, P.h, g.cminx, g.dimx) + (int)lane / 9 - 1;
+        const int yy = cell_coord(xi.y, P.h, g.cminy, g.dimy) + ((int)lane / 3) % 3 - 1;
+        const int zz = cell_coord(xi.z, P.h, g.cminz, g.dimz) + (int)lane % 3 - 1;
+        if (xx >= 0 && xx < g.dimx && yy >= 0 && yy < g.dimy && zz >= 0 && zz < g.dimz) {
+            const unsigned c = brick_morton(xx, yy, zz, g);
+            s = cell_start[c];
+            e = cell_start[c + 1];
+            if (P.nb > 0) {
+                bs = bcell_start[c];
+                be = bcell_start[c + 1];
+            }
+        }
+    }
+    const size_t nf = (size_t)P.nf;
+    unsigned nF = 0, nB = 0;
+    warp_candidates(pos, s, e, xi, P.h2_exact, lane, P.capF, nbr_f, nf, i, nF);
+    if (P.nb > 0) warp_candidates(bpos, bs, be, xi, P.h2_exact, lane, P.capB, nbr_b, nf, i, nB);
+    if (lane != 0) return;
     cnt_f[i] = min(nF, P.capF);
     cnt_b[i] = min(nB, P.capB);
     if (nF > P.capF || nB > P.capB) {
@@ -334,21 +375,16 @@ void launch_build_lists(const SimParams& P, const SceneRef& S, const float4* pos
                         unsigned* cnt_b, DevState* st, cudaStream_t s)
 {
     if (P.nf <= 0) return;
-    /* lanes per particle: enough threads to fill the GPU (148 SMs x 2048) */
-    const int tpp = P.nf >= (1 << 19) ? 1 : P.nf >= (1 << 17) ? 2 : P.nf >= (1 << 15) ? 4 : 8;
-    const long long nt = (long long)P.nf * tpp;
-    if (tpp == 1)
-        k_ns_build_lists<1><<<blocks_for(nt, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
-                                                                 cnt_f, nbr_b, cnt_b, st);
-    else if (tpp == 2)
-        k_ns_build_lists<2><<<blocks_for(nt, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
-                                                                 cnt_f, nbr_b, cnt_b, st);
-    else if (tpp == 4)
-        k_ns_build_lists<4><<<blocks_for(nt, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
-                                                                 cnt_f, nbr_b, cnt_b, st);
+    /* A warp per particle below 2^16 particles, where one lane's serial walk
+       over ~216 candidates is the critical path (32k: 32 vs 56 us per build);
+       one lane per particle above, where the particles fill the GPU and the
+       warp's extra instructions cost more (125k: 0.069 vs 0.096 ms). */
+    if (P.nf < (1 << 16))
+        k_ns_build_lists_warp<<<blocks_for((long long)P.nf * 32, 128), 128, 0, s>>>(
+            P, S, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f, nbr_b, cnt_b, st);
     else
-        k_ns_build_lists<8><<<blocks_for(nt, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
-                                                                 cnt_f, nbr_b, cnt_b, st);
+        k_ns_build_lists<<<blocks_for(P.nf, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
+                                                                cnt_f, nbr_b, cnt_b, st);
 }
 
 void launch_boundary_volume(const SimParams& P, const SceneRef& S, float4* bpos, const unsigned* bcell_start,

@@ -1399,12 +1399,13 @@ int launch_barrier_timeout_probe(DevState* st, cudaStream_t s)
 
 static inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
-/* Lanes per particle for the WCSPH density and force passes: enough threads
-   to fill the GPU (148 SMs x 2048) in small scenes, one lane from 2^19
-   particles on. */
+/* Lanes per particle for the WCSPH density and force passes: 4 below 2^16
+   particles, where one lane per particle leaves most of the GPU idle and its
+   serial neighbour walk is the critical path (32k particles: forces 42.8 ->
+   18.4 us, density 25 -> 14 us); one lane above. */
 static int small_scene_lanes(int n)
 {
-    return n >= (1 << 19) ? 1 : n >= (1 << 17) ? 2 : n >= (1 << 15) ? 4 : 8;
+    return n < (1 << 16) ? 4 : 1;
 }
 
 void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool eos, int block, cudaStream_t s)
@@ -1415,13 +1416,9 @@ void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool 
     else if (alpha && A.divres) k_density<true, false, true><<<g, block, 0, s>>>(P, A);
     else if (alpha) k_density<true, false><<<g, block, 0, s>>>(P, A);
     else if (small_scene_lanes(P.nf) > 1) {
-        const int tpp = small_scene_lanes(P.nf);
-        const int gl = blocks_for((long long)P.nf * tpp, block);
-        void (*k)(SimParams, DeviceArrays) =
-            tpp == 2 ? (eos ? k_density_lanes<true, 2> : k_density_lanes<false, 2>)
-            : tpp == 4 ? (eos ? k_density_lanes<true, 4> : k_density_lanes<false, 4>)
-                       : (eos ? k_density_lanes<true, 8> : k_density_lanes<false, 8>);
-        k<<<gl, block, 0, s>>>(P, A);
+        const int gl = blocks_for((long long)P.nf * 4, block);
+        if (eos) k_density_lanes<true, 4><<<gl, block, 0, s>>>(P, A);
+        else k_density_lanes<false, 4><<<gl, block, 0, s>>>(P, A);
     }
     else if (eos) k_density<false, true><<<g, block, 0, s>>>(P, A);
     else k_density<false, false><<<g, block, 0, s>>>(P, A);
@@ -1443,9 +1440,7 @@ void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, int bloc
         const int tpp = small_scene_lanes(P.nf);
         const int gw = P.nf > 0 ? blocks_for((long long)P.nf * tpp, block) : 1;
         if (tpp == 1) k_forces<FORCE_WCSPH, 1><<<gw, block, 0, s>>>(P, A);
-        else if (tpp == 2) k_forces<FORCE_WCSPH, 2><<<gw, block, 0, s>>>(P, A);
-        else if (tpp == 4) k_forces<FORCE_WCSPH, 4><<<gw, block, 0, s>>>(P, A);
-        else k_forces<FORCE_WCSPH, 8><<<gw, block, 0, s>>>(P, A);
+        else k_forces<FORCE_WCSPH, 4><<<gw, block, 0, s>>>(P, A);
         break;
     }
     default: k_forces<FORCE_PRESSURE><<<g, block, 0, s>>>(P, A); break;
