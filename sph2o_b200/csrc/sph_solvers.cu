@@ -345,7 +345,10 @@ __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
                 const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
                 if (vm == 1) {
                     const float dot = (dvx * p.rx + dvy * p.ry) + dvz * p.rz;
-                    const float c = visc_c * (P.mass / rho_j) * dot / (p.s + eps_h2) * f;
+                    /* nu (m / rho_j) dot / (|r|^2 + 0.01 h^2) gradW with one fast
+                       division (this pass is compared with the reference to a
+                       relative tolerance, not bit for bit) */
+                    const float c = visc_c * __fdividef(P.mass * dot, rho_j * (p.s + eps_h2)) * f;
                     ax += c * p.rx; ay += c * p.ry; az += c * p.rz;
                 } else if (vm == 0) {
                     const float c = P.mass / rho_j * visco_lapl(p.rl, P);
