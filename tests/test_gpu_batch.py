@@ -1,7 +1,9 @@
 """Batches of independent scenes (sph_batch_*): each scene of a batch must
-evolve exactly as it does alone. WCSPH: bit-identical states. DFSPH: the
-same iteration counts per scene and step, states equal to 1e-6 (norm-wise;
-the per-scene FP64 residual sums are reduced in a different order)."""
+evolve exactly as it does alone. WCSPH: bit-identical states (batch and
+scenes here are all below 2^16 particles, so both take the same lanes per
+particle in the force pass). DFSPH: the same iteration counts per scene and
+step, states equal to 1e-6 (norm-wise; the per-scene FP64 residual sums are
+reduced in a different order)."""
 import numpy as np
 import pytest
 
