@@ -28,6 +28,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+import hashlib
 import json
 import os
 import shutil
@@ -37,6 +38,8 @@ import sys
 import tempfile
 import threading
 import time
+
+import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -63,10 +66,37 @@ BYTES = {
 }
 
 
-# DRAM traffic of the density-solver launch per neighbour pass on the 1M
-# workload, measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of a
-# 3-iteration launch = 1.952 GB over 8 passes; profiles/dfsph_1m_pass_kernels.md).
-NCU_DENSITY_SOLVE_BYTES_PER_PASS = 1.952e9 / 8.0
+# Measured DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) of
+# a kernel on a workload, per neighbour pass, recorded together with a hash of
+# the CUDA sources the kernel is compiled from. A record is used only while
+# those sources are unchanged; otherwise the line reports no traffic.
+TRAFFIC_RECORDS = os.path.join(ROOT, "profiles", "density_solver_dfsph_1m_dram_traffic.json")
+SOLVER_SOURCES = ("sph2o_b200/csrc/sph_solvers.cu", "sph2o_b200/csrc/sph_device.cuh",
+                  "sph2o_b200/csrc/sph_internal.h")
+
+
+def solver_source_key():
+    """sha256 (16 hex digits) of the sources of the solver kernels."""
+    h = hashlib.sha256()
+    for rel in SOLVER_SOURCES:
+        with open(os.path.join(ROOT, rel), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def traffic_record(kernel, workload):
+    """The measured-traffic record of `kernel` on `workload` for the current
+    sources, or None."""
+    try:
+        with open(TRAFFIC_RECORDS) as f:
+            recs = json.load(f).get("records", [])
+    except (OSError, ValueError):
+        return None
+    key = solver_source_key()
+    for r in recs:
+        if r.get("kernel") == kernel and r.get("workload") == workload and r.get("source_key") == key:
+            return r
+    return None
 
 
 def workloads():
@@ -101,6 +131,9 @@ def batched_run(steps, warmup, method=0, count=256, loop_steps=None, indices=Non
     scs = [Scene.from_dict(d) for d in dicts]
     batch = Batch(scs)
     total = batch.nf
+    # launch shape and cell order picked by the library's autotuner (trial
+    # steps from a snapshot that is restored), cached per GPU and workload
+    tuned = batch.autotune(trial_steps=3, cache_path=os.path.join(tempfile.gettempdir(), "sph2o_autotune.json"))
     batch.step(warmup)
     torch.cuda.synchronize()
     t0 = _t.perf_counter()
@@ -108,7 +141,7 @@ def batched_run(steps, warmup, method=0, count=256, loop_steps=None, indices=Non
     wall_batch = _t.perf_counter() - t0
     dev_ms = st["device_ms"]
     batch.close()
-    loop_steps = loop_steps or max(1, min(steps, 10))
+    loop_steps = loop_steps or steps  # the same window as the batch
     sims = [Simulation.from_scene(sc) for sc in scs]
     for sim in sims:
         sim.step(warmup)
@@ -128,7 +161,9 @@ def batched_run(steps, warmup, method=0, count=256, loop_steps=None, indices=Non
     return {"scenes": len(scs), "fluid_particles": total, "steps": steps, "value": batched,
             "value_wall": batched_wall, "per_scene_loop": loop, "speedup_vs_loop": batched_wall / loop,
             "ms_per_step": dev_ms / steps, "mean_iterations": st["total_iterations"] / max(1, steps) / count,
-            "method": "WCSPH" if method == 0 else "DFSPH"}
+            "method": "WCSPH" if method == 0 else "DFSPH", "loop_steps": loop_steps, "autotuned": tuned,
+            "timing": f"batch: {steps} steps after {warmup} warm-up steps; per-scene loop: {loop_steps} steps after "
+                      f"the same warm-up, every scene in turn; wall clock for both in speedup_vs_loop"}
 
 
 def adjoint_run(steps=500, every=50, repeats=3):
@@ -254,24 +289,63 @@ def dist_setup():
     return world, rank, local
 
 
-def reference_run(scene_dict, steps, warmup, threads=None):
-    """Time SPH2O's OpenMP CPU path on this host for the given scene."""
+def physical_cores():
+    """Physical cores this process may run on (SMT siblings counted once)."""
+    try:
+        cpus = sorted(os.sched_getaffinity(0))
+    except AttributeError:
+        cpus = list(range(os.cpu_count() or 1))
+    cores = set()
+    for c in cpus:
+        try:
+            with open(f"/sys/devices/system/cpu/cpu{c}/topology/core_id") as f:
+                core = f.read().strip()
+            with open(f"/sys/devices/system/cpu/cpu{c}/topology/physical_package_id") as f:
+                pkg = f.read().strip()
+            cores.add((pkg, core))
+        except OSError:
+            cores.add(("cpu", c))
+    return max(1, len(cores))
+
+
+def reference_run(scene_dict, steps, warmup, threads=None, state=None):
+    """Time SPH2O's OpenMP CPU path on this host for the given scene: one
+    OpenMP thread per physical core (OMP_PLACES=cores, OMP_PROC_BIND=close).
+    `state` = (positions, velocities) replaces the scene's initial fluid
+    state (caller order)."""
     if not os.path.exists(REF_BIN):
         return None, "reference build missing (oracle/_ref/sph2o_ref_fast; run make -C oracle)"
-    threads = threads or os.cpu_count() or 1
+    threads = threads or physical_cores()
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close", OMP_PLACES="cores")
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "scene.json")
         with open(path, "w") as f:
             json.dump(scene_dict, f)
-        r = subprocess.run([REF_BIN, "-c", path, "--mode", "time", "--steps", str(steps), "--warmup", str(warmup),
-                            "--threads", str(threads)], capture_output=True, text=True, env=env, timeout=1800)
+        cmd = [REF_BIN, "-c", path, "--mode", "time", "--steps", str(steps), "--warmup", str(warmup),
+               "--threads", str(threads)]
+        if state is not None:
+            from oracle import sphd
+            sp = os.path.join(td, "state.sphd")
+            sphd.write(sp, {"pos": np.asarray(state[0], np.float32), "vel": np.asarray(state[1], np.float32)})
+            cmd += ["--state-in", sp]
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
     if r.returncode != 0:
         return None, f"reference run failed: {r.stderr.strip()[-200:]}"
     line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
     out = json.loads(line)
     out["threads"] = threads
     return out, None
+
+
+def cpu_baseline_entry(res, err, sample):
+    """The cpu_baseline object of a line from a reference_run result."""
+    if res is None:
+        return {"value": None, "unit": UNIT, "cores": physical_cores(), "kind": "reference", "sample": err}
+    return {"value": res["particle_steps_per_s"], "unit": UNIT, "cores": res["threads"], "kind": "reference",
+            "sample": f"{sample}; {res['steps']} timed steps after {res['warmup']} warm-up steps, SPH2O sources "
+                      f"built -O3 -ffast-math -fopenmp, {res['threads']} OpenMP threads (one per physical core) "
+                      f"on {cpu_model()}; mean iterations {res['mean_iterations']:.2f} + "
+                      f"{res['mean_iterations_v']:.2f}"}
 
 
 def cpu_model():
@@ -298,11 +372,20 @@ def bytes_per_launch(phase, nf, nb_active, its):
     return nf * per + 16 * nb_active * passes
 
 
+def reference_window(steps, warmup):
+    """Steps of the CPU reference sample for a GPU window of `steps` timed
+    steps after `warmup`: the same window when it is short (at most 40 steps,
+    about 40 s on 16 cores for the 1M scene), else its first 20 steps after
+    at most 5 warm-up steps."""
+    if steps + warmup <= 40:
+        return steps, warmup
+    return min(steps, 20), min(warmup, 5)
+
+
 def run_reference_arm(args, name, desc, scene_dict, world, rank):
     if rank != 0:
         return 0
-    steps = max(1, min(args.steps, 10))
-    warm = max(1, min(args.warmup, 2))
+    steps, warm = reference_window(args.steps, args.warmup)
     res, err = reference_run(scene_dict, steps, warm)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
@@ -315,19 +398,147 @@ def run_reference_arm(args, name, desc, scene_dict, world, rank):
         "config": {"workload": desc, "fluid_particles": res["fluid_particles"],
                    "boundary_particles": res["boundary_particles"], "mean_iterations": res["mean_iterations"],
                    "mean_iterations_v": res["mean_iterations_v"]},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": res["threads"], "kind": "reference",
-                         "sample": f"{steps} timed steps after {warm} warm-up steps of the same scene, "
-                                   f"SPH2O sources built -O3 -ffast-math -fopenmp, {cpu_model()}"},
+        "cpu_baseline": cpu_baseline_entry(res, None, "the same scene and step window as the GPU arm"),
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
 
 
+# ---- across ranks (one process per GPU; gloo on CPU in the tests) -------------------------------------------
+
+def max_over_ranks(x, world, device="cpu"):
+    """The largest of a per-rank number over all ranks (all_reduce MAX)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world, device="cpu"):
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def replica_value(particles, steps, device_ms, world, device="cpu"):
+    """Whole-job particle-steps/s of `world` replicas of one scene: all ranks'
+    particle-steps over the slowest rank's device time."""
+    max_ms = max_over_ranks(device_ms, world, device)
+    return world * particles * steps / (max_ms / 1e3), max_ms
+
+
+def batch_shard(count, world, rank):
+    """This rank's scenes of the batched workload (greedy longest-processing-
+    time on fluid particles; every rank computes the same partition)."""
+    from sph2o_b200 import scenes as S
+    from sph2o_b200.sharding import scene_cost, shard_for_rank
+    costs = [scene_cost(p["dims"][0] * p["dims"][1] * p["dims"][2]) for p in S.batched_scene_params(count)]
+    return shard_for_rank(costs, world, rank)
+
+
+def combine_batch_results(res, world, device="cpu"):
+    """Whole-job batched rate: all ranks' fluid particles over the slowest
+    rank's step time (no collective touches particle data)."""
+    if world <= 1:
+        return res
+    tmax = max_over_ranks(res["ms_per_step"], world, device)
+    tot = sum_over_ranks(res["fluid_particles"], world, device)
+    res = dict(res)
+    res["value"] = tot / (tmax / 1e3)
+    res["fluid_particles_all_ranks"] = int(tot)
+    res["ms_per_step_max_rank"] = tmax
+    return res
+
+
+# ---- secondary workloads --------------------------------------------------------------------------------------
+
+def config_run(name, steps, warmup, cpu=True, cpu_window=None):
+    """One named workload on this GPU (device-timed window of `steps` after
+    `warmup`) and, when cpu, the reference's OpenMP path on the host cores over
+    `cpu_window` = (steps, warmup) (default: the same window)."""
+    from sph2o_b200.api import Scene, Simulation
+    desc, make = workloads()[name]
+    d = make()
+    scene = Scene.from_dict(d)
+    sim = Simulation.from_scene(scene)
+    nf, nb = sim.nf, sim.nb
+    if warmup:
+        sim.step(warmup)
+    st = sim.step(steps)
+    sim.close()
+    scene.close()
+    out = {"workload": desc, "fluid_particles": nf, "boundary_particles": nb, "steps": steps, "warmup": warmup,
+           "value": nf * steps / (st["device_ms"] / 1e3), "unit": UNIT, "ms_per_step": st["device_ms"] / steps,
+           "mean_iterations": st["total_iterations"] / steps, "mean_iterations_v": st["total_iterations_v"] / steps,
+           "last_avg_density_error": st["avg_density_error"], "l2": l2_note(nf, nb),
+           "timing": "CUDA events on the library stream around the window"}
+    if cpu:
+        cs, cw = cpu_window or (steps, warmup)
+        res, err = reference_run(d, cs, cw)
+        out["cpu_baseline"] = cpu_baseline_entry(
+            res, err, "the same scene and step window" if (cs, cw) == (steps, warmup) else "the same scene")
+        if res is not None:
+            out["vs_cpu_baseline"] = out["value"] / res["particle_steps_per_s"]
+    return out
+
+
+def later_window_run(scene_dict, desc, start, steps, cpu=True, cpu_steps=5, cpu_warmup=3):
+    """The same scene later in the run: steps start + 1 .. start + steps (the
+    first `start` steps untimed). The CPU reference starts from the GPU's
+    state after step `start` (positions and velocities; its adaptive time
+    step restarts from the scene's), takes a few warm-up steps, then a
+    bounded sample."""
+    from sph2o_b200.api import Scene, Simulation
+    scene = Scene.from_dict(scene_dict)
+    sim = Simulation.from_scene(scene)
+    nf = sim.nf
+    sim.step(start)
+    x, v, _ = sim.state()
+    st = sim.step(steps)
+    sim.close()
+    scene.close()
+    out = {"workload": desc + f", steps {start + 1}-{start + steps}", "fluid_particles": nf, "steps": steps,
+           "warmup": start, "value": nf * steps / (st["device_ms"] / 1e3), "unit": UNIT,
+           "ms_per_step": st["device_ms"] / steps, "mean_iterations": st["total_iterations"] / steps,
+           "mean_iterations_v": st["total_iterations_v"] / steps, "last_avg_density_error": st["avg_density_error"],
+           "density_error_gate": bool(st["avg_density_error"] <= 1e-3), "simulated_time_s": st["time"]}
+    if cpu:
+        res, err = reference_run(scene_dict, cpu_steps, cpu_warmup, state=(x, v))
+        out["cpu_baseline"] = cpu_baseline_entry(res, err, f"the same scene from the GPU state after step {start}")
+        if res is not None:
+            out["vs_cpu_baseline"] = out["value"] / res["particle_steps_per_s"]
+    return out
+
+
+def neighbor_search_roofline(sim, prof, steps, peak, peak_kind):
+    """Sort + list build against HBM: algorithmic bytes per fluid particle =
+    52 (sort: read position and velocity 24, write them reordered 24, cell
+    offset 4) + 20 (list build: read position 12, write two list lengths 8)
+    + 4 per neighbour-list entry written, over their event time per step."""
+    fo, fi, bo, bi = sim.neighbors()
+    entries = int(fi.size) + int(bi.size)
+    nf = sim.nf
+    ms = (prof["sort"]["ms"] + prof["lists"]["ms"]) / steps
+    algo = nf * (52 + 20) + 4 * entries
+    achieved = algo / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_kind": f"of {peak_kind}", "algorithmic_bytes_per_step": algo, "ms_per_step": ms,
+            "list_entries_per_particle": entries / nf,
+            "kernels": "k_ns_count, scan, k_ns_scatter, k_ns_rank_gather (sort); k_ns_build_lists (lists)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="double_dam_break_dfsph_1m")
@@ -336,7 +547,7 @@ def main():
     ap.add_argument("--batch-method", type=int, default=0)
     ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--no-secondary", action="store_true",
-                    help="skip the adjoint and batched-scenes measurements added to the JSON line")
+                    help="skip the secondary workloads (other configurations, later window, adjoint, batches)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     name = args.workload
@@ -352,15 +563,14 @@ def main():
         print(json.dumps(res))
         return 0
 
-    import numpy as np
     import torch
     import torch.distributed as dist
 
     torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     from sph2o_b200.api import Scene, Simulation, select_device
 
     select_device(local)
@@ -397,12 +607,7 @@ def main():
         dist.barrier()
     clocks = sampler.stop()
 
-    dev_ms = stats["device_ms"]
-    t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * nf * args.steps / (max_ms / 1e3)
+    value, max_ms = replica_value(nf, args.steps, stats["device_ms"], world, dev)
     its = stats["total_iterations"] / max(args.steps, 1)
     itsv = stats["total_iterations_v"] / max(args.steps, 1)
 
@@ -415,14 +620,17 @@ def main():
     nb_active = nb  # upper bound of boundary particles with a fluid neighbour
     algo = bytes_per_launch(dom, nf, nb_active, it_for)
     achieved = algo / (avg_ms / 1e3) / 1e9
-    traffic, traffic_note = None, None
-    if dom == "density_solve" and name == "double_dam_break_dfsph_1m":
-        traffic = NCU_DENSITY_SOLVE_BYTES_PER_PASS * (2 + 2 * it_for)
-        traffic_note = ("ncu DRAM bytes per neighbour pass of this kernel on this workload (1.952 GB per "
-                        "3-iteration launch, profiles/dfsph_1m_pass_kernels.md) x the timed window's passes")
+    traffic, traffic_note = None, "no DRAM capture recorded for this build of the kernel"
+    rec = traffic_record("k_dfsph_solve(density)", name) if dom == "density_solve" else None
+    if rec is not None:
+        traffic = rec["dram_bytes_per_pass"] * (2 + 2 * it_for)
+        traffic_note = (f"ncu DRAM bytes per neighbour pass of this kernel on this workload, captured for this "
+                        f"build of the solver sources (key {rec['source_key']}), x the window's mean passes per "
+                        f"launch")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "traffic_note": traffic_note, "kernel": dom, "peak_kind": f"of {peak_kind}",
-                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": avg_ms}
+                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": avg_ms,
+                "neighbor_search": neighbor_search_roofline(sim, prof, args.steps, peak, peak_kind)}
 
     # End to end through the C ABI with host buffers, over the same window:
     # the state entering it is uploaded from pinned host memory, every step
@@ -445,55 +653,46 @@ def main():
         rc = L.sph_step(sim._h, 1, st1)
         e2e_its += st1.total_iterations
     rc = rc or L.sph_get_state(sim._h, _fptr(px), _fptr(pv), _fptr(pr))
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
     e2e = None
     if rc == 0:
-        e2e = {"value": world * nf * ke / float(te.item()), "unit": UNIT,
+        e2e = {"value": world * nf * ke / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": (nf * 24) // ke,
                "d2h_bytes_per_step": ctypes.sizeof(StepStats) + (nf * 28) // ke,
                "steps": ke, "mean_iterations": e2e_its / ke,
                "note": "state uploaded once from pinned host memory, per-step statistics read back by every "
                        "sph_step call, final state (x, v, rho) read back; same window as value"}
+    sim.close()
+    scene.close()
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        res, err = reference_run(scene_dict, 3, 1)
-        if res is not None:
-            cpu = {"value": res["particle_steps_per_s"], "unit": UNIT, "cores": res["threads"], "kind": "reference",
-                   "sample": f"3 timed steps after 1 warm-up step of the same scene (SPH2O sources, -O3 "
-                             f"-ffast-math -fopenmp, {cpu_model()}); mean iterations {res['mean_iterations']:.2f}"
-                             f" + {res['mean_iterations_v']:.2f}"}
-        else:
-            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference", "sample": err}
+    on_cpu = rank == 0 and world == 1 and not args.no_cpu_baseline
+    if on_cpu:
+        cs, cw = reference_window(args.steps, args.warmup)
+        res, err = reference_run(scene_dict, cs, cw)
+        cpu = cpu_baseline_entry(res, err, "the same scene" + (" and step window as value"
+                                                               if (cs, cw) == (args.steps, args.warmup) else ""))
 
     secondary = None
     if not args.no_secondary:
-        secondary = {"adjoint_wcsph_32k": adjoint_run()}
+        secondary = {}
+        if name == "double_dam_break_dfsph_1m":
+            secondary["double_dam_break_dfsph_1m_later"] = later_window_run(scene_dict, desc, 200, 100, cpu=on_cpu)
+        secondary["double_dam_break_pcisph_1m"] = config_run("double_dam_break_pcisph_1m", 20, 5, cpu=on_cpu,
+                                                             cpu_window=(5, 2))
+        secondary["dam_break_wcsph_8k"] = config_run("dam_break_wcsph_8k", 2000, 20, cpu=on_cpu)
+        secondary["dam_break_dfsph_125k"] = config_run("dam_break_dfsph_125k", 50, 20, cpu=on_cpu,
+                                                       cpu_window=(30, 20))
+        secondary["adjoint_wcsph_32k"] = adjoint_run()
         # independent scenes shard across ranks: each steps its own subset as
         # one batch; only the timing and particle totals are reduced
-        from sph2o_b200 import scenes as S
-        from sph2o_b200.sharding import scene_cost, shard_for_rank
-        costs = [scene_cost(p["dims"][0] * p["dims"][1] * p["dims"][2])
-                 for p in S.batched_scene_params(args.batch_scenes)]
-        shard = shard_for_rank(costs, world, rank)
-        for m, name in ((0, "batched_wcsph_256"), (2, "batched_dfsph_256")):
+        shard = batch_shard(args.batch_scenes, world, rank)
+        for m, bname in ((0, "batched_wcsph_256"), (2, "batched_dfsph_256")):
             res = batched_run(50, 3, method=m, count=args.batch_scenes, indices=shard)
-            if world > 1:
-                red = torch.tensor([res["ms_per_step"], float(res["fluid_particles"])], dtype=torch.float64,
-                                   device="cuda")
-                tmax = red[:1].clone()
-                dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-                tot = red[1:].clone()
-                dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-                res["value"] = float(tot.item()) / (float(tmax.item()) / 1e3)
-                res["fluid_particles_all_ranks"] = int(tot.item())
-                res["ms_per_step_max_rank"] = float(tmax.item())
+            res = combine_batch_results(res, world, dev)
             res["sharding"] = {"ranks": world, "scenes_this_rank": len(shard),
                                "rule": "greedy longest-processing-time on fluid particles, no collective on particle data"}
-            secondary[name] = res
+            secondary[bname] = res
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -517,8 +716,6 @@ def main():
     }
     if rank == 0:
         print(json.dumps(line))
-    sim.close()
-    scene.close()
     if world > 1:
         dist.destroy_process_group()
     return 0

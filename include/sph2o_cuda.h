@@ -373,14 +373,18 @@ int sph_debug_barrier_timeout(sph_ctx* ctx);
    process whose device memory is pooled by a framework, or on a real-time
    path that may not take the allocator's locks or its implicit
    synchronisation. No counterpart in the reference (SPH2O is CPU-only); the
-   density is SPHSolver::computeFluidDensities' sum, equal bit for bit to
-   sph_compute_phase(SPH_PHASE_DENSITY) for the same particles.
+   density is SPHSolver::computeFluidDensities' sum.
    Inputs and output are device pointers owned by the caller:
      xyz      nf * 3 floats, fluid positions
      bxyzpsi  nb * 4 floats, boundary x, y, z and psi = rho0 * V_b
+              (may be NULL when nb = 0)
      rho_out  nf floats, written in the order of xyz
-   domain_min/max (host, 3 floats each) bound the particles; particles outside
-   still get correct densities, only slower. Work is queued on `stream`
+   domain_min/max (host, 3 finite floats each) bound the particles. For
+   particles inside them the densities equal
+   sph_compute_phase(SPH_PHASE_DENSITY) bit for bit; a particle outside is
+   clamped into an edge cell of the grid, still finds all its neighbours but
+   sums them in another order, so its density agrees only to rounding (and
+   takes longer). Work is queued on `stream`
    (a cudaStream_t; NULL = the legacy default stream) and the call returns
    without waiting. Nothing is allocated: the neighbour-search scratch is a
    fixed file-scope device array of about 9.5 MiB that every GPU loading this
@@ -391,7 +395,10 @@ int sph_debug_barrier_timeout(sph_ctx* ctx);
    work overlaps on the GPU race and must be serialised by the caller. The
    first call on each device looks up the array's address
    (cudaGetSymbolAddress) with that device current; make it before any stream
-   capture on that device. */
+   capture on that device. The address is kept per device and CUDA context:
+   after cudaDeviceReset the next call looks it up again, so that call also
+   belongs outside a stream capture. Non-finite bounds, or bounds whose cell
+   indices do not fit in an int, return SPH_ERR_ARG. */
 int sph_density_noalloc(float particle_radius, float density0, const float* xyz, unsigned nf,
                         const float* bxyzpsi, unsigned nb, const float domain_min[3],
                         const float domain_max[3], float* rho_out, void* stream);

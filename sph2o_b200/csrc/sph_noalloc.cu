@@ -22,15 +22,24 @@
  *     by the caller;
  *   - the first call on each device looks up the array's device address with
  *     cudaGetSymbolAddress (once, with that device current); make that first
- *     call before any stream capture on the device.
+ *     call before any stream capture on the device. The address is cached per
+ *     device ordinal and CUDA context id, so after cudaDeviceReset (a new
+ *     primary context, the module possibly reloaded elsewhere) the next call
+ *     looks it up again -- that call, too, belongs outside a stream capture.
  * The kernels reuse the pipeline's sort (sph_grid.cu) and evaluate each
  * density over the 27 cells in the same order and with the same exact
- * arithmetic as the context path, so the result equals
- * sph_compute_phase(SPH_PHASE_DENSITY) bit for bit for the same particles.
+ * arithmetic as the context path, so for particles inside domain_min/max the
+ * result equals sph_compute_phase(SPH_PHASE_DENSITY) bit for bit. A particle
+ * outside the grid is clamped into an edge cell: it still finds every
+ * neighbour, but visits them in another order, so its density can differ
+ * from the context path's in the last bits.
  */
 #include "../../include/sph2o_cuda.h"
 #include "sph_internal.h"
 
+#include <cuda.h> /* driver types only: the two driver calls are fetched at run time */
+
+#include <climits>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -71,7 +80,43 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 namespace {
 
 std::mutex g_setup_mutex;
-unsigned char* g_scratch_dev[64] = {};  /* device address per device ordinal */
+
+/* Device address of the scratch per device ordinal, valid for the CUDA
+   context it was looked up in (ctx_id; 0 = unknown). */
+struct ScratchAddr {
+    unsigned long long ctx_id;
+    unsigned char* ptr;
+};
+ScratchAddr g_scratch_dev[64] = {};
+
+/* Unique id of the context current on this thread (cuCtxGetCurrent +
+   cuCtxGetId, fetched through cudaGetDriverEntryPoint so the library does not
+   link libcuda). Returns false when no context is current or the driver
+   calls are unavailable. Called under g_setup_mutex. */
+bool current_context_id(unsigned long long* id)
+{
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool resolved = false;
+    if (!resolved) {
+        cudaDriverEntryPointQueryResult q1{}, q2{};
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<GetCurrent>(f1);
+            get_id = reinterpret_cast<GetId>(f2);
+        }
+        resolved = true;
+    }
+    if (!get_current || !get_id) return false;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
 
 __global__ void k_na_pack_fluid(int n, const float* __restrict__ xyz, float4* __restrict__ out,
                                 unsigned* __restrict__ ids)
@@ -153,7 +198,7 @@ extern "C" int sph_density_noalloc(float particle_radius, float density0, const 
                                          "exceed SPH_NOALLOC_MAX_BOUNDARY = " + std::to_string(kMaxBoundary));
 
     /* grid over the caller's domain (+1 cell), brick-padded; particles outside
-       it are clamped into the edge cells and still found */
+       it are clamped into the edge cells: still found, in another order */
     SimParams P{};
     P.r = particle_radius;
     P.h = 4.0f * particle_radius;
@@ -170,9 +215,14 @@ extern "C" int sph_density_noalloc(float particle_radius, float density0, const 
     P.nb = (int)nb;
     int cmin[3], dim[3];
     for (int k = 0; k < 3; ++k) {
+        if (!std::isfinite(domain_min[k]) || !std::isfinite(domain_max[k]))
+            return na_fail(SPH_ERR_ARG, "sph_density_noalloc: domain bounds must be finite");
         if (!(domain_max[k] >= domain_min[k])) return na_fail(SPH_ERR_ARG, "domain_max < domain_min");
         const double a = std::floor((double)domain_min[k] / P.h) - 1.0;
         const double b = std::floor((double)domain_max[k] / P.h) + 1.0;
+        if (a < (double)(INT_MIN / 2) || b > (double)(INT_MAX / 2))
+            return na_fail(SPH_ERR_ARG, "sph_density_noalloc: domain bounds too far from the origin for cell "
+                                        "indices of edge 4r");
         if (b - a + 1.0 > (double)kMaxCells) return na_fail(SPH_ERR_CAPACITY, "sph_density_noalloc: domain too large");
         cmin[k] = (int)a;
         dim[k] = ((int)(b - a + 1.0) + 3) / 4 * 4;
@@ -195,14 +245,20 @@ extern "C" int sph_density_noalloc(float particle_radius, float density0, const 
     unsigned char* base = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_setup_mutex);
-        if (!g_scratch_dev[dev]) {
+        unsigned long long ctx = 0;
+        const bool known = current_context_id(&ctx);
+        ScratchAddr& slot = g_scratch_dev[dev];
+        if (!slot.ptr || !known || slot.ctx_id != ctx) {
+            /* first call on this device, or its context changed (cudaDeviceReset) */
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess)
                 return na_fail(SPH_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            g_scratch_dev[dev] = static_cast<unsigned char*>(p);
+            if (!current_context_id(&ctx)) ctx = 0;  /* the lookup made the primary context current */
+            slot.ptr = static_cast<unsigned char*>(p);
+            slot.ctx_id = ctx;
         }
-        base = g_scratch_dev[dev];
+        base = slot.ptr;
     }
     if (nf == 0) return SPH_OK;
 
