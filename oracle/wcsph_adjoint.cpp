@@ -25,6 +25,8 @@
  * pair in scatter form -- a different arrangement from the GPU's gather
  * form, so the two check each other.
  */
+#include <omp.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -120,20 +122,29 @@ struct Problem {
         const size_t n = x.size();
         Grid fg{h, {}};
         fg.build(x);
-        L.fo.assign(n + 1, 0);
-        L.bo.assign(n + 1, 0);
-        L.fi.clear();
-        L.bi.clear();
-        for (size_t i = 0; i < n; ++i) {
-            std::vector<uint32_t> f, b;
+        /* per-particle sets in parallel (read-only grid lookups), then CSR */
+        std::vector<std::vector<uint32_t>> F(n), B(n);
+#pragma omp parallel for schedule(dynamic, 256)
+        for (long i = 0; i < (long)n; ++i) {
+            std::vector<uint32_t>& f = F[i];
+            std::vector<uint32_t>& b = B[i];
             fg.around(x[i], [&](uint32_t j) { const V r = x[i] - x[j]; if (std::sqrt(dot(r, r)) <= h) f.push_back(j); });
             bgrid.around(x[i], [&](uint32_t k) { const V r = x[i] - bx[k]; if (std::sqrt(dot(r, r)) <= h) b.push_back(k); });
             std::sort(f.begin(), f.end());
             std::sort(b.begin(), b.end());
-            L.fi.insert(L.fi.end(), f.begin(), f.end());
-            L.bi.insert(L.bi.end(), b.begin(), b.end());
-            L.fo[i + 1] = (uint32_t)L.fi.size();
-            L.bo[i + 1] = (uint32_t)L.bi.size();
+        }
+        L.fo.assign(n + 1, 0);
+        L.bo.assign(n + 1, 0);
+        for (size_t i = 0; i < n; ++i) {
+            L.fo[i + 1] = L.fo[i] + (uint32_t)F[i].size();
+            L.bo[i + 1] = L.bo[i] + (uint32_t)B[i].size();
+        }
+        L.fi.resize(L.fo[n]);
+        L.bi.resize(L.bo[n]);
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)n; ++i) {
+            std::copy(F[i].begin(), F[i].end(), L.fi.begin() + L.fo[i]);
+            std::copy(B[i].begin(), B[i].end(), L.bi.begin() + L.bo[i]);
         }
     }
 
@@ -200,7 +211,9 @@ extern "C" {
    stiffness k (overriding the description's, so that central differences
    can step them). Returns the loss; when dv0 is not NULL also the gradients
    dL/dx0, dL/dv0 (n*3 each, caller order), dL/dnu and dL/dk. x_out (may be
-   NULL) receives x(T). All per-step states are kept (test sizes only). */
+   NULL) receives x(T). With a gradient every step's state and lists are
+   kept in host memory (about 100 B per particle and step); a loss-only run
+   (dv0 NULL) keeps one step. Loops run on OpenMP threads. */
 int sph_oracle_wcsph_adjoint(const sph_scene_desc* d, double nu, double k, unsigned nf, const double* x0,
                              const double* v0, unsigned nb, const double* bxyz, int nsteps, const double* target,
                              double* loss, double* x_out, double* dx0, double* dv0, double* dnu, double* dk)
@@ -234,9 +247,14 @@ int sph_oracle_wcsph_adjoint(const sph_scene_desc* d, double nu, double k, unsig
     }
 
     const size_t n = nf;
-    std::vector<std::vector<V>> xs(nsteps + 1), vs(nsteps + 1);
-    std::vector<Lists> Ls(nsteps);
-    std::vector<std::vector<double>> rhos(nsteps), ps(nsteps);
+    /* every step's state, lists, densities and pressures are kept when the
+       gradient is wanted (the backward sweep reads them newest first);
+       a loss-only run keeps one slot */
+    const bool keep = dv0 != nullptr;
+    const int slots = keep ? nsteps : 1;
+    std::vector<std::vector<V>> xs(keep ? nsteps + 1 : 2), vs(keep ? nsteps + 1 : 2);
+    std::vector<Lists> Ls(slots);
+    std::vector<std::vector<double>> rhos(slots), ps(slots);
     xs[0].resize(n);
     vs[0].resize(n);
     for (size_t i = 0; i < n; ++i) {
@@ -245,32 +263,54 @@ int sph_oracle_wcsph_adjoint(const sph_scene_desc* d, double nu, double k, unsig
     }
     std::vector<V> a;
     for (int s = 0; s < nsteps; ++s) {
-        P.lists(xs[s], Ls[s]);
-        P.density(xs[s], Ls[s], rhos[s], ps[s]);
-        P.accel(xs[s], vs[s], Ls[s], rhos[s], ps[s], a);
-        xs[s + 1].resize(n);
-        vs[s + 1].resize(n);
+        const int cur = keep ? s : 0, nxt = keep ? s + 1 : 1, slot = keep ? s : 0;
+        P.lists(xs[cur], Ls[slot]);
+        P.density(xs[cur], Ls[slot], rhos[slot], ps[slot]);
+        P.accel(xs[cur], vs[cur], Ls[slot], rhos[slot], ps[slot], a);
+        xs[nxt].resize(n);
+        vs[nxt].resize(n);
         for (size_t i = 0; i < n; ++i) {
-            vs[s + 1][i] = vs[s][i] + a[i] * P.dt;
-            xs[s + 1][i] = xs[s][i] + vs[s + 1][i] * P.dt;
+            vs[nxt][i] = vs[cur][i] + a[i] * P.dt;
+            xs[nxt][i] = xs[cur][i] + vs[nxt][i] * P.dt;
+        }
+        if (!keep) {
+            xs[0].swap(xs[1]);
+            vs[0].swap(vs[1]);
         }
     }
+    const std::vector<V>& xT = xs[keep ? nsteps : 0];
     double l = 0.0;
     std::vector<V> xb(n), vb(n);
     for (size_t i = 0; i < n; ++i) {
-        const V dd = xs[nsteps][i] - V(target[3 * i], target[3 * i + 1], target[3 * i + 2]);
+        const V dd = xT[i] - V(target[3 * i], target[3 * i + 1], target[3 * i + 2]);
         l += dot(dd, dd);
         xb[i] = dd * (2.0 / (double)n);
     }
     *loss = l / (double)n;
     if (x_out)
         for (size_t i = 0; i < n; ++i) {
-            x_out[3 * i] = xs[nsteps][i].x; x_out[3 * i + 1] = xs[nsteps][i].y; x_out[3 * i + 2] = xs[nsteps][i].z;
+            x_out[3 * i] = xT[i].x; x_out[3 * i + 1] = xT[i].y; x_out[3 * i + 2] = xT[i].z;
         }
     if (!dv0) return SPH_OK;
 
     double gnu = 0.0, gk = 0.0;
     const double eh2 = 0.01 * P.h2, m = P.mass, rho0 = P.rho0, dt = P.dt;
+    /* The scatter writes to both particles of a pair; each OpenMP thread
+       scatters into its own copy of the targets, summed after each sweep. */
+    const int T = omp_get_max_threads();
+    std::vector<std::vector<V>> txn(T, std::vector<V>(n)), tvn(T, std::vector<V>(n));
+    std::vector<std::vector<double>> tA(T, std::vector<double>(n)), tR(T, std::vector<double>(n));
+    std::vector<V> abar(n), xn(n), vn(n);
+    std::vector<double> Abar(n), Bbar(n), rbar(n);
+    auto clear = [&]() {
+#pragma omp parallel for schedule(static)
+        for (int t = 0; t < T; ++t) {
+            std::fill(txn[t].begin(), txn[t].end(), V());
+            std::fill(tvn[t].begin(), tvn[t].end(), V());
+            std::fill(tA[t].begin(), tA[t].end(), 0.0);
+            std::fill(tR[t].begin(), tR[t].end(), 0.0);
+        }
+    };
     for (int s = nsteps - 1; s >= 0; --s) {
         const std::vector<V>& x = xs[s];
         const std::vector<V>& v = vs[s];
@@ -278,69 +318,91 @@ int sph_oracle_wcsph_adjoint(const sph_scene_desc* d, double nu, double k, unsig
         const std::vector<double>& rho = rhos[s];
         const std::vector<double>& p = ps[s];
         /* x' = x + dt v', v' = v + dt a */
-        std::vector<V> abar(n), xn(n), vn(n);
         for (size_t i = 0; i < n; ++i) {
             const V vt = vb[i] + xb[i] * dt;
             abar[i] = vt * dt;
             xn[i] = xb[i];
             vn[i] = vt;
         }
-        std::vector<double> Abar(n, 0.0), Bbar(n, 0.0), rbar(n, 0.0);
+        std::fill(Bbar.begin(), Bbar.end(), 0.0);
+        clear();
         /* scatter over directed pairs (i receives from j): a_i's terms */
-        for (size_t i = 0; i < n; ++i) {
-            const double Ai = p[i] / (rho[i] * rho[i]), Bi = p[i] / (rho0 * rho0);
-            for (uint32_t kk = L.fo[i]; kk < L.fo[i + 1]; ++kk) {
-                const uint32_t j = L.fi[kk];
-                const V rr = x[i] - x[j];
-                double f, g;
-                P.K.fg(rr, f, g);
-                if (f == 0.0 && g == 0.0) continue;
-                const double Aj = p[j] / (rho[j] * rho[j]);
-                /* pressure: a_i -= m (A_i + A_j) f r */
-                const double t = m * f * dot(abar[i], rr);
-                Abar[i] -= t;
-                Abar[j] -= t;
-                const V hv = hess(f, g, rr, abar[i]) * (-m * (Ai + Aj));
-                xn[i] += hv;
-                xn[j] -= hv;
-                if (P.nu != 0.0) {
-                    /* a_i += nu (m / rho_j) phi f r, phi = (v_ij . r) / D */
-                    const V vij = v[i] - v[j];
-                    const double D = dot(rr, rr) + eh2, vr = dot(vij, rr), phi = vr / D;
-                    const V c = abar[i] * (P.nu * m / rho[j]);
-                    const double cr = dot(c, rr);
-                    const V dv = rr * (f * cr / D);
-                    vn[i] += dv;
-                    vn[j] -= dv;
-                    const V dr = (vij * cr + c * vr) * (f / D) + rr * (vr * cr * (g / D - 2.0 * f / (D * D)));
-                    xn[i] += dr;
-                    xn[j] -= dr;
-                    rbar[j] -= P.nu * m / (rho[j] * rho[j]) * phi * f * dot(abar[i], rr);
-                    gnu += (m / rho[j]) * phi * f * dot(abar[i], rr);
+#pragma omp parallel reduction(+ : gnu)
+        {
+            const int t = omp_get_thread_num();
+            V* XN = txn[t].data();
+            V* VN = tvn[t].data();
+            double* AB = tA[t].data();
+            double* RB = tR[t].data();
+#pragma omp for schedule(dynamic, 256)
+            for (long i = 0; i < (long)n; ++i) {
+                const double Ai = p[i] / (rho[i] * rho[i]), Bi = p[i] / (rho0 * rho0);
+                for (uint32_t kk = L.fo[i]; kk < L.fo[i + 1]; ++kk) {
+                    const uint32_t j = L.fi[kk];
+                    const V rr = x[i] - x[j];
+                    double f, g;
+                    P.K.fg(rr, f, g);
+                    if (f == 0.0 && g == 0.0) continue;
+                    const double Aj = p[j] / (rho[j] * rho[j]);
+                    /* pressure: a_i -= m (A_i + A_j) f r */
+                    const double tt = m * f * dot(abar[i], rr);
+                    AB[i] -= tt;
+                    AB[j] -= tt;
+                    const V hv = hess(f, g, rr, abar[i]) * (-m * (Ai + Aj));
+                    XN[i] += hv;
+                    XN[j] -= hv;
+                    if (P.nu != 0.0) {
+                        /* a_i += nu (m / rho_j) phi f r, phi = (v_ij . r) / D */
+                        const V vij = v[i] - v[j];
+                        const double D = dot(rr, rr) + eh2, vr = dot(vij, rr), phi = vr / D;
+                        const V c = abar[i] * (P.nu * m / rho[j]);
+                        const double cr = dot(c, rr);
+                        const V dv = rr * (f * cr / D);
+                        VN[i] += dv;
+                        VN[j] -= dv;
+                        const V dr = (vij * cr + c * vr) * (f / D) + rr * (vr * cr * (g / D - 2.0 * f / (D * D)));
+                        XN[i] += dr;
+                        XN[j] -= dr;
+                        RB[j] -= P.nu * m / (rho[j] * rho[j]) * phi * f * dot(abar[i], rr);
+                        gnu += (m / rho[j]) * phi * f * dot(abar[i], rr);
+                    }
                 }
-            }
-            for (uint32_t kk = L.bo[i]; kk < L.bo[i + 1]; ++kk) {
-                const uint32_t b = L.bi[kk];
-                const V rr = x[i] - P.bx[b];
-                double f, g;
-                P.K.fg(rr, f, g);
-                if (f == 0.0 && g == 0.0) continue;
-                const double t = P.psi[b] * f * dot(abar[i], rr);
-                Abar[i] -= t;
-                Bbar[i] -= t;
-                xn[i] += hess(f, g, rr, abar[i]) * (-P.psi[b] * (Ai + Bi));
-                if (P.nub != 0.0) {
-                    const double D = dot(rr, rr) + eh2, vr = dot(v[i], rr), phi = vr / D;
-                    const V c = abar[i] * (P.nub * P.psi[b] / rho[i]);
-                    const double cr = dot(c, rr);
-                    vn[i] += rr * (f * cr / D);
-                    xn[i] += (v[i] * cr + c * vr) * (f / D) + rr * (vr * cr * (g / D - 2.0 * f / (D * D)));
-                    rbar[i] -= P.nub * P.psi[b] / (rho[i] * rho[i]) * phi * f * dot(abar[i], rr);
+                for (uint32_t kk = L.bo[i]; kk < L.bo[i + 1]; ++kk) {
+                    const uint32_t b = L.bi[kk];
+                    const V rr = x[i] - P.bx[b];
+                    double f, g;
+                    P.K.fg(rr, f, g);
+                    if (f == 0.0 && g == 0.0) continue;
+                    const double tt = P.psi[b] * f * dot(abar[i], rr);
+                    AB[i] -= tt;
+                    Bbar[i] -= tt;
+                    XN[i] += hess(f, g, rr, abar[i]) * (-P.psi[b] * (Ai + Bi));
+                    if (P.nub != 0.0) {
+                        const double D = dot(rr, rr) + eh2, vr = dot(v[i], rr), phi = vr / D;
+                        const V c = abar[i] * (P.nub * P.psi[b] / rho[i]);
+                        const double cr = dot(c, rr);
+                        VN[i] += rr * (f * cr / D);
+                        XN[i] += (v[i] * cr + c * vr) * (f / D) + rr * (vr * cr * (g / D - 2.0 * f / (D * D)));
+                        RB[i] -= P.nub * P.psi[b] / (rho[i] * rho[i]) * phi * f * dot(abar[i], rr);
+                    }
                 }
             }
         }
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)n; ++i) {
+            double A = 0.0, R = 0.0;
+            for (int t = 0; t < T; ++t) {
+                A += tA[t][i];
+                R += tR[t][i];
+                xn[i] += txn[t][i];
+                vn[i] += tvn[t][i];
+            }
+            Abar[i] = A;
+            rbar[i] = R;
+        }
         /* A = p / rho^2, B = p / rho0^2, EOS */
-        for (size_t i = 0; i < n; ++i) {
+#pragma omp parallel for schedule(static) reduction(+ : gk)
+        for (long i = 0; i < (long)n; ++i) {
             const double pbar = Abar[i] / (rho[i] * rho[i]) + Bbar[i] / (rho0 * rho0);
             rbar[i] += -2.0 * p[i] * Abar[i] / (rho[i] * rho[i] * rho[i]);
             if (p[i] > 0.0) {
@@ -350,23 +412,32 @@ int sph_oracle_wcsph_adjoint(const sph_scene_desc* d, double nu, double k, unsig
             }
         }
         /* density: rho_i = sum_j m W(x_i - x_j) + sum_b psi_b W(x_i - x_b) */
-        for (size_t i = 0; i < n; ++i) {
-            for (uint32_t kk = L.fo[i]; kk < L.fo[i + 1]; ++kk) {
-                const uint32_t j = L.fi[kk];
-                const V rr = x[i] - x[j];
-                double f, g;
-                P.K.fg(rr, f, g);
-                const V gw = rr * (m * rbar[i] * f);
-                xn[i] += gw;
-                xn[j] -= gw;
-            }
-            for (uint32_t kk = L.bo[i]; kk < L.bo[i + 1]; ++kk) {
-                const V rr = x[i] - P.bx[L.bi[kk]];
-                double f, g;
-                P.K.fg(rr, f, g);
-                xn[i] += rr * (P.psi[L.bi[kk]] * rbar[i] * f);
+        clear();
+#pragma omp parallel
+        {
+            V* XN = txn[omp_get_thread_num()].data();
+#pragma omp for schedule(dynamic, 256)
+            for (long i = 0; i < (long)n; ++i) {
+                for (uint32_t kk = L.fo[i]; kk < L.fo[i + 1]; ++kk) {
+                    const uint32_t j = L.fi[kk];
+                    const V rr = x[i] - x[j];
+                    double f, g;
+                    P.K.fg(rr, f, g);
+                    const V gw = rr * (m * rbar[i] * f);
+                    XN[i] += gw;
+                    XN[j] -= gw;
+                }
+                for (uint32_t kk = L.bo[i]; kk < L.bo[i + 1]; ++kk) {
+                    const V rr = x[i] - P.bx[L.bi[kk]];
+                    double f, g;
+                    P.K.fg(rr, f, g);
+                    XN[i] += rr * (P.psi[L.bi[kk]] * rbar[i] * f);
+                }
             }
         }
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)n; ++i)
+            for (int t = 0; t < T; ++t) xn[i] += txn[t][i];
         xb.swap(xn);
         vb.swap(vn);
     }

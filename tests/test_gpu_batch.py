@@ -67,3 +67,75 @@ def test_batch_rejects_mixed_shared_parameters():
     c = Scene.from_dict(S.small(method=S.DFSPH, radius=0.03))
     with pytest.raises(Exception):
         Batch([a, c])
+
+
+# ---- batches against the reference itself ----------------------------------------------------------------------
+
+BATCH_REF_STEPS = 20
+def _c4_subset(method):
+    dicts = S.batched_scenes(256, method=method)
+    sizes = [p["dims"][0] * p["dims"][1] * p["dims"][2] for p in S.batched_scene_params(256)]
+    order = sorted(range(256), key=lambda k: sizes[k])
+    picks = [order[0], order[-1]] + [order[k] for k in (51, 102, 153, 204)]
+    return [dicts[k] for k in picks], [sizes[k] for k in picks]
+
+
+@pytest.mark.parametrize("method", [S.WCSPH, S.DFSPH], ids=["wcsph", "dfsph"])
+def test_c4_batch_scenes_against_reference(method, tmp_path):
+    """Six scenes of the 256-scene batched workload -- the smallest, the
+    largest and four quantiles of its log-uniform sizes, each with its own
+    viscosity -- stepped as one batch; every scene against the reference run
+    alone on it: iteration counts, time and dt at every step equal to the
+    FP32 reference's, final aggregates against the FP64 reference within the
+    trace bars of test_gpu_parity."""
+    from ref_runs import REF32, Reference, check_aggregates, check_trace, have_reference
+
+    if not have_reference():
+        pytest.skip("reference build missing (make -C oracle)")
+    dicts, sizes = _c4_subset(method)
+    assert min(sizes) < 3000 and max(sizes) > 35000
+    refs = []
+    for k, d in enumerate(dicts):
+        ref = Reference(d, tmp_path / f"s{k}")
+        r32 = ref.run(REF32, "step", BATCH_REF_STEPS)
+        refs.append((r32, ref.f64_from_f32_inputs(r32, "step", BATCH_REF_STEPS)))
+    scs = [Scene.from_dict(d) for d in dicts]
+    b = Batch(scs)
+    for s in range(BATCH_REF_STEPS):
+        b.step(1)
+        for k in range(len(scs)):
+            check_trace(b.scene_stats(k), refs[k][0]["step_stats"][s], f"{s} (scene {k})")
+    for k, d in enumerate(dicts):
+        x, v, r = b.scene_state(k)
+        rho0 = d["Fluid"]["FluidModel"][0]["density0"]
+        mass = rho0 * (2 * d["Configuration"]["particleRadius"]) ** 3
+        r32, r64 = refs[k]
+        check_aggregates(x, v, r, rho0, mass, r64["step_stats"][-1], r32["step_stats"][-1])
+        assert rel_err(x, r32["pos"]) <= 1e-5, k
+    b.close()
+
+
+def test_wcsph_golden_batch_against_reference_traces():
+    """The two WCSPH goldens that share every batch-wide parameter (plain
+    Akinci box tank, and OBJ-mesh boundary objects; different time steps) as
+    one batch: each scene's time at every step and its final state against
+    its golden traces from the reference's FP32 and FP64 builds."""
+    from conftest import load_golden
+    from ref_runs import check_aggregates
+
+    names = ["wcsph_artificial", "geometry_wcsph_quirks"]
+    gs = [load_golden(n) for n in names]
+    scs = [Scene.from_dict(g["scene"]) for g in gs]
+    b = Batch(scs)
+    steps = min(g["trace_f32"].shape[0] for g in gs)
+    for s in range(steps):
+        b.step(1)
+        for k, g in enumerate(gs):
+            st = b.scene_stats(k)
+            assert abs(st["time"] - g["trace_f32"][s, 0]) <= 1e-5 * g["trace_f32"][s, 0], (names[k], s)
+    for k, g in enumerate(gs):
+        x, v, r = b.scene_state(k)
+        rho0 = g["scene"]["Fluid"]["FluidModel"][0]["density0"]
+        mass = rho0 * (2 * g["scene"]["Configuration"]["particleRadius"]) ** 3
+        check_aggregates(x, v, r, rho0, mass, g["trace_f64"][steps - 1], g["trace_f32"][steps - 1])
+    b.close()
