@@ -1,10 +1,13 @@
 """GPU WCSPH adjoint (sph_wcsph_forward / sph_wcsph_backward) against the
 FP64 CPU adjoint of the oracle (pinned by test_oracle_adjoint.py) and FP64
-central differences, plus size-independent properties at the full
-32,768-particle, 500-step workload.
+central differences: on 720-particle scenes over 40 steps, and at the full
+differentiable workload (32,768 particles, 500 steps, checkpoint every 50),
+where the FP64 adjoint is first pinned to converged central differences.
 
 Tolerances: the GPU runs in FP32, the oracle in FP64; gradients agree within
-1e-3 relative (norm-wise for vectors), the bar the adjoint is built to."""
+1e-3 relative (norm-wise for vectors), the bar the adjoint is built to -- at
+the full workload, or within 3x the FP64 gradient's own change under
+FP32-level rounding of its inputs where that is larger."""
 import numpy as np
 import pytest
 
@@ -157,30 +160,107 @@ def test_unsupported_configurations_rejected():
     sim.close()
 
 
-def test_full_size_32k_500_steps():
-    """The differentiable workload at full size: 32,768 particles, 500 steps,
-    checkpoint every 50. Properties: finite gradients; checkpoint interval
-    50 and 100 give bit-identical gradients; a small step against the
-    gradient lowers the loss by about the first-order prediction."""
+FULL_STEPS = 500
+
+
+@pytest.fixture(scope="module")
+def full():
+    """The differentiable workload at full size (32,768 particles, 500 steps
+    at dt = 2e-4, checkpoint every 50): the GPU's loss and gradients, the
+    FP64 CPU adjoint of the same inputs, and the FP64 adjoint of the inputs
+    perturbed at FP32 rounding level (relative 6e-8, seeded) -- the
+    problem's own conditioning, which bounds how close any FP32
+    implementation can come to FP64."""
     sc = Scene.from_dict(S.adjoint_wcsph_32k())
+    desc = sc.desc()
     x0, _ = sc.fluid()
     b = sc.boundary()
     v0, t = S.adjoint_problem(x0)
-    sim = Simulation(sc.desc(), x0, b, vel=v0)
-    loss = sim.wcsph_forward(500, t, ckpt_every=50)
+    sim = Simulation(desc, x0, b, vel=v0)
+    loss = sim.wcsph_forward(FULL_STEPS, t, ckpt_every=50)
     g = sim.wcsph_backward()
     sim.close()
-    assert np.all(np.isfinite(g["v0"])) and np.isfinite(g["viscosity"]) and np.isfinite(g["stiffness"])
-    sim = Simulation(sc.desc(), x0, b, vel=v0)
-    loss2 = sim.wcsph_forward(500, t, ckpt_every=100)
+    ref = wcsph_adjoint(desc, x0, v0, b, FULL_STEPS, t)
+    rng = np.random.default_rng(7)
+    x1 = x0.astype(np.float64) * (1 + 6e-8 * rng.uniform(-1, 1, x0.shape))
+    v1 = v0.astype(np.float64) * (1 + 6e-8 * rng.uniform(-1, 1, v0.shape))
+    pert = wcsph_adjoint(desc, x1, v1, b, FULL_STEPS, t)
+    cond = {"v0": rel_norm(pert["v0"], ref["v0"]),
+            "viscosity": abs(pert["viscosity"] - ref["viscosity"]) / abs(ref["viscosity"]),
+            "stiffness": abs(pert["stiffness"] - ref["stiffness"]) / abs(ref["stiffness"])}
+    print("FP64 gradient change under FP32-level input rounding:", cond)
+    return desc, sc, x0, v0, b, t, loss, g, ref, cond
+
+
+def test_full_size_fp64_adjoint_equals_converged_central_differences(full):
+    """The FP64 CPU adjoint is the derivative of the FP64 forward map at the
+    full workload: central differences along three seeded directions of v0
+    (eps = 1e-7) and of the viscosity and stiffness (eps = 1e-6 relative)
+    agree within 1e-3. (At eps = 1e-4 they do not converge: over 500 steps
+    thousands of particles cross the Tait EOS clamp p = max(0, .) and pairs
+    cross the spline's joins, so the loss is only piecewise smooth at that
+    scale -- 1.5e-2 and 1.8e-1 off for two of the directions, converging as
+    eps shrinks.)"""
+    desc, sc, x0, v0, b, t, loss, g, ref, cond = full
+    v = v0.astype(np.float64)
+    for k in range(3):
+        d = np.random.default_rng(100 + k).normal(size=x0.shape)
+        eps = 1e-7
+        lp = wcsph_adjoint(desc, x0, v + eps * d, b, FULL_STEPS, t, grad=False)["loss"]
+        lm = wcsph_adjoint(desc, x0, v - eps * d, b, FULL_STEPS, t, grad=False)["loss"]
+        fd = (lp - lm) / (2 * eps)
+        ad = float(np.sum(ref["v0"] * d))
+        assert abs(ad - fd) <= TOL * abs(fd), (k, ad, fd)
+    for name, key in (("viscosity", "nu"), ("stiffness", "k")):
+        val = float(getattr(desc, name))
+        e = 1e-6 * val
+        lp = wcsph_adjoint(desc, x0, v, b, FULL_STEPS, t, grad=False, **{key: val + e})["loss"]
+        lm = wcsph_adjoint(desc, x0, v, b, FULL_STEPS, t, grad=False, **{key: val - e})["loss"]
+        fd = (lp - lm) / (2 * e)
+        assert abs(ref[name] - fd) <= TOL * abs(fd), (name, ref[name], fd)
+
+
+def test_full_size_gpu_gradients_against_fp64(full):
+    """GPU (FP32) loss and gradients against the FP64 adjoint at the full
+    workload. Bar: 1e-3 relative, or 3x the FP64 gradient's own change
+    under FP32-level rounding of its inputs where that is larger (measured
+    in the fixture: about 1.4e-3 for dL/dv0 and 2.7e-3 for dL/dstiffness),
+    since no FP32 run can resolve the gradient more finely than its inputs'
+    rounding moves it. Directional derivatives along three seeded
+    directions are held to the v0 bar relative to |g| |d| / sqrt(3N)."""
+    desc, sc, x0, v0, b, t, loss, g, ref, cond = full
+    assert abs(loss - ref["loss"]) <= 1e-5 * ref["loss"], (loss, ref["loss"])
+    gv = g["v0"].astype(np.float64)
+    assert np.all(np.isfinite(gv))
+    bar = {k: max(TOL, 3.0 * c) for k, c in cond.items()}
+    got = {"v0": rel_norm(gv, ref["v0"]),
+           "viscosity": abs(g["viscosity"] - ref["viscosity"]) / abs(ref["viscosity"]),
+           "stiffness": abs(g["stiffness"] - ref["stiffness"]) / abs(ref["stiffness"])}
+    print("GPU vs FP64 adjoint:", got, "bars:", bar)
+    for k in got:
+        assert got[k] <= bar[k], (k, got[k], bar[k])
+    scale = np.linalg.norm(ref["v0"]) / np.sqrt(ref["v0"].size)
+    for k in range(3):
+        d = np.random.default_rng(100 + k).normal(size=x0.shape)
+        err = abs(float(np.sum(gv * d)) - float(np.sum(ref["v0"] * d)))
+        assert err <= bar["v0"] * scale * np.linalg.norm(d), (k, err)
+
+
+def test_full_size_checkpointing_and_descent(full):
+    """Checkpoint interval 50 and 100 give bit-identical gradients; a small
+    step against the gradient lowers the loss by about the first-order
+    prediction."""
+    desc, sc, x0, v0, b, t, loss, g, ref, cond = full
+    sim = Simulation(desc, x0, b, vel=v0)
+    loss2 = sim.wcsph_forward(FULL_STEPS, t, ckpt_every=100)
     g2 = sim.wcsph_backward()
     sim.close()
     assert loss == loss2 and np.array_equal(g["v0"], g2["v0"])
     gv = g["v0"].astype(np.float64)
     gn = float(np.linalg.norm(gv))
     alpha = 0.01 / gn  # move v0 by 0.01 m/s (norm) against the gradient
-    sim = Simulation(sc.desc(), x0, b, vel=(v0 - alpha * gv).astype(np.float32))
-    lower = sim.wcsph_forward(500, t, ckpt_every=500)
+    sim = Simulation(desc, x0, b, vel=(v0 - alpha * gv).astype(np.float32))
+    lower = sim.wcsph_forward(FULL_STEPS, t, ckpt_every=FULL_STEPS)
     sim.close()
     predicted = alpha * gn * gn
     assert lower < loss
