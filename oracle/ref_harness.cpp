@@ -15,9 +15,22 @@
  * PCISPHSolver::avgDensityError (read by pressureSolver, PCISPHSolver.cpp:374).
  *
  * Usage:
- *   sph2o_ref -c scene.json --mode step|neighbors|phases|time
+ *   sph2o_ref -c scene.json --mode step|neighbors|phases|time|frames
  *             [--steps N] [--warmup W] [--out file.sphd]
  *             [--state-in file.sphd] [--boundary-in file.sphd] [--threads T]
+ *             [--gpu]
+ *
+ * --mode frames turns saving on and calls SPHSimulation::step() N times, so
+ * the reference itself decides when to save (TimeHelper::hasToSave) and
+ * writes <scene>_NNNN.json with SceneLoader::writeFluid
+ * (SPHSimulation.cpp:179-187, SceneLoader.cpp:211-275).
+ *
+ * --gpu (only in the sph2o_ref_gpu build, compiled with SPH2O_HARNESS_GPU and
+ * linked with libsph2o_cuda.so) installs the reference-side binding
+ * include/sph2o_gpu_solver.hpp: after the scene is imported, the configured
+ * CPU solver is handed to a GPUSolver that replaces it, as a maintainer
+ * would do in SPHSimulation::init(); SPHSimulation::init/step and
+ * writeFluid then run unchanged around the GPU step.
  *
  * Output (.sphd): "SPHD0001", then records
  *   u32 name_len, name, char dtype ('f' f32, 'd' f64, 'i' i32, 'u' u32),
@@ -34,6 +47,9 @@
 #include "json/json.hpp"
 
 #include "../sph2o_b200/host/scene_rng.h"
+#ifdef SPH2O_HARNESS_GPU
+#include "sph2o_gpu_solver.hpp"
+#endif
 
 #include <omp.h>
 #include <cstdio>
@@ -55,6 +71,10 @@ struct DFAccess : DFSPHSolver {
 };
 struct PCIAccess : PCISPHSolver {
     static Real& avgDens(PCISPHSolver* s) { return s->*(&PCIAccess::avgDensityError); }
+};
+/* The simulation's solver slot (to install the GPU binding without editing SPH2O). */
+struct SimAccess : SPHSimulation {
+    static SPHSolver*& slot(SPHSimulation* s) { return s->*(&SimAccess::solver); }
 };
 /* Normals of PCISPH boundary particles (a protected member without a getter). */
 struct PCIBoundaryAccess : PCISPHBoundaryObject {
@@ -139,6 +159,7 @@ private:
 struct Opts {
     std::string scene, mode = "step", out, state_in, boundary_in;
     int steps = 1, warmup = 0, threads = 0;
+    bool gpu = false;
 };
 
 Opts parse(int argc, char** argv)
@@ -158,6 +179,7 @@ Opts parse(int argc, char** argv)
         else if (a == "--state-in") o.state_in = next();
         else if (a == "--boundary-in") o.boundary_in = next();
         else if (a == "--threads") o.threads = std::atoi(next().c_str());
+        else if (a == "--gpu") o.gpu = true;
         else { fprintf(stderr, "unknown option %s\n", a.c_str()); exit(2); }
     }
     if (o.scene.empty()) { fprintf(stderr, "-c scene.json is required\n"); exit(2); }
@@ -342,18 +364,50 @@ int main(int argc, char** argv)
 
     FluidObject* fo = sim->getFluidModel(0);
     std::vector<Real> init_pos = fluid_vec3(fo, 0), init_vel = fluid_vec3(fo, 1);
-
-    sim->init();
-    SPHSolver* solver = sim->getSolver();
     const int method = sim->getSimulationMethod();
-    if (method == SPHSimulation::DFSPH_METHOD) DFAccess::itsV(static_cast<DFSPHSolver*>(solver)) = 0;
-    if (method == SPHSimulation::PCISPH_METHOD) PCIAccess::avgDens(static_cast<PCISPHSolver*>(solver)) = 0;
+
+#ifdef SPH2O_HARNESS_GPU
+    GPUSolver* gpu = nullptr;
+    if (o.gpu) {
+        gpu = new GPUSolver(sim->getSolver());
+        SimAccess::slot(sim) = gpu;
+    }
+#else
+    if (o.gpu) { fprintf(stderr, "--gpu needs the sph2o_ref_gpu build\n"); return 2; }
+#endif
+    if (o.mode == "frames") sim->activateSave(true);
+    try {
+        sim->init();
+    } catch (const std::exception& e) {
+        fprintf(stderr, "%s\n", e.what());
+        return 3;
+    }
+    SPHSolver* solver = sim->getSolver();
+    if (!o.gpu && method == SPHSimulation::DFSPH_METHOD) DFAccess::itsV(static_cast<DFSPHSolver*>(solver)) = 0;
+    if (!o.gpu && method == SPHSimulation::PCISPH_METHOD) PCIAccess::avgDens(static_cast<PCISPHSolver*>(solver)) = 0;
+    /* after a GPU step the fluid object's arrays are refreshed on demand */
+    auto refresh = [&]() {
+#ifdef SPH2O_HARNESS_GPU
+        if (gpu) gpu->pull();
+#endif
+    };
+
+    if (o.mode == "frames") {
+        for (int s = 0; s < o.steps; ++s) sim->step();
+        printf("{\"steps\": %d, \"frames_written\": %u, \"time\": %.9g}\n", o.steps, sim->getFrame() - 1,
+               (double)sim->getTime());
+        return 0;
+    }
 
     const uint64_t n = fo->getSize();
     std::vector<Real> bpos, bvol;
     boundary_arrays(sim, bpos, bvol);
     const uint64_t nb = bpos.size() / 3;
 
+    if (o.gpu && o.mode != "time" && o.mode != "step") {
+        fprintf(stderr, "--gpu supports the step, time and frames modes\n");
+        return 2;
+    }
     if (o.mode == "time") {
         for (int s = 0; s < o.warmup; ++s) sim->step();
         const double t0 = omp_get_wtime();
@@ -436,11 +490,14 @@ int main(int argc, char** argv)
     std::vector<double> stats, active;
     for (int s = 0; s < o.steps; ++s) {
         sim->step();
+        refresh();
         active.push_back((double)fo->getNumActiveParticles());
         double agg[5];
         aggregates(sim, agg);
         double avg = 0, avgv = 0, itv = 0;
-        if (method == SPHSimulation::DFSPH_METHOD) {
+        if (o.gpu) {
+            /* the GPU binding reports iterations through SPHSolver's counter only */
+        } else if (method == SPHSimulation::DFSPH_METHOD) {
             DFSPHSolver* df = static_cast<DFSPHSolver*>(solver);
             avg = DFAccess::avgDens(df); avgv = DFAccess::avgDiv(df); itv = DFAccess::itsV(df);
         } else if (method == SPHSimulation::PCISPH_METHOD) {
