@@ -308,11 +308,11 @@ def physical_cores():
     return max(1, len(cores))
 
 
-def reference_run(scene_dict, steps, warmup, threads=None, state=None):
+def reference_run(scene_dict, steps, warmup, threads=None, state=None, dt=None):
     """Time SPH2O's OpenMP CPU path on this host for the given scene: one
     OpenMP thread per physical core (OMP_PLACES=cores, OMP_PROC_BIND=close).
     `state` = (positions, velocities) replaces the scene's initial fluid
-    state (caller order)."""
+    state (caller order); `dt` the initial time step."""
     if not os.path.exists(REF_BIN):
         return None, "reference build missing (oracle/_ref/sph2o_ref_fast; run make -C oracle)"
     threads = threads or physical_cores()
@@ -328,6 +328,8 @@ def reference_run(scene_dict, steps, warmup, threads=None, state=None):
             sp = os.path.join(td, "state.sphd")
             sphd.write(sp, {"pos": np.asarray(state[0], np.float32), "vel": np.asarray(state[1], np.float32)})
             cmd += ["--state-in", sp]
+        if dt is not None:
+            cmd += ["--dt-in", repr(float(dt))]
         r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
     if r.returncode != 0:
         return None, f"reference run failed: {r.stderr.strip()[-200:]}"
@@ -493,8 +495,8 @@ def config_run(name, steps, warmup, cpu=True, cpu_window=None):
 def later_window_run(scene_dict, desc, start, steps, cpu=True, cpu_steps=5, cpu_warmup=3):
     """The same scene later in the run: steps start + 1 .. start + steps (the
     first `start` steps untimed). The CPU reference starts from the GPU's
-    state after step `start` (positions and velocities; its adaptive time
-    step restarts from the scene's), takes a few warm-up steps, then a
+    state after step `start` (positions, velocities and time step; its
+    solver warm start begins empty), takes a few warm-up steps, then a
     bounded sample."""
     from sph2o_b200.api import Scene, Simulation
     scene = Scene.from_dict(scene_dict)
@@ -502,6 +504,7 @@ def later_window_run(scene_dict, desc, start, steps, cpu=True, cpu_steps=5, cpu_
     nf = sim.nf
     sim.step(start)
     x, v, _ = sim.state()
+    _, dt_start = sim.time()
     st = sim.step(steps)
     sim.close()
     scene.close()
@@ -511,7 +514,7 @@ def later_window_run(scene_dict, desc, start, steps, cpu=True, cpu_steps=5, cpu_
            "mean_iterations_v": st["total_iterations_v"] / steps, "last_avg_density_error": st["avg_density_error"],
            "density_error_gate": bool(st["avg_density_error"] <= 1e-3), "simulated_time_s": st["time"]}
     if cpu:
-        res, err = reference_run(scene_dict, cpu_steps, cpu_warmup, state=(x, v))
+        res, err = reference_run(scene_dict, cpu_steps, cpu_warmup, state=(x, v), dt=dt_start)
         out["cpu_baseline"] = cpu_baseline_entry(res, err, f"the same scene from the GPU state after step {start}")
         if res is not None:
             out["vs_cpu_baseline"] = out["value"] / res["particle_steps_per_s"]
@@ -629,8 +632,7 @@ def main():
                         f"launch")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "traffic_note": traffic_note, "kernel": dom, "peak_kind": f"of {peak_kind}",
-                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": avg_ms,
-                "neighbor_search": neighbor_search_roofline(sim, prof, args.steps, peak, peak_kind)}
+                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": avg_ms}
 
     # End to end through the C ABI with host buffers, over the same window:
     # the state entering it is uploaded from pinned host memory, every step
@@ -662,6 +664,8 @@ def main():
                "steps": ke, "mean_iterations": e2e_its / ke,
                "note": "state uploaded once from pinned host memory, per-step statistics read back by every "
                        "sph_step call, final state (x, v, rho) read back; same window as value"}
+    # list lengths for the neighbour-search bytes (read after the timed runs)
+    roofline["neighbor_search"] = neighbor_search_roofline(sim, prof, args.steps, peak, peak_kind)
     sim.close()
     scene.close()
 

@@ -18,7 +18,7 @@
  *   sph2o_ref -c scene.json --mode step|neighbors|phases|time|frames
  *             [--steps N] [--warmup W] [--out file.sphd]
  *             [--state-in file.sphd] [--boundary-in file.sphd] [--threads T]
- *             [--gpu]
+ *             [--dt-in dt] [--gpu]
  *
  * --mode frames turns saving on and calls SPHSimulation::step() N times, so
  * the reference itself decides when to save (TimeHelper::hasToSave) and
@@ -160,6 +160,7 @@ struct Opts {
     std::string scene, mode = "step", out, state_in, boundary_in;
     int steps = 1, warmup = 0, threads = 0;
     bool gpu = false;
+    double dt_in = 0.0;
 };
 
 Opts parse(int argc, char** argv)
@@ -180,6 +181,7 @@ Opts parse(int argc, char** argv)
         else if (a == "--boundary-in") o.boundary_in = next();
         else if (a == "--threads") o.threads = std::atoi(next().c_str());
         else if (a == "--gpu") o.gpu = true;
+        else if (a == "--dt-in") o.dt_in = std::atof(next().c_str());
         else { fprintf(stderr, "unknown option %s\n", a.c_str()); exit(2); }
     }
     if (o.scene.empty()) { fprintf(stderr, "-c scene.json is required\n"); exit(2); }
@@ -360,6 +362,9 @@ int main(int argc, char** argv)
     if (sim->numberFluidModels() != 1) { fprintf(stderr, "harness expects one fluid model\n"); return 2; }
     apply_jitter(sim, o.scene);
     if (!o.state_in.empty()) load_state(sim, o.state_in);
+    /* a run resumed from another run's state continues with its time step
+       (DFSPH adapts it from the previous one, DFSPHSolver.cpp:1090-1162) */
+    if (o.dt_in > 0.0) sim->setTimeStep((Real)o.dt_in);
     if (!o.boundary_in.empty()) load_boundary(sim, o.boundary_in);
 
     FluidObject* fo = sim->getFluidModel(0);

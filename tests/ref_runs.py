@@ -26,6 +26,7 @@ class Reference:
 
     def __init__(self, scene, workdir):
         self.dir = str(workdir)
+        os.makedirs(self.dir, exist_ok=True)
         self.scene = os.path.join(self.dir, "scene.json")
         with open(self.scene, "w") as f:
             json.dump(scene, f)
