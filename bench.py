@@ -641,20 +641,33 @@ def main():
     from sph2o_b200.api import StepStats, _fptr, lib
     L = lib()
     ke = args.steps
+    x_in, v_in = px.copy(), pv.copy()
+
+    def api_window():
+        """The caller's sequence: upload, ke single steps with their
+        statistics, read back. Returns (status, iterations)."""
+        px[:] = x_in
+        pv[:] = v_in
+        rc = L.sph_set_state(sim._h, _fptr(px), _fptr(pv))
+        rc = rc or L.sph_set_time(sim._h, t_w, dt_w)
+        its_sum = 0
+        st1 = StepStats()
+        for _ in range(ke):
+            if rc:
+                break
+            rc = L.sph_step(sim._h, 1, st1)
+            its_sum += st1.total_iterations
+        rc = rc or L.sph_get_state(sim._h, _fptr(px), _fptr(pv), _fptr(pr))
+        return rc, its_sum
+
+    # untimed once: the library captures its one-step CUDA graphs (one per
+    # buffer assignment the single steps pass through) on first use
+    api_window()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    rc = L.sph_set_state(sim._h, _fptr(px), _fptr(pv))
-    rc = rc or L.sph_set_time(sim._h, t_w, dt_w)
-    e2e_its = 0
-    st1 = StepStats()
-    for _ in range(ke):
-        if rc:
-            break
-        rc = L.sph_step(sim._h, 1, st1)
-        e2e_its += st1.total_iterations
-    rc = rc or L.sph_get_state(sim._h, _fptr(px), _fptr(pv), _fptr(pr))
+    rc, e2e_its = api_window()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
     e2e = None
     if rc == 0:
@@ -663,7 +676,8 @@ def main():
                "d2h_bytes_per_step": ctypes.sizeof(StepStats) + (nf * 28) // ke,
                "steps": ke, "mean_iterations": e2e_its / ke,
                "note": "state uploaded once from pinned host memory, per-step statistics read back by every "
-                       "sph_step call, final state (x, v, rho) read back; same window as value"}
+                       "sph_step call, final state (x, v, rho) read back; same window as value, after one "
+                       "untimed pass of the same calls (one-step graph capture)"}
     # list lengths for the neighbour-search bytes (read after the timed runs)
     roofline["neighbor_search"] = neighbor_search_roofline(sim, prof, args.steps, peak, peak_kind)
     sim.close()

@@ -153,6 +153,7 @@ public:
                 d.adhesion = (float)ad->getAdhesionCoef();
             }
         }
+        desc_ = d;
         if (sph_create(&d, &ctx_) != SPH_OK) fail(sph_global_error());
 
         const uint n = f->getSize();
@@ -205,6 +206,9 @@ public:
     }
 
     sph_ctx* context() { return ctx_; }
+    /* The description init() built from the simulation (valid once init()
+       has read the parameters, even if the context could not be created). */
+    const sph_scene_desc& description() const { return desc_; }
 
 private:
     /* TimeHelper::hasToSave's test, evaluated without its side effect: the
@@ -226,6 +230,7 @@ private:
 
     SPHSolver* cpu_ = nullptr;
     sph_ctx* ctx_ = nullptr;
+    sph_scene_desc desc_{};
     uint n_ = 0;
 };
 

@@ -385,6 +385,18 @@ int main(int argc, char** argv)
         sim->init();
     } catch (const std::exception& e) {
         fprintf(stderr, "%s\n", e.what());
+#ifdef SPH2O_HARNESS_GPU
+        if (gpu) { /* the description the binding read from SPH2O, as 32-bit words */
+            const sph_scene_desc& d = gpu->description();
+            const unsigned char* p = reinterpret_cast<const unsigned char*>(&d);
+            for (size_t k = 0; k < sizeof(d); k += 4) {
+                uint32_t w;
+                std::memcpy(&w, p + k, 4);
+                fprintf(stderr, "%08x%c", w, (k / 4) % 8 == 7 ? '\n' : ' ');
+            }
+            fprintf(stderr, "\n");
+        }
+#endif
         return 3;
     }
     SPHSolver* solver = sim->getSolver();

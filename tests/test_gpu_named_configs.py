@@ -37,26 +37,13 @@ import numpy as np
 import pytest
 
 from conftest import rel_err
-from ref_runs import REF32, REF64, Reference, check_aggregates, check_trace, have_reference
+from ref_runs import REF32, REF64, Reference, check_aggregates, check_state_vs_f64, check_trace, have_reference
 from sph2o_b200 import api
 from sph2o_b200 import scenes as S
 from sph2o_b200.api import Scene, Simulation
 
 pytestmark = pytest.mark.gpu
 need_ref = pytest.mark.skipif(not have_reference(), reason="reference build missing (make -C oracle)")
-
-
-def check_state_vs_f64(x, v, r32, r64):
-    """State after several steps: no further from the FP64 reference than
-    1.5x the FP32 reference's own distance from it (or 1e-5), positions and
-    velocities norm-wise. After one step the FP32 bars hold; over several
-    steps the solvers' FP32 round-off (residuals of a difference of two
-    ~1000 densities) grows in both FP32 implementations alike."""
-    ex, ev = rel_err(r32["pos"], r64["pos"]), rel_err(r32["vel"], r64["vel"])
-    gx, gv = rel_err(x, r64["pos"]), rel_err(v, r64["vel"])
-    print(f"positions: GPU-FP64 {gx:.3g}, FP32 ref-FP64 {ex:.3g}; velocities: GPU-FP64 {gv:.3g}, FP32 ref-FP64 {ev:.3g}")
-    assert gx <= max(1e-5, 1.5 * ex), (gx, ex)
-    assert gv <= max(1e-5, 1.5 * ev), (gv, ev)
 
 
 # ---- C3: 1,000,000 particles, DFSPH --------------------------------------------------------------------------
