@@ -411,8 +411,12 @@ int main(int argc, char** argv)
 
     if (o.mode == "frames") {
         for (int s = 0; s < o.steps; ++s) sim->step();
-        printf("{\"steps\": %d, \"frames_written\": %u, \"time\": %.9g}\n", o.steps, sim->getFrame() - 1,
-               (double)sim->getTime());
+        bool on_gpu = false;
+#ifdef SPH2O_HARNESS_GPU
+        on_gpu = gpu != nullptr && sim->getSolver() == gpu;
+#endif
+        printf("{\"steps\": %d, \"frames_written\": %u, \"time\": %.9g, \"gpu_solver\": %s}\n", o.steps,
+               sim->getFrame() - 1, (double)sim->getTime(), on_gpu ? "true" : "false");
         return 0;
     }
 

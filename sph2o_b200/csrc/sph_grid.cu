@@ -21,6 +21,7 @@
  * (src/SPH2O/BoundaryObject/AkinciBoundaryObject.cpp:10-34) runs on it.
  */
 #include "sph_device.cuh"
+#include "sph_grid_body.cuh"
 #include "sph_internal.h"
 
 namespace sph {
@@ -31,9 +32,7 @@ __global__ void __launch_bounds__(256) k_ns_count(SimParams P, SceneRef S, int n
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (n_dev ? (int)*n_dev : n)) return;
-    const unsigned c = cell_index(pos[i], P.h, grid_for(P, S, (unsigned)i));
-    cell_of[i] = c;
-    slot[i] = atomicAdd(&cell_count[c], 1u);
+    ns_count_at(P, S, i, pos, cell_count, cell_of, slot);
 }
 
 /* Exclusive scan, phase 1: each 1024-thread block scans 4096 populations,
@@ -125,9 +124,7 @@ __global__ void __launch_bounds__(256) k_ns_scatter(int n, const unsigned* n_dev
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (n_dev ? (int)*n_dev : n)) return;
-    const unsigned p = cell_start[cell_of[i]] + slot[i];
-    tmp_key[p] = orig[i];
-    tmp_src[p] = (unsigned)i;
+    ns_scatter_at(i, cell_of, slot, cell_start, orig, tmp_key, tmp_src);
 }
 
 /* Rank inside the cell by caller-order id, then move the carried state. */
@@ -138,21 +135,7 @@ __global__ void __launch_bounds__(256) k_ns_rank_gather(int n, const unsigned* _
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= (g.n_dev ? (int)*g.n_dev : n)) return;
-    const unsigned src = tmp_src[p];
-    const unsigned c = cell_of[src];
-    const unsigned key = tmp_key[p];
-    const unsigned s = cell_start[c], e = cell_start[c + 1];
-    unsigned rank = 0;
-    for (unsigned q = s; q < e; ++q) rank += tmp_key[q] < key ? 1u : 0u;
-    const unsigned dst = s + rank;
-    g.orig_out[dst] = key;
-    if (g.cell_out) g.cell_out[dst] = c;
-    if (g.v4_in[0]) g.v4_out[0][dst] = g.v4_in[0][src];
-    if (g.v4_in[1]) g.v4_out[1][dst] = g.v4_in[1][src];
-    if (g.v4_in[2]) g.v4_out[2][dst] = g.v4_in[2][src];
-    if (g.v4_in[3]) g.v4_out[3][dst] = g.v4_in[3][src];
-    if (g.f_in[0]) g.f_out[0][dst] = g.f_in[0][src];
-    if (g.f_in[1]) g.f_out[1][dst] = g.f_in[1][src];
+    ns_rank_gather_at(p, cell_of, cell_start, tmp_key, tmp_src, g);
 }
 
 /* Neighbour lists in the reference's candidate order, filtered at |r| <= h. */
@@ -197,43 +180,6 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
     }
 }
 
-/* The same lists for small scenes, one warp per particle: lane k < 27 loads
-   the range of the particle's k-th cell (the reference's offset order), a
-   warp scan lays the 27 ranges end to end, and the warp then tests the
-   concatenated candidates 32 at a time; a ballot ranks each round's accepted
-   candidates, so entries are written in candidate order. The serial walk of a
-   particle shrinks from ~216 candidates (or 27 cells) to ~7 rounds. */
-__device__ __forceinline__ void warp_candidates(const float4* __restrict__ xs, unsigned s, unsigned e, float4 xi,
-                                                float s2max, unsigned lane, unsigned cap, unsigned* __restrict__ list,
-                                                size_t nf, int i, unsigned& n)
-{
-    const unsigned cnt = e - s;
-    unsigned incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (unsigned)o) incl += v;
-    }
-    const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
-    const unsigned excl = incl - cnt;
-    for (unsigned u0 = 0; u0 < total; u0 += 32) {
-        const unsigned u = min(u0 + lane, total - 1u);
-        /* cell of candidate u: the number of lanes whose ranges end at or before u */
-        unsigned k = 0;
-#pragma unroll
-        for (unsigned step = 16; step >= 1; step >>= 1)
-            if (__shfl_sync(0xffffffffu, incl, k + step - 1) <= u) k += step;
-        const unsigned q = __shfl_sync(0xffffffffu, s, k) + (u - __shfl_sync(0xffffffffu, excl, k));
-        const bool in = u0 + lane < total && dist2_exact(xi, xs[q]) <= s2max;
-        const unsigned bits = __ballot_sync(0xffffffffu, in);
-        if (in) {
-            const unsigned r = n + __popc(bits & ((1u << lane) - 1u));
-            if (r < cap) __stcs(list + (size_t)r * nf + i, q);
-        }
-        n += __popc(bits);
-    }
-}
-
 __global__ void __launch_bounds__(128) k_ns_build_lists_warp(SimParams P, SceneRef S,
                                                              const float4* __restrict__ pos,
                                                              const unsigned* __restrict__ cell_start,
@@ -246,35 +192,7 @@ __global__ void __launch_bounds__(128) k_ns_build_lists_warp(SimParams P, SceneR
     const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     /* the whole warp shares i and leaves together */
     if (i >= active_n(P, st)) return;
-    const unsigned lane = threadIdx.x & 31u;
-    const float4 xi = pos[i];
-    const Grid g = grid_for(P, S, (unsigned)i);
-    unsigned s = 0, e = 0, bs = 0, be = 0;
-    if (lane < 27) {
-        const int xx = cell_coord(xi.x, P.h, g.cminx, g.dimx) + (int)lane / 9 - 1;
-        const int yy = cell_coord(xi.y, P.h, g.cminy, g.dimy) + ((int)lane / 3) % 3 - 1;
-        const int zz = cell_coord(xi.z, P.h, g.cminz, g.dimz) + (int)lane % 3 - 1;
-        if (xx >= 0 && xx < g.dimx && yy >= 0 && yy < g.dimy && zz >= 0 && zz < g.dimz) {
-            const unsigned c = brick_morton(xx, yy, zz, g);
-            s = cell_start[c];
-            e = cell_start[c + 1];
-            if (P.nb > 0) {
-                bs = bcell_start[c];
-                be = bcell_start[c + 1];
-            }
-        }
-    }
-    const size_t nf = (size_t)P.nf;
-    unsigned nF = 0, nB = 0;
-    warp_candidates(pos, s, e, xi, P.h2_exact, lane, P.capF, nbr_f, nf, i, nF);
-    if (P.nb > 0) warp_candidates(bpos, bs, be, xi, P.h2_exact, lane, P.capB, nbr_b, nf, i, nB);
-    if (lane != 0) return;
-    cnt_f[i] = min(nF, P.capF);
-    cnt_b[i] = min(nB, P.capB);
-    if (nF > P.capF || nB > P.capB) {
-        atomicAdd(&st->overflow, 1u);
-        atomicOr(&st->err, ERRBIT_OVERFLOW);
-    }
+    build_lists_warp_at(P, S, i, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f, nbr_b, cnt_b, st);
 }
 
 /* Akinci boundary volume V_b = 1 / sum_b' W(x_b - x_b') over the 27 cells

@@ -11,21 +11,10 @@
 #include <cuda_runtime.h>
 
 #include "sph_device.cuh"
+#include "sph_grid_body.cuh"
 
 namespace sph {
 
-/* Arrays moved by the rank/gather step of the sort (NULL entries skipped).
-   n_dev (may be NULL): device count of the particles to sort, read by the
-   kernels in place of n (the fluid's active count when emitters add to it). */
-struct GatherSet {
-    const unsigned* n_dev;
-    unsigned* orig_out;
-    unsigned* cell_out;
-    const float4* v4_in[4];
-    float4* v4_out[4];
-    const float* f_in[2];
-    float* f_out[2];
-};
 
 /* Device pointers of one scene, handed to the solver launchers. */
 struct DeviceArrays {

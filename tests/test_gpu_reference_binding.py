@@ -11,10 +11,14 @@ the GPU step. Checks:
   * frames: the reference's own run (TimeHelper::hasToSave +
     SceneLoader::writeFluid), the binding inside SPH2O, and this
     repository's driver (sph2o -o true) write the same frame files (names
-    and count); the binding's and the driver's frames are identical; against
-    the reference's frames they are bit-exact for WCSPH, and within the
-    one-step bars of test_gpu_parity for DFSPH (1e-5 positions, 2e-4
-    velocities, 1e-5 time and time step).
+    and count); the binding's and the driver's frames are identical (the
+    binding run reports that SPH2O stepped with the GPU solver); against the
+    reference's frames: WCSPH time and time step equal, positions and
+    velocities within 1e-5 (norm-wise); DFSPH time and time step within
+    1e-5, positions within 1e-5, velocities within 2e-4 -- the bars of
+    test_gpu_parity (the force pass is held to a relative tolerance, not to
+    the bit, so near-cancelling velocity components differ in their last
+    bits).
 """
 import glob
 import json
@@ -87,8 +91,10 @@ def test_frames_match_the_reference(method, tmp_path):
     s_bind = write_scene(d, dirs["binding"])
     s_drv = write_scene(d, dirs["driver"])
     subprocess.run([REF32, "-c", s_ref, "--mode", "frames", "--steps", str(steps)], check=True, capture_output=True)
-    subprocess.run([REFGPU, "-c", s_bind, "--mode", "frames", "--steps", str(steps), "--gpu"], check=True,
-                   capture_output=True)
+    r = subprocess.run([REFGPU, "-c", s_bind, "--mode", "frames", "--steps", str(steps), "--gpu"], check=True,
+                       capture_output=True, text=True)
+    info = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+    assert info["gpu_solver"] is True
     subprocess.run([DRIVER, "-c", s_drv, "-o", "true", "--steps", str(steps), "--quiet"], check=True,
                    capture_output=True)
     ref, bind, drv = (read_frames(dirs[k]) for k in ("reference", "binding", "driver"))
@@ -102,7 +108,8 @@ def test_frames_match_the_reference(method, tmp_path):
         assert np.array_equal(b["x"], c["x"]) and np.array_equal(b["v"], c["v"]), name
         if method == S.WCSPH:
             assert a["time"] == b["time"] and a["timeStep"] == b["timeStep"], name
-            assert np.array_equal(a["x"], b["x"]) and np.array_equal(a["v"], b["v"]), name
+            assert rel_err(b["x"], a["x"]) <= 1e-5, name
+            assert rel_err(b["v"], a["v"]) <= 1e-5, name
         else:
             assert abs(float(a["time"]) - float(b["time"])) <= 1e-5 * float(a["time"]), name
             assert abs(float(a["timeStep"]) - float(b["timeStep"])) <= 1e-5 * float(a["timeStep"]), name
