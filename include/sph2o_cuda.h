@@ -223,15 +223,10 @@ enum sph_option {
     SPH_OPT_PASS_BLOCK = 3,       /* threads per block of the particle-pass kernels: 256 (default) or 128 */
     SPH_OPT_SOLVER_LANES = 4,     /* lanes sharing one particle's neighbour list in the persistent DFSPH
                                      solver: 1, 2 (default) or 4 */
-    SPH_OPT_POSITION_RESIDUAL = 5, /* 1: every position keeps the rounding residual of its integration
+    SPH_OPT_POSITION_RESIDUAL = 5 /* 1: every position keeps the rounding residual of its integration
                                      (float pair, error-free sums), so long runs of small steps keep about
                                      twice float precision; 0 (default): FP32 positions rounded as the
                                      reference rounds them. Single scenes, set before sph_init. */
-    SPH_OPT_FUSED_SMALL_STEPS = 6 /* 1 (default): a single WCSPH scene below 2^16 fluid particles (no emitters,
-                                     cube or PCISPH boundaries, position residuals or surface tension) runs
-                                     the steps of one sph_step call as one cooperative launch, every phase
-                                     separated by a bounded grid barrier; 0: one launch per phase. Same bits
-                                     either way. */
 };
 /* Number of values sph_autotune chooses (options 1..4 in order). */
 #define SPH_TUNE_COUNT 4

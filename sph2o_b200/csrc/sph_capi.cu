@@ -103,9 +103,6 @@ struct sph_ctx {
     /* CUDA graphs of two steps, keyed by the buffer assignment they start
        from (the sort swaps buffers, two steps may return to the start) */
     bool use_graphs = true;
-    /* small WCSPH scenes: whole steps in one cooperative launch (SPH_OPT_FUSED_SMALL_STEPS) */
-    bool fused_small = true;
-    int grid_small = 0;
     /* tunables (sph_set_option / sph_autotune) */
     int pass_block = 256;
     int solver_occ = 8;
@@ -504,43 +501,9 @@ int zero_accum(sph_ctx* c)
     return SPH_OK;
 }
 
-/* Whether WCSPH steps of this context run as one cooperative launch
-   (k_wcsph_small_steps): a single small scene without emitters, cube or
-   PCISPH boundaries, position residuals or surface tension, not profiled
-   phase by phase. */
-bool small_fused_ok(const sph_ctx* c)
-{
-    return c->fused_small && c->desc.simulation_method == SPH_WCSPH && !c->nscenes && !c->P.dynamic &&
-           c->cubes.empty() && !c->P.pcib && !c->P.pos_lo && !c->P.st_on && !c->prof && c->nf > 0 &&
-           c->nf < (1u << 16) && c->P.ncells / 4096u <= kSmallStepMaxChunks && c->grid_small > 0;
-}
-
-/* nsteps WCSPH steps in one launch. The buffers end as the separate kernels
-   leave them: the state back in pos/vel, the sorted copies of the last step
-   in pos2/vel2 (the adjoint's recompute reads them), the caller-order ids
-   swapped once per step. */
-int step_wcsph_small(sph_ctx* c, int nsteps)
-{
-    if (nsteps <= 0) return SPH_OK;
-    SmallStepArrays W{};
-    W.pos = c->pos; W.vel = c->vel; W.pos_s = c->pos2; W.vel_s = c->vel2;
-    W.orig_a = c->orig; W.orig_b = c->orig2;
-    W.cell_count = c->cell_count; W.cell_start = c->cell_start; W.chunk_sums = c->block_sums;
-    W.cell_of = c->cell_of; W.slot = c->slot; W.tmp_key = c->tmp_key; W.tmp_src = c->tmp_src;
-    W.cell_sorted = c->cell_sorted;
-    const int e = launch_wcsph_small_steps(c->P, arrays(c), W, nsteps, c->grid_small, c->stream);
-    if (e != 0)
-        return fail(c, SPH_ERR_CUDA, std::string("small-scene step launch: ") + cudaGetErrorString((cudaError_t)e));
-    c->launches += 1;
-    if (nsteps & 1) std::swap(c->orig, c->orig2);
-    c->lists_valid = false;
-    return check_launch(c, "wcsph small-scene steps");
-}
-
 int step_wcsph(sph_ctx* c)
 {
     int rc;
-    if (small_fused_ok(c)) return step_wcsph_small(c, 1);
     if ((rc = neighbor_search(c)) != SPH_OK) return rc;
     DeviceArrays A = arrays(c);
     { Phase ph(c, SPH_PROF_DENSITY, 1); launch_density(c->P, A, false, true, c->pass_block, c->stream); }
@@ -782,8 +745,6 @@ bool graph_steps(sph_ctx* c, int nsteps, int* rc)
    graphs; while profiling every step runs eagerly. */
 int run_steps(sph_ctx* c, int nsteps)
 {
-    /* small WCSPH scenes: all the steps in one cooperative launch */
-    if (small_fused_ok(c)) return step_wcsph_small(c, nsteps);
     int left = nsteps;
     while (left > 0) {
         int rc = SPH_OK;
@@ -1133,8 +1094,6 @@ int sph_init(sph_ctx* c)
 
     c->grid_pcisph = persistent_grid(true, false);
     if (c->grid_pcisph <= 0) return fail(c, SPH_ERR_CUDA, "cannot size the persistent solver grid");
-    c->grid_small = small_steps_grid();
-    if (c->grid_small <= 0) return fail(c, SPH_ERR_CUDA, "cannot size the small-scene step grid");
     for (int dv = 0; dv < 2; ++dv)
         for (int o = 0; o < 2; ++o)
             for (int t = 0; t < 3; ++t) {
@@ -1722,11 +1681,6 @@ int sph_set_option(sph_ctx* c, int option, int value)
         if (c->initialized) return fail(c, SPH_ERR_STATE, "position residuals are chosen before sph_init");
         c->pos_lo = value;
         return SPH_OK;
-    case SPH_OPT_FUSED_SMALL_STEPS:
-        if (value != 0 && value != 1) return fail(c, SPH_ERR_ARG, "the fused small-scene step option is 0 or 1");
-        c->fused_small = value != 0;
-        drop_graphs(c);
-        return SPH_OK;
     default:
         return fail(c, SPH_ERR_ARG, "unknown option");
     }
@@ -1742,7 +1696,6 @@ int sph_get_option(const sph_ctx* c, int option, int* value)
     case SPH_OPT_PASS_BLOCK: *value = c->pass_block; return SPH_OK;
     case SPH_OPT_SOLVER_LANES: *value = c->solver_tpp; return SPH_OK;
     case SPH_OPT_POSITION_RESIDUAL: *value = c->pos_lo; return SPH_OK;
-    case SPH_OPT_FUSED_SMALL_STEPS: *value = c->fused_small ? 1 : 0; return SPH_OK;
     default: return SPH_ERR_ARG;
     }
 }

@@ -1,10 +1,9 @@
 /*
  * Per-particle bodies of the neighbour search (sph_grid.cu): the counting
  * sort's count, scatter and rank + gather steps and the small-scene list
- * build (a warp per particle). The kernels of sph_grid.cu call them with one
- * thread (or warp) per index; the fused small-scene WCSPH step of
- * sph_solvers.cu calls the same bodies from its grid-stride phases, so both
- * paths produce the same bits.
+ * build (a warp per particle), kept apart from their kernels (one thread or
+ * warp per index) so that other kernels can run the same steps on their own
+ * index ranges, and the GatherSet the sort moves state with.
  */
 #ifndef SPH2O_GRID_BODY_CUH
 #define SPH2O_GRID_BODY_CUH

@@ -154,25 +154,6 @@ void launch_adjoint_finish(int n, const double* part, double* red, cudaStream_t 
 void launch_adjoint_step(const SimParams& P, const AdjointArrays& J, cudaStream_t s);
 void launch_adjoint_unpack(int n, const float4* in, float* out3, cudaStream_t s);
 
-/* Small-scene WCSPH steps in one cooperative launch (k_wcsph_small_steps):
-   every phase of SPH2O's WCSPH step (counting sort, warp list build, 4-lane
-   density and force passes) as a grid-stride loop over the bodies the
-   separate kernels use, phases separated by the bounded grid barrier. pos/vel
-   hold the state entering each step and receive the integrated state;
-   pos_s/vel_s the cell-sorted copies the passes read; orig_a/orig_b the
-   caller-order ids, which trade places every step (step s sorts from orig_a
-   when s is even). Needs nf < 2^16 and at most kSmallStepMaxChunks chunks
-   of 4096 cells. */
-struct SmallStepArrays {
-    float4 *pos, *vel, *pos_s, *vel_s;
-    unsigned *orig_a, *orig_b;
-    unsigned *cell_count, *cell_start, *chunk_sums, *cell_of, *slot, *tmp_key, *tmp_src, *cell_sorted;
-};
-constexpr unsigned kSmallStepMaxChunks = 1024;
-int small_steps_grid();
-int launch_wcsph_small_steps(const SimParams& P, const DeviceArrays& A, const SmallStepArrays& W, int nsteps, int grid,
-                             cudaStream_t s);
-
 /* co-resident grid size of the persistent solver kernels (0 on error) */
 int persistent_grid(bool pcisph, bool divergence, bool batch = false, int occ = 8, int tpp = 1);
 constexpr int kSolverBlock = 256;

@@ -1411,144 +1411,6 @@ int launch_barrier_timeout_probe(DevState* st, cudaStream_t s)
 
 /* ---------------------------------------------------------------------- */
 
-/* ---------------------------------------------------------------------- */
-/* Small scenes: whole WCSPH steps in one cooperative launch.              */
-/* Below 2^16 particles a step is ~10 short dependent launches (counting    */
-/* sort, warp list build, 4-lane density and force passes), each a few      */
-/* microseconds of latency on an almost idle GPU. k_wcsph_small_steps runs  */
-/* nsteps steps in one persistent launch: every phase is a grid-stride loop */
-/* over the same per-particle bodies the separate kernels use               */
-/* (sph_grid_body.cuh, density_lanes_at, forces_at), and phases are         */
-/* separated by the bounded grid barrier, so the results are the separate   */
-/* kernels' bit for bit. The step itself is SPH2O's WCSPHSolver::step        */
-/* (WCSPHSolver.cpp:14-78): neighbour search, densities + Tait pressures,    */
-/* pressure and viscosity forces, symplectic Euler.                          */
-
-/* Exclusive scan of populations count[chunk * 4096 .. + 4096) into start
-   (chunk-local offsets), zeroing the populations for the next search; the
-   chunk's total goes to chunk_sums[chunk]. One block of kSolverBlock threads,
-   16 cells per thread. */
-__device__ __forceinline__ void scan_chunk_block(unsigned* __restrict__ count, unsigned* __restrict__ start,
-                                                 unsigned* __restrict__ chunk_sums, unsigned chunk,
-                                                 unsigned* warp_tot)
-{
-    static_assert(kSolverBlock * 16 == 4096, "one chunk of 4096 cells per block");
-    const size_t base = (size_t)chunk * 4096 + (size_t)threadIdx.x * 16;
-    uint4 c[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        c[k] = *reinterpret_cast<const uint4*>(count + base + 4 * k);
-        *reinterpret_cast<uint4*>(count + base + 4 * k) = make_uint4(0, 0, 0, 0);
-    }
-    unsigned t = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) t += c[k].x + c[k].y + c[k].z + c[k].w;
-    unsigned incl = t;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    if (lane == 31) warp_tot[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-        constexpr int nw = kSolverBlock / 32;
-        const unsigned w = lane < nw ? warp_tot[lane] : 0u;
-        unsigned wi = w;
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned v = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += v;
-        }
-        if (lane < nw) warp_tot[lane] = wi - w;
-        if (lane == nw - 1) chunk_sums[chunk] = wi;
-    }
-    __syncthreads();
-    unsigned run = warp_tot[wid] + incl - t;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        uint4 o;
-        o.x = run; run += c[k].x;
-        o.y = run; run += c[k].y;
-        o.z = run; run += c[k].z;
-        o.w = run; run += c[k].w;
-        *reinterpret_cast<uint4*>(start + base + 4 * k) = o;
-    }
-    __syncthreads();  /* warp_tot is reused by the next chunk */
-}
-
-template <int TPP>
-__global__ void __launch_bounds__(kSolverBlock, 4) k_wcsph_small_steps(SimParams P, DeviceArrays A,
-                                                                       SmallStepArrays W, int nsteps)
-{
-    __shared__ unsigned s_warp[32];
-    __shared__ unsigned s_off[kSmallStepMaxChunks];
-    __shared__ float s_red[32];
-    DevState* st = A.st;
-    const int n = P.nf;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nthr = gridDim.x * blockDim.x;
-    const unsigned nchunks = P.ncells / 4096u;
-    const SceneRef S{};
-    /* the passes read the sorted copies and integrate into the state buffers */
-    DeviceArrays B = A;
-    B.pos = W.pos_s;
-    B.vel = W.vel_s;
-    B.pos_alt = W.pos;
-    B.vel_alt = W.vel;
-    B.cell_start = W.cell_start;
-    for (int s = 0; s < nsteps; ++s) {
-        unsigned* orig_in = (s & 1) ? W.orig_b : W.orig_a;
-        unsigned* orig_out = (s & 1) ? W.orig_a : W.orig_b;
-        /* counting sort into cells (HashTable::insertFluidParticle, HashTable.cpp:3-12) */
-        for (int i = tid; i < n; i += nthr) ns_count_at(P, S, i, W.pos, W.cell_count, W.cell_of, W.slot);
-        if (!grid_barrier(st)) return;
-        for (unsigned ch = blockIdx.x; ch < nchunks; ch += gridDim.x)
-            scan_chunk_block(W.cell_count, W.cell_start, W.chunk_sums, ch, s_warp);
-        if (!grid_barrier(st)) return;
-        /* chunk offsets, scanned by every block into shared memory */
-        for (unsigned ch = threadIdx.x; ch < nchunks; ch += blockDim.x) s_off[ch] = W.chunk_sums[ch];
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned run = 0;
-            for (unsigned ch = 0; ch < nchunks; ++ch) {
-                const unsigned v = s_off[ch];
-                s_off[ch] = run;
-                run += v;
-            }
-            if (blockIdx.x == 0) W.cell_start[P.ncells] = run;
-        }
-        __syncthreads();
-        for (unsigned c = (unsigned)tid; c < P.ncells; c += (unsigned)nthr) W.cell_start[c] += s_off[c >> 12];
-        if (!grid_barrier(st)) return;
-        for (int i = tid; i < n; i += nthr) ns_scatter_at(i, W.cell_of, W.slot, W.cell_start, orig_in, W.tmp_key, W.tmp_src);
-        if (!grid_barrier(st)) return;
-        {
-            GatherSet g{};
-            g.orig_out = orig_out;
-            g.cell_out = W.cell_sorted;
-            g.v4_in[0] = W.pos; g.v4_out[0] = W.pos_s;
-            g.v4_in[1] = W.vel; g.v4_out[1] = W.vel_s;
-            for (int p = tid; p < n; p += nthr) ns_rank_gather_at(p, W.cell_of, W.cell_start, W.tmp_key, W.tmp_src, g);
-        }
-        if (!grid_barrier(st)) return;
-        /* neighbour lists, a warp per particle (HashTable::neighborhoodSearch, HashTable.cpp:23-86) */
-        {
-            const int warp = tid >> 5, nwarps = nthr >> 5;
-            for (int i = warp; i < n; i += nwarps)
-                build_lists_warp_at(P, S, i, W.pos_s, W.cell_start, A.bpos, A.bcell_start, const_cast<unsigned*>(A.nbr_f),
-                                    const_cast<unsigned*>(A.cnt_f), const_cast<unsigned*>(A.nbr_b),
-                                    const_cast<unsigned*>(A.cnt_b), st);
-        }
-        if (!grid_barrier(st)) return;
-        /* densities and Tait pressures (SPHSolver.cpp:42-89, WCSPHSolver.cpp:80-95) */
-        for (int t = tid; t < n * TPP; t += nthr) density_lanes_at<true, TPP>(P, B, t);
-        if (!grid_barrier(st)) return;
-        /* pressure + non-pressure forces and integration (WCSPHSolver.cpp:132-188, SPHSolver.cpp:139-168) */
-        for (int t = tid; t < n * TPP; t += nthr) forces_at<FORCE_WCSPH, TPP>(P, B, t, t == 0, s_red);
-        if (!grid_barrier(st)) return;
-    }
-}
-
 static inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
 /* Lanes per particle for the WCSPH density and force passes: 4 below 2^16
@@ -1652,33 +1514,6 @@ int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cud
     const int need = blocks_for(P.nf > 0 ? P.nf : 1, kSolverBlock);
     const int g = grid < need ? grid : need;
     return coop_launch((const void*)k_pcisph_solve, P, A, g > 0 ? g : 1, s);
-}
-
-/* WCSPH steps of a small scene in one cooperative launch (k_wcsph_small_steps) */
-static const void* small_steps_fn() { return (const void*)k_wcsph_small_steps<4>; }
-
-int small_steps_grid()
-{
-    int dev = 0, sms = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, small_steps_fn(), kSolverBlock, 0) != cudaSuccess)
-        return 0;
-    return per_sm * sms;
-}
-
-int launch_wcsph_small_steps(const SimParams& P, const DeviceArrays& A, const SmallStepArrays& W, int nsteps, int grid,
-                             cudaStream_t s)
-{
-    /* enough blocks for a warp per particle in the list build, at most the co-resident ones */
-    const int need = blocks_for((long long)(P.nf > 0 ? P.nf : 1) * 32, kSolverBlock);
-    const int g = grid < need ? grid : need;
-    SimParams p = P;
-    DeviceArrays a = A;
-    SmallStepArrays w = W;
-    int n = nsteps;
-    void* args[] = {&p, &a, &w, &n};
-    return (int)cudaLaunchCooperativeKernel(small_steps_fn(), dim3(g > 0 ? g : 1), dim3(kSolverBlock), args, 0, s);
 }
 
 } // namespace sph
