@@ -521,14 +521,11 @@ def later_window_run(scene_dict, desc, start, steps, cpu=True, cpu_steps=5, cpu_
     return out
 
 
-def neighbor_search_roofline(sim, prof, steps, peak, peak_kind):
+def neighbor_search_roofline(nf, entries, prof, steps, peak, peak_kind):
     """Sort + list build against HBM: algorithmic bytes per fluid particle =
     52 (sort: read position and velocity 24, write them reordered 24, cell
     offset 4) + 20 (list build: read position 12, write two list lengths 8)
     + 4 per neighbour-list entry written, over their event time per step."""
-    fo, fi, bo, bi = sim.neighbors()
-    entries = int(fi.size) + int(bi.size)
-    nf = sim.nf
     ms = (prof["sort"]["ms"] + prof["lists"]["ms"]) / steps
     algo = nf * (52 + 20) + 4 * entries
     achieved = algo / (ms / 1e3) / 1e9
@@ -620,7 +617,12 @@ def main():
     launches = prof[dom]["launches"]
     avg_ms = prof[dom]["ms"] / launches
     it_for = its if dom == "density_solve" else itsv
-    nb_active = nb  # upper bound of boundary particles with a fluid neighbour
+    # boundary particles with a fluid neighbour, counted from the lists after
+    # the timed runs (the boundary is static; the fluid's reach changes slowly)
+    fo, fi, bo, bi = sim.neighbors()
+    nb_active = int(np.unique(bi).size)
+    list_entries = int(fi.size) + int(bi.size)
+    del fo, fi, bo, bi
     algo = bytes_per_launch(dom, nf, nb_active, it_for)
     achieved = algo / (avg_ms / 1e3) / 1e9
     traffic, traffic_note = None, "no DRAM capture recorded for this build of the kernel"
@@ -632,7 +634,8 @@ def main():
                         f"launch")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "traffic_note": traffic_note, "kernel": dom, "peak_kind": f"of {peak_kind}",
-                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": avg_ms}
+                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": avg_ms,
+                "boundary_particles_with_fluid_neighbour": nb_active}
 
     # End to end through the C ABI with host buffers, over the same window:
     # the state entering it is uploaded from pinned host memory, every step
@@ -678,8 +681,7 @@ def main():
                "note": "state uploaded once from pinned host memory, per-step statistics read back by every "
                        "sph_step call, final state (x, v, rho) read back; same window as value, after one "
                        "untimed pass of the same calls (one-step graph capture)"}
-    # list lengths for the neighbour-search bytes (read after the timed runs)
-    roofline["neighbor_search"] = neighbor_search_roofline(sim, prof, args.steps, peak, peak_kind)
+    roofline["neighbor_search"] = neighbor_search_roofline(nf, list_entries, prof, args.steps, peak, peak_kind)
     sim.close()
     scene.close()
 
