@@ -1018,9 +1018,6 @@ __global__ void __launch_bounds__(kSolverBlock, 8) k_dfsph_solve_batch(SimParams
 /* ---------------------------------------------------------------------- */
 /* PCISPH                                                                   */
 
-/* lanes sharing a particle in the PCISPH solver's two neighbour passes */
-constexpr int kPciLanes = 4;
-
 __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, DeviceArrays A)
 {
     __shared__ double s_red[32];
@@ -1067,17 +1064,9 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
         }
         if (!grid_barrier(st)) return;
         /* predictFluidDensities over the start-of-step candidates of the 27
-           cells around the particle's current cell, then updatePressure.
-           kPciLanes lanes share a particle: in each round they evaluate
-           consecutive candidates of a cell, and every lane of the group adds
-           the round's terms in candidate order (shuffled to it); rejected
-           candidates and padding add +0, which leaves the non-negative sum
-           unchanged -- the reference's sequential sum bit for bit. */
+           cells around the particle's current cell, then updatePressure */
         double local = 0.0;
-        for_particles<kPciLanes>(nfi, [&](int i, int sub, bool valid) {
-            if (!valid) return;
-            const unsigned lane = threadIdx.x & 31u, first = lane - (unsigned)sub;
-            const unsigned gmask = ((1u << kPciLanes) - 1u) << first;
+        for (int i = tid; i < nfi; i += nthr) {
             const float4 xi = A.pos[i];
             const float4 pi = A.predr[i];
             /* all fluid candidates of the 27 cells first, then all boundary
@@ -1086,38 +1075,25 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
             float rho = 0.0f;
             for_cells27(xi, P.h, g, [&](unsigned c) {
                 const unsigned e = A.cell_start[c + 1];
-                for (unsigned q0 = A.cell_start[c]; q0 < e; q0 += kPciLanes) {
-                    const unsigned q = q0 + (unsigned)sub;
-                    float w = 0.0f;
-                    if (q < e) {
-                        const float s2 = dist2_exact(pi, A.predr[q]);
-                        if (s2 <= P.h2_guard) w = __fmul_rn(P.mass, cs_W_exact(s2, P));
-                    }
-#pragma unroll
-                    for (int l = 0; l < kPciLanes; ++l) rho = __fadd_rn(rho, __shfl_sync(gmask, w, first + l));
+                for (unsigned q = A.cell_start[c]; q < e; ++q) {
+                    const float s2 = dist2_exact(pi, A.predr[q]);
+                    if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(P.mass, cs_W_exact(s2, P)));
                 }
             });
             if (P.nb > 0)
                 for_cells27(xi, P.h, g, [&](unsigned c) {
                     const unsigned e = A.bcell_start[c + 1];
-                    for (unsigned q0 = A.bcell_start[c]; q0 < e; q0 += kPciLanes) {
-                        const unsigned q = q0 + (unsigned)sub;
-                        float w = 0.0f;
-                        if (q < e) {
-                            const float4 xb = A.bpos[q];
-                            const float s2 = dist2_exact(pi, xb);
-                            if (s2 <= P.h2_guard) w = __fmul_rn(xb.w, cs_W_exact(s2, P));
-                        }
-#pragma unroll
-                        for (int l = 0; l < kPciLanes; ++l) rho = __fadd_rn(rho, __shfl_sync(gmask, w, first + l));
+                    for (unsigned q = A.bcell_start[c]; q < e; ++q) {
+                        const float4 xb = A.bpos[q];
+                        const float s2 = dist2_exact(pi, xb);
+                        if (s2 <= P.h2_guard) rho = __fadd_rn(rho, __fmul_rn(xb.w, cs_W_exact(s2, P)));
                     }
                 });
-            if (sub != 0) return;
             A.rho[i] = rho;
             const float err = fmaxf(0.0f, __fsub_rn(rho, P.rho0));
             A.press[i] = __fadd_rn(A.press[i], __fmul_rn(P.pcisph_delta, err));
             local += (double)(err / P.rho0);
-        });
+        }
         if (P.pcib)
             /* predictBoundaryDensities (Poly6) and their pressure update with
                the fluid's scaling factor (PCISPHSolver.cpp:211-244, 279-297) */
@@ -1133,66 +1109,43 @@ __global__ void __launch_bounds__(kSolverBlock, 4) k_pcisph_solve(SimParams P, D
         avg = *(volatile double*)&A.accum[it] / (double)nfi;
         /* computePressureAcc at the current positions, with the reference's
            exact gradient arithmetic: the result feeds the next predicted
-           positions, whose densities enter the ill-conditioned p update. The
-           lanes of a particle's group evaluate consecutive list entries (the
-           exact gradient is the expensive part) and every lane subtracts the
-           round's terms in list order; padding subtracts +0, which changes
-           no sum. */
-        for_particles<kPciLanes>(nfi, [&](int i, int sub, bool valid) {
-            if (!valid) return;
-            const unsigned lane = threadIdx.x & 31u, first = lane - (unsigned)sub;
-            const unsigned gmask = ((1u << kPciLanes) - 1u) << first;
+           positions, whose densities enter the ill-conditioned p update */
+        for (int i = tid; i < nfi; i += nthr) {
             const float4 xi = A.pos[i];
             const float rho_i = A.rho[i];
             const float dpi = __fdiv_rn(A.press[i], __fmul_rn(rho_i, rho_i));
             float ax = 0.0f, ay = 0.0f, az = 0.0f;
             const unsigned nF = A.cnt_f[i], nB = A.cnt_b[i];
-            for (unsigned k0 = 0; k0 < nF; k0 += kPciLanes) {
-                const unsigned kk = k0 + (unsigned)sub;
-                float tx = 0.0f, ty = 0.0f, tz = 0.0f;
-                if (kk < nF) {
-                    const unsigned j = list_at(A.nbr_f, kk, nf, i);
-                    const float4 xj = A.pos[j];
-                    const float rho_j = A.rho[j];
-                    float gx, gy, gz;
-                    cs_gradW_exact(__fsub_rn(xi.x, xj.x), __fsub_rn(xi.y, xj.y), __fsub_rn(xi.z, xj.z), P, gx, gy, gz);
-                    const float c = __fmul_rn(P.mass, __fadd_rn(dpi, __fdiv_rn(A.press[j], __fmul_rn(rho_j, rho_j))));
-                    tx = __fmul_rn(c, gx); ty = __fmul_rn(c, gy); tz = __fmul_rn(c, gz);
-                }
-#pragma unroll
-                for (int l = 0; l < kPciLanes; ++l) {
-                    ax = __fsub_rn(ax, __shfl_sync(gmask, tx, first + l));
-                    ay = __fsub_rn(ay, __shfl_sync(gmask, ty, first + l));
-                    az = __fsub_rn(az, __shfl_sync(gmask, tz, first + l));
-                }
+            for (unsigned kk = 0; kk < nF; ++kk) {
+                const unsigned j = list_at(A.nbr_f, kk, nf, i);
+                const float4 xj = A.pos[j];
+                const float rho_j = A.rho[j];
+                float gx, gy, gz;
+                cs_gradW_exact(__fsub_rn(xi.x, xj.x), __fsub_rn(xi.y, xj.y), __fsub_rn(xi.z, xj.z), P, gx, gy, gz);
+                const float c = __fmul_rn(P.mass, __fadd_rn(dpi, __fdiv_rn(A.press[j], __fmul_rn(rho_j, rho_j))));
+                ax = __fsub_rn(ax, __fmul_rn(c, gx));
+                ay = __fsub_rn(ay, __fmul_rn(c, gy));
+                az = __fsub_rn(az, __fmul_rn(c, gz));
             }
-            for (unsigned k0 = 0; k0 < nB; k0 += kPciLanes) {
-                const unsigned kk = k0 + (unsigned)sub;
-                float tx = 0.0f, ty = 0.0f, tz = 0.0f;
-                if (kk < nB) {
-                    const unsigned bq = list_at(A.nbr_b, kk, nf, i);
-                    const float4 xb = A.bpos[bq];
-                    float gx, gy, gz, c;
-                    if (P.pcib) {
-                        /* m_b (p_i / rho_i^2 + p_b / rho_b^2) Spiky::gradW (PCISPHSolver.cpp:336-347) */
-                        spiky_gradW(__fsub_rn(xi.x, xb.x), __fsub_rn(xi.y, xb.y), __fsub_rn(xi.z, xb.z), P, gx, gy, gz);
-                        const float rb = A.bdens[bq];
-                        c = __fmul_rn(xb.w, __fadd_rn(dpi, __fdiv_rn(A.bpress[bq], __fmul_rn(rb, rb))));
-                    } else {
-                        cs_gradW_exact(__fsub_rn(xi.x, xb.x), __fsub_rn(xi.y, xb.y), __fsub_rn(xi.z, xb.z), P, gx, gy, gz);
-                        c = __fmul_rn(xb.w, dpi);
-                    }
-                    tx = __fmul_rn(c, gx); ty = __fmul_rn(c, gy); tz = __fmul_rn(c, gz);
+            for (unsigned kk = 0; kk < nB; ++kk) {
+                const unsigned bq = list_at(A.nbr_b, kk, nf, i);
+                const float4 xb = A.bpos[bq];
+                float gx, gy, gz, c;
+                if (P.pcib) {
+                    /* m_b (p_i / rho_i^2 + p_b / rho_b^2) Spiky::gradW (PCISPHSolver.cpp:336-347) */
+                    spiky_gradW(__fsub_rn(xi.x, xb.x), __fsub_rn(xi.y, xb.y), __fsub_rn(xi.z, xb.z), P, gx, gy, gz);
+                    const float rb = A.bdens[bq];
+                    c = __fmul_rn(xb.w, __fadd_rn(dpi, __fdiv_rn(A.bpress[bq], __fmul_rn(rb, rb))));
+                } else {
+                    cs_gradW_exact(__fsub_rn(xi.x, xb.x), __fsub_rn(xi.y, xb.y), __fsub_rn(xi.z, xb.z), P, gx, gy, gz);
+                    c = __fmul_rn(xb.w, dpi);
                 }
-#pragma unroll
-                for (int l = 0; l < kPciLanes; ++l) {
-                    ax = __fsub_rn(ax, __shfl_sync(gmask, tx, first + l));
-                    ay = __fsub_rn(ay, __shfl_sync(gmask, ty, first + l));
-                    az = __fsub_rn(az, __shfl_sync(gmask, tz, first + l));
-                }
+                ax = __fsub_rn(ax, __fmul_rn(c, gx));
+                ay = __fsub_rn(ay, __fmul_rn(c, gy));
+                az = __fsub_rn(az, __fmul_rn(c, gz));
             }
-            if (sub == 0) A.pacc[i] = make_float4(ax, ay, az, 0.0f);
-        });
+            A.pacc[i] = make_float4(ax, ay, az, 0.0f);
+        }
         ++it;
     }
     if (!grid_barrier(st)) return;
@@ -1558,8 +1511,7 @@ int launch_dfsph_solve_batch(const SimParams& P, const DeviceArrays& A, bool div
 
 int launch_pcisph_solve(const SimParams& P, const DeviceArrays& A, int grid, cudaStream_t s)
 {
-    /* kPciLanes lanes per particle in the neighbour passes */
-    const int need = blocks_for((long long)(P.nf > 0 ? P.nf : 1) * kPciLanes, kSolverBlock);
+    const int need = blocks_for(P.nf > 0 ? P.nf : 1, kSolverBlock);
     const int g = grid < need ? grid : need;
     return coop_launch((const void*)k_pcisph_solve, P, A, g > 0 ? g : 1, s);
 }
