@@ -462,16 +462,22 @@ def combine_batch_results(res, world, device="cpu"):
 
 # ---- secondary workloads --------------------------------------------------------------------------------------
 
-def config_run(name, steps, warmup, cpu=True, cpu_window=None):
+def config_run(name, steps, warmup, cpu=True, cpu_window=None, tune=True):
     """One named workload on this GPU (device-timed window of `steps` after
     `warmup`) and, when cpu, the reference's OpenMP path on the host cores over
-    `cpu_window` = (steps, warmup) (default: the same window)."""
+    `cpu_window` = (steps, warmup) (default: the same window). With tune, the
+    library's autotuner picks cell order, solver occupancy, pass block and
+    solver lanes first (trial steps from a restored snapshot, cached per GPU
+    and workload)."""
     from sph2o_b200.api import Scene, Simulation
     desc, make = workloads()[name]
     d = make()
     scene = Scene.from_dict(d)
     sim = Simulation.from_scene(scene)
     nf, nb = sim.nf, sim.nb
+    tuned = None
+    if tune:
+        tuned = sim.autotune(trial_steps=3, cache_path=os.path.join(tempfile.gettempdir(), "sph2o_autotune.json"))
     if warmup:
         sim.step(warmup)
     st = sim.step(steps)
@@ -480,7 +486,7 @@ def config_run(name, steps, warmup, cpu=True, cpu_window=None):
     out = {"workload": desc, "fluid_particles": nf, "boundary_particles": nb, "steps": steps, "warmup": warmup,
            "value": nf * steps / (st["device_ms"] / 1e3), "unit": UNIT, "ms_per_step": st["device_ms"] / steps,
            "mean_iterations": st["total_iterations"] / steps, "mean_iterations_v": st["total_iterations_v"] / steps,
-           "last_avg_density_error": st["avg_density_error"], "l2": l2_note(nf, nb),
+           "last_avg_density_error": st["avg_density_error"], "l2": l2_note(nf, nb), "autotuned": tuned,
            "timing": "CUDA events on the library stream around the window"}
     if cpu:
         cs, cw = cpu_window or (steps, warmup)
