@@ -406,26 +406,6 @@ __device__ __forceinline__ unsigned list_at(const unsigned* list, unsigned kk, s
 }
 
 /* ---------------------------------------------------------------------- */
-/* Programmatic dependent launch. The pass kernels of a step are launched    */
-/* with cudaLaunchAttributeProgrammaticStreamSerialization (launch_pdl,      */
-/* sph_internal.h), so a kernel's launch and block scheduling overlap the    */
-/* tail of the kernel before it. Every such kernel starts with pdl_wait(),   */
-/* which returns once the preceding grid has completed and its memory is     */
-/* visible -- the kernel reads exactly what it reads after an ordinary       */
-/* launch -- and then pdl_trigger(), which lets the next kernel's blocks be  */
-/* scheduled as this grid's last blocks start. Without the launch attribute  */
-/* both are no-ops.                                                          */
-
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
-__device__ __forceinline__ void pdl_enter()
-{
-    pdl_wait();
-    pdl_trigger();
-}
-
-/* ---------------------------------------------------------------------- */
 /* Reductions                                                               */
 
 __device__ __forceinline__ double warp_sum(double v)

@@ -30,7 +30,6 @@ __global__ void __launch_bounds__(256) k_ns_count(SimParams P, SceneRef S, int n
                                                   const float4* __restrict__ pos, unsigned* __restrict__ cell_count,
                                                   unsigned* __restrict__ cell_of, unsigned* __restrict__ slot)
 {
-    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (n_dev ? (int)*n_dev : n)) return;
     ns_count_at(P, S, i, pos, cell_count, cell_of, slot);
@@ -41,7 +40,6 @@ __global__ void __launch_bounds__(256) k_ns_count(SimParams P, SceneRef S, int n
 __global__ void __launch_bounds__(1024) k_scan_local(unsigned* __restrict__ count, unsigned* __restrict__ start,
                                                      unsigned* __restrict__ block_sums)
 {
-    pdl_enter();
     __shared__ unsigned warp_tot[32];
     const size_t base = (size_t)blockIdx.x * 4096 + (size_t)threadIdx.x * 4;
     uint4 c = *reinterpret_cast<const uint4*>(count + base);
@@ -74,7 +72,6 @@ __global__ void __launch_bounds__(1024) k_scan_local(unsigned* __restrict__ coun
 __global__ void __launch_bounds__(1024) k_scan_blocks(unsigned* __restrict__ block_sums, int nblocks,
                                                       unsigned* __restrict__ total_out)
 {
-    pdl_enter();
     __shared__ unsigned warp_tot[32];
     __shared__ unsigned carry;
     if (threadIdx.x == 0) carry = 0;
@@ -112,7 +109,6 @@ __global__ void __launch_bounds__(1024) k_scan_blocks(unsigned* __restrict__ blo
 /* Phase 3: add the block offsets. */
 __global__ void __launch_bounds__(1024) k_scan_add(unsigned* __restrict__ start, const unsigned* __restrict__ block_sums)
 {
-    pdl_enter();
     const size_t base = (size_t)blockIdx.x * 4096 + (size_t)threadIdx.x * 4;
     const unsigned off = block_sums[blockIdx.x];
     uint4 s = *reinterpret_cast<uint4*>(start + base);
@@ -126,7 +122,6 @@ __global__ void __launch_bounds__(256) k_ns_scatter(int n, const unsigned* n_dev
                                                     const unsigned* __restrict__ orig,
                                                     unsigned* __restrict__ tmp_key, unsigned* __restrict__ tmp_src)
 {
-    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (n_dev ? (int)*n_dev : n)) return;
     ns_scatter_at(i, cell_of, slot, cell_start, orig, tmp_key, tmp_src);
@@ -138,7 +133,6 @@ __global__ void __launch_bounds__(256) k_ns_rank_gather(int n, const unsigned* _
                                                         const unsigned* __restrict__ tmp_key,
                                                         const unsigned* __restrict__ tmp_src, GatherSet g)
 {
-    pdl_enter();
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= (g.n_dev ? (int)*g.n_dev : n)) return;
     ns_rank_gather_at(p, cell_of, cell_start, tmp_key, tmp_src, g);
@@ -153,7 +147,6 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
                                                         unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b,
                                                         DevState* st)
 {
-    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= active_n(P, st)) return;
     const float4 xi = pos[i];
@@ -196,7 +189,6 @@ __global__ void __launch_bounds__(128) k_ns_build_lists_warp(SimParams P, SceneR
                                                              unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b,
                                                              DevState* st)
 {
-    pdl_enter();
     const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     /* the whole warp shares i and leaves together */
     if (i >= active_n(P, st)) return;
@@ -286,15 +278,13 @@ void launch_sort(const SimParams& P, const SceneRef& S, int n, const float4* pos
         cudaMemsetAsync(cell_start, 0, ((size_t)P.ncells + 1) * sizeof(unsigned), s);
         return;
     }
-    launch_pdl(k_ns_count, blocks_for(n, 256), 256, s, P, S, n, g.n_dev, pos_for_keys, cell_count, cell_of, slot);
+    k_ns_count<<<blocks_for(n, 256), 256, 0, s>>>(P, S, n, g.n_dev, pos_for_keys, cell_count, cell_of, slot);
     const int nblk = (int)(P.ncells / 4096);
-    launch_pdl(k_scan_local, nblk, 1024, s, cell_count, cell_start, block_sums);
-    launch_pdl(k_scan_blocks, 1, 1024, s, block_sums, nblk, cell_start + P.ncells);
-    launch_pdl(k_scan_add, nblk, 1024, s, cell_start, (const unsigned*)block_sums);
-    launch_pdl(k_ns_scatter, blocks_for(n, 256), 256, s, n, g.n_dev, (const unsigned*)cell_of, (const unsigned*)slot,
-               (const unsigned*)cell_start, orig_in, tmp_key, tmp_src);
-    launch_pdl(k_ns_rank_gather, blocks_for(n, 256), 256, s, n, (const unsigned*)cell_of, (const unsigned*)cell_start,
-               (const unsigned*)tmp_key, (const unsigned*)tmp_src, g);
+    k_scan_local<<<nblk, 1024, 0, s>>>(cell_count, cell_start, block_sums);
+    k_scan_blocks<<<1, 1024, 0, s>>>(block_sums, nblk, cell_start + P.ncells);
+    k_scan_add<<<nblk, 1024, 0, s>>>(cell_start, block_sums);
+    k_ns_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, g.n_dev, cell_of, slot, cell_start, orig_in, tmp_key, tmp_src);
+    k_ns_rank_gather<<<blocks_for(n, 256), 256, 0, s>>>(n, cell_of, cell_start, tmp_key, tmp_src, g);
 }
 
 void launch_build_lists(const SimParams& P, const SceneRef& S, const float4* pos, const unsigned* cell_start,
@@ -308,11 +298,11 @@ void launch_build_lists(const SimParams& P, const SceneRef& S, const float4* pos
        one lane per particle above, where the particles fill the GPU and the
        warp's extra instructions cost more (125k: 0.069 vs 0.096 ms). */
     if (P.nf < (1 << 16))
-        launch_pdl(k_ns_build_lists_warp, blocks_for((long long)P.nf * 32, 128), 128, s, P, S, pos, cell_start, bpos,
-                   bcell_start, nbr_f, cnt_f, nbr_b, cnt_b, st);
+        k_ns_build_lists_warp<<<blocks_for((long long)P.nf * 32, 128), 128, 0, s>>>(
+            P, S, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f, nbr_b, cnt_b, st);
     else
-        launch_pdl(k_ns_build_lists, blocks_for(P.nf, 128), 128, s, P, S, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f,
-                   nbr_b, cnt_b, st);
+        k_ns_build_lists<<<blocks_for(P.nf, 128), 128, 0, s>>>(P, S, pos, cell_start, bpos, bcell_start, nbr_f,
+                                                                cnt_f, nbr_b, cnt_b, st);
 }
 
 void launch_boundary_volume(const SimParams& P, const SceneRef& S, float4* bpos, const unsigned* bcell_start,

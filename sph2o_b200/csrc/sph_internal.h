@@ -15,25 +15,6 @@
 
 namespace sph {
 
-/* Launch with programmatic stream serialization: the kernel may be
-   scheduled while the previous kernel on the stream finishes; the kernel
-   itself waits for that grid (pdl_enter, sph_device.cuh) before reading. */
-template <typename... KArgs, typename... Args>
-inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args)
-{
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, args...);
-}
-
 
 /* Device pointers of one scene, handed to the solver launchers. */
 struct DeviceArrays {

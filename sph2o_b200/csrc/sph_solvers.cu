@@ -195,7 +195,6 @@ __device__ __forceinline__ float boundary_density(const SimParams& P, const Devi
 template <bool ALPHA, bool EOS, bool DIVRES = false>
 __global__ void __launch_bounds__(256, 8) k_density(SimParams P, DeviceArrays A)
 {
-    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= active_n(P, A.st)) return;
     const size_t nf = (size_t)P.nf;
@@ -283,13 +282,11 @@ __device__ __forceinline__ void density_lanes_at(const SimParams& P, const Devic
 template <bool EOS, int TPP>
 __global__ void __launch_bounds__(256) k_density_lanes(SimParams P, DeviceArrays A)
 {
-    pdl_enter();
     density_lanes_at<EOS, TPP>(P, A, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __global__ void __launch_bounds__(256, 8) k_normals(SimParams P, DeviceArrays A)
 {
-    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= active_n(P, A.st)) return;
     const size_t nf = (size_t)P.nf;
@@ -486,7 +483,6 @@ __device__ __forceinline__ void forces_at(const SimParams& P, const DeviceArrays
 template <int MODE, int TPP = 1>
 __global__ void __launch_bounds__(256, 6) k_forces(SimParams P, DeviceArrays A)
 {
-    pdl_enter();
     __shared__ float s_red[32];
     forces_at<MODE, TPP>(P, A, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.x == 0 && threadIdx.x == 0, s_red);
 }
@@ -1430,38 +1426,38 @@ void launch_density(const SimParams& P, const DeviceArrays& A, bool alpha, bool 
 {
     if (P.nf <= 0) return;
     const int g = blocks_for(P.nf, block);
-    if (alpha && eos) launch_pdl(k_density<true, true>, g, block, s, P, A);
-    else if (alpha && A.divres) launch_pdl(k_density<true, false, true>, g, block, s, P, A);
-    else if (alpha) launch_pdl(k_density<true, false>, g, block, s, P, A);
+    if (alpha && eos) k_density<true, true><<<g, block, 0, s>>>(P, A);
+    else if (alpha && A.divres) k_density<true, false, true><<<g, block, 0, s>>>(P, A);
+    else if (alpha) k_density<true, false><<<g, block, 0, s>>>(P, A);
     else if (small_scene_lanes(P.nf) > 1) {
         const int gl = blocks_for((long long)P.nf * 4, block);
-        if (eos) launch_pdl(k_density_lanes<true, 4>, gl, block, s, P, A);
-        else launch_pdl(k_density_lanes<false, 4>, gl, block, s, P, A);
+        if (eos) k_density_lanes<true, 4><<<gl, block, 0, s>>>(P, A);
+        else k_density_lanes<false, 4><<<gl, block, 0, s>>>(P, A);
     }
-    else if (eos) launch_pdl(k_density<false, true>, g, block, s, P, A);
-    else launch_pdl(k_density<false, false>, g, block, s, P, A);
+    else if (eos) k_density<false, true><<<g, block, 0, s>>>(P, A);
+    else k_density<false, false><<<g, block, 0, s>>>(P, A);
 }
 
 void launch_normals(const SimParams& P, const DeviceArrays& A, int block, cudaStream_t s)
 {
     if (P.nf <= 0) return;
-    launch_pdl(k_normals, blocks_for(P.nf, block), block, s, P, A);
+    k_normals<<<blocks_for(P.nf, block), block, 0, s>>>(P, A);
 }
 
 void launch_forces(const SimParams& P, const DeviceArrays& A, int mode, int block, cudaStream_t s)
 {
     const int g = P.nf > 0 ? blocks_for(P.nf, block) : 1;
     switch (mode) {
-    case FORCE_NP: launch_pdl(k_forces<FORCE_NP>, g, block, s, P, A); break;
-    case FORCE_NP_CFL: launch_pdl(k_forces<FORCE_NP_CFL>, g, block, s, P, A); break;
+    case FORCE_NP: k_forces<FORCE_NP><<<g, block, 0, s>>>(P, A); break;
+    case FORCE_NP_CFL: k_forces<FORCE_NP_CFL><<<g, block, 0, s>>>(P, A); break;
     case FORCE_WCSPH: {
         const int tpp = small_scene_lanes(P.nf);
         const int gw = P.nf > 0 ? blocks_for((long long)P.nf * tpp, block) : 1;
-        if (tpp == 1) launch_pdl(k_forces<FORCE_WCSPH, 1>, gw, block, s, P, A);
-        else launch_pdl(k_forces<FORCE_WCSPH, 4>, gw, block, s, P, A);
+        if (tpp == 1) k_forces<FORCE_WCSPH, 1><<<gw, block, 0, s>>>(P, A);
+        else k_forces<FORCE_WCSPH, 4><<<gw, block, 0, s>>>(P, A);
         break;
     }
-    default: launch_pdl(k_forces<FORCE_PRESSURE>, g, block, s, P, A); break;
+    default: k_forces<FORCE_PRESSURE><<<g, block, 0, s>>>(P, A); break;
     }
 }
 
