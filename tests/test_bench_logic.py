@@ -72,3 +72,24 @@ def test_roofline_byte_counts():
     assert ns["algorithmic_bytes_per_step"] == 1000 * 72 + 4 * 30000
     assert abs(ns["achieved"] - (1000 * 72 + 4 * 30000) / 0.2e-3 / 1e9) < 1e-9
     assert abs(ns["frac"] - ns["achieved"] / 6500.0) < 1e-12
+
+
+def test_reference_arm_prints_one_line(tmp_path):
+    """`bench.py --impl reference` runs the reference's OpenMP build on the
+    host (no GPU needed) and prints the contract's JSON line."""
+    import subprocess
+
+    if not os.path.exists(bench.REF_BIN):
+        pytest.skip("reference build missing (make -C oracle)")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                        "dam_break_wcsph_8k", "--steps", "3", "--warmup", "1"], capture_output=True, text=True,
+                       timeout=600, cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr[-500:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "particle-steps/s" and d["value"] > 0
+    assert d["steps"] == 3 and d["warmup"] == 1 and d["higher_is_better"] is True
+    assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
+    assert d["config"]["fluid_particles"] == 8000
