@@ -803,7 +803,11 @@ __global__ void __launch_bounds__(kSolverBlock, OCC) k_dfsph_solve(SimParams P, 
     }
 
     const float scale = DIV ? dt : ts2;
-    for (int i = tid; i < nfi; i += nthr) kws[i] *= scale;
+    /* the particle-to-lane mapping of the zeroing and accumulation passes:
+       with no iteration there is no barrier after the zeroing */
+    for_particles<TPP>(nfi, [&](int i, int sub, bool valid) {
+        if (valid && sub == 0) kws[i] *= scale;
+    });
     if (!DIV) {
         /* DFSPHSolver::updatePositions */
         bool bad = false;
