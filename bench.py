@@ -541,6 +541,22 @@ def neighbor_search_roofline(nf, entries, prof, steps, peak, peak_kind):
             "kernels": "k_ns_count, scan, k_ns_scatter, k_ns_rank_gather (sort); k_ns_build_lists (lists)"}
 
 
+def pair_evaluations(entries, its, itsv, prof, steps, window_ms, surface_tension=False):
+    """Neighbour-pair evaluations of a DFSPH step (the pair-bound side of the
+    roofline): every list entry (fluid and boundary) is evaluated once per
+    neighbour pass. Passes per step: density + alpha + divergence error,
+    surface-tension normals when on, non-pressure forces, the density solver's
+    warm start (2) and 2 per iteration, the divergence solver's warm-start
+    correction (its residual comes from the density pass) and 2 per
+    iteration."""
+    passes = 2 + (1 if surface_tension else 0) + (2 + 2 * its) + (1 + 2 * itsv)
+    solver_passes = 2 + 2 * its
+    return {"list_entries": entries, "passes_per_step": passes,
+            "per_step": entries * passes, "per_s": entries * passes * steps / (window_ms / 1e3),
+            "density_solver_per_s": entries * solver_passes * steps / (prof["density_solve"]["ms"] / 1e3),
+            "unit": "neighbour-pair evaluations"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -707,6 +723,11 @@ def main():
     roofline.update({"achieved": achieved, "frac": achieved / peak, "algorithmic_bytes_per_launch": algo,
                      "boundary_particles_with_fluid_neighbour": nb_active})
     roofline["neighbor_search"] = neighbor_search_roofline(nf, list_entries, prof, args.steps, peak, peak_kind)
+    if scene_dict["Configuration"].get("simulationMethod") == 2:
+        roofline["pair_evaluations"] = pair_evaluations(list_entries, its, itsv, prof, args.steps, max_ms,
+                                                        surface_tension=any(
+                                                            fm.get("surfaceTension", 0.0) != 0.0
+                                                            for fm in scene_dict["Fluid"]["FluidModel"]))
     sim.close()
     scene.close()
 

@@ -93,3 +93,19 @@ def test_reference_arm_prints_one_line(tmp_path):
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["config"]["fluid_particles"] == 8000
+
+
+def test_pair_evaluation_count():
+    """Neighbour passes of a DFSPH step: density + alpha + divergence error,
+    forces, the density solver's warm start (2) and 2 per iteration, the
+    divergence solver's warm-start correction and 2 per iteration (its
+    warm-start residual comes from the density pass); normals with surface
+    tension."""
+    import bench
+    prof = {"density_solve": {"ms": 10.0}}
+    r = bench.pair_evaluations(1000, 2.0, 1.0, prof, 20, 30.0)
+    assert r["passes_per_step"] == 2 + 6 + 3
+    assert r["per_step"] == 11000
+    assert abs(r["per_s"] - 11000 * 20 / 0.030) < 1e-6
+    assert abs(r["density_solver_per_s"] - 1000 * 6 * 20 / 0.010) < 1e-6
+    assert bench.pair_evaluations(1000, 2.0, 1.0, prof, 20, 30.0, surface_tension=True)["passes_per_step"] == 12
