@@ -223,10 +223,15 @@ enum sph_option {
     SPH_OPT_PASS_BLOCK = 3,       /* threads per block of the particle-pass kernels: 256 (default) or 128 */
     SPH_OPT_SOLVER_LANES = 4,     /* lanes sharing one particle's neighbour list in the persistent DFSPH
                                      solver: 1, 2 (default) or 4 */
-    SPH_OPT_POSITION_RESIDUAL = 5 /* 1: every position keeps the rounding residual of its integration
+    SPH_OPT_POSITION_RESIDUAL = 5,/* 1: every position keeps the rounding residual of its integration
                                      (float pair, error-free sums), so long runs of small steps keep about
                                      twice float precision; 0 (default): FP32 positions rounded as the
                                      reference rounds them. Single scenes, set before sph_init. */
+    SPH_OPT_LIST_STAGED = 6       /* neighbour-list build of single scenes of 2^16 fluid particles and more
+                                     in brick cell order: 1 one block per 4x4x4-cell brick with the
+                                     positions of the 6x6x6 cells around it staged in shared memory;
+                                     0 (default) one thread per particle reading the cells from global
+                                     memory. Both write the same lists. */
 };
 /* Number of values sph_autotune chooses (options 1..4 in order). */
 #define SPH_TUNE_COUNT 4

@@ -27,7 +27,8 @@ STATUS = {
     -7: "SPH_ERR_NO_DEVICE", -8: "SPH_ERR_IO", -9: "SPH_ERR_CAPACITY",
 }
 PHASE_DENSITY, PHASE_ALPHA, PHASE_NONPRESSURE_ACC, PHASE_PRESSURE, PHASE_PRESSURE_ACC = range(5)
-OPT_CUDA_GRAPHS, OPT_CELL_ORDER, OPT_SOLVER_OCCUPANCY, OPT_PASS_BLOCK, OPT_SOLVER_LANES, OPT_POSITION_RESIDUAL = range(6)
+(OPT_CUDA_GRAPHS, OPT_CELL_ORDER, OPT_SOLVER_OCCUPANCY, OPT_PASS_BLOCK, OPT_SOLVER_LANES, OPT_POSITION_RESIDUAL,
+ OPT_LIST_STAGED) = range(7)
 TUNE_COUNT = 4
 PROF_NAMES = ["sort", "lists", "density", "normals", "forces", "density_solve", "divergence_solve",
               "pressure_solve"]

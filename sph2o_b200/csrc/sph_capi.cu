@@ -106,6 +106,7 @@ struct sph_ctx {
     /* tunables (sph_set_option / sph_autotune) */
     int pass_block = 256;
     int solver_occ = 8;
+    bool staged_lists = false; /* SPH_OPT_LIST_STAGED */
     int solver_tpp = 2;  /* measured best on B200 for the 1M-particle scene (1, 2, 4: 1.03, 0.84, 0.92 ms) */
     float4* braw = nullptr;      /* boundary in caller order (re-sorted when the cell order changes) */
     unsigned* bid = nullptr;
@@ -465,7 +466,7 @@ int neighbor_search(sph_ctx* c)
     {
         Phase ph(c, SPH_PROF_LISTS, 1);
         launch_build_lists(c->P, SceneRef{c->d_scenes, c->d_scene_of}, c->pos, c->cell_start, c->bpos, c->bcell_start, c->nbr_f, c->cnt_f, c->nbr_b,
-                           c->cnt_b, c->st, c->stream);
+                           c->cnt_b, c->st, c->stream, c->staged_lists);
     }
     if (c->P.pcib) {
         /* the fluid's cells get candidate lists at this search */
@@ -1681,6 +1682,11 @@ int sph_set_option(sph_ctx* c, int option, int value)
         if (c->initialized) return fail(c, SPH_ERR_STATE, "position residuals are chosen before sph_init");
         c->pos_lo = value;
         return SPH_OK;
+    case SPH_OPT_LIST_STAGED:
+        if (value != 0 && value != 1) return fail(c, SPH_ERR_ARG, "the staged-list option is 0 or 1");
+        c->staged_lists = value == 1;
+        drop_graphs(c);
+        return SPH_OK;
     default:
         return fail(c, SPH_ERR_ARG, "unknown option");
     }
@@ -1696,6 +1702,7 @@ int sph_get_option(const sph_ctx* c, int option, int* value)
     case SPH_OPT_PASS_BLOCK: *value = c->pass_block; return SPH_OK;
     case SPH_OPT_SOLVER_LANES: *value = c->solver_tpp; return SPH_OK;
     case SPH_OPT_POSITION_RESIDUAL: *value = c->pos_lo; return SPH_OK;
+    case SPH_OPT_LIST_STAGED: *value = c->staged_lists ? 1 : 0; return SPH_OK;
     default: return SPH_ERR_ARG;
     }
 }

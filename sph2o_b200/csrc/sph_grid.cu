@@ -139,16 +139,15 @@ __global__ void __launch_bounds__(256) k_ns_rank_gather(int n, const unsigned* _
 }
 
 /* Neighbour lists in the reference's candidate order, filtered at |r| <= h. */
-__global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S, const float4* __restrict__ pos,
-                                                        const unsigned* __restrict__ cell_start,
-                                                        const float4* __restrict__ bpos,
-                                                        const unsigned* __restrict__ bcell_start,
-                                                        unsigned* __restrict__ nbr_f, unsigned* __restrict__ cnt_f,
-                                                        unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b,
-                                                        DevState* st)
+__device__ __forceinline__ void build_lists_at(const SimParams& P, const SceneRef& S, int i,
+                                               const float4* __restrict__ pos,
+                                               const unsigned* __restrict__ cell_start,
+                                               const float4* __restrict__ bpos,
+                                               const unsigned* __restrict__ bcell_start,
+                                               unsigned* __restrict__ nbr_f, unsigned* __restrict__ cnt_f,
+                                               unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b,
+                                               DevState* st)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= active_n(P, st)) return;
     const float4 xi = pos[i];
     const size_t nf = (size_t)P.nf;
     /* |r| <= h as the reference rounds it, without the square root */
@@ -177,6 +176,158 @@ __global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S,
     if (nF > P.capF || nB > P.capB) {
         atomicAdd(&st->overflow, 1u);
         atomicOr(&st->err, ERRBIT_OVERFLOW);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_ns_build_lists(SimParams P, SceneRef S, const float4* __restrict__ pos,
+                                                        const unsigned* __restrict__ cell_start,
+                                                        const float4* __restrict__ bpos,
+                                                        const unsigned* __restrict__ bcell_start,
+                                                        unsigned* __restrict__ nbr_f, unsigned* __restrict__ cnt_f,
+                                                        unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b,
+                                                        DevState* st)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= active_n(P, st)) return;
+    build_lists_at(P, S, i, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f, nbr_b, cnt_b, st);
+}
+
+/* ---------------------------------------------------------------------- */
+/* List build with each brick's halo staged in shared memory.               */
+
+/* the global-memory walk of one particle of a single scene, kept out of line */
+__device__ __noinline__ void build_lists_global(const SimParams& P, int i, const float4* __restrict__ pos,
+                                                const unsigned* __restrict__ cell_start,
+                                                const float4* __restrict__ bpos,
+                                                const unsigned* __restrict__ bcell_start,
+                                                unsigned* __restrict__ nbr_f, unsigned* __restrict__ cnt_f,
+                                                unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b,
+                                                DevState* st)
+{
+    build_lists_at(P, SceneRef{}, i, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f, nbr_b, cnt_b, st);
+}
+
+/* Fluid particles of one brick's 6 x 6 x 6-cell halo that fit in shared
+   memory (45 KB of float4); a brick with more takes the cells from global
+   memory instead. */
+constexpr unsigned kHaloCap = 2816;
+constexpr int kStagedBlock = 256;
+
+/* One block per 4 x 4 x 4-cell brick (single scenes in brick order). The
+   block lists the 216 cells around the brick with their fluid and boundary
+   ranges, lays the fluid cells' positions end to end in shared memory (one
+   warp per cell, coalesced), then every thread walks its particles' 27 cells
+   in the reference's offset order over the staged copies: the same
+   candidates in the same order, the same exact test, the same global slot
+   ids written, so the lists equal k_ns_build_lists's entry for entry. */
+__global__ void __launch_bounds__(kStagedBlock) k_ns_build_lists_staged(
+    SimParams P, const float4* __restrict__ pos, const unsigned* __restrict__ cell_start,
+    const float4* __restrict__ bpos, const unsigned* __restrict__ bcell_start, unsigned* __restrict__ nbr_f,
+    unsigned* __restrict__ cnt_f, unsigned* __restrict__ nbr_b, unsigned* __restrict__ cnt_b, DevState* st)
+{
+    __shared__ float4 s_pos[kHaloCap];
+    __shared__ unsigned s_off[217]; /* staged offset of each halo cell; [216] = total */
+    __shared__ unsigned s_gs[216];  /* global slot of each halo cell's first fluid particle */
+    __shared__ unsigned s_bs[216], s_be[216];
+    const Grid g = grid_single(P);
+    const unsigned b = blockIdx.x;
+    const unsigned c0 = b << 6;
+    const unsigned ps = cell_start[c0], pe = cell_start[c0 + 64];
+    if (ps == pe) return; /* the whole block leaves */
+    const int bx = (int)(b % (unsigned)g.nbx), by = (int)((b / (unsigned)g.nbx) % (unsigned)g.nby);
+    const int bz = (int)(b / ((unsigned)g.nbx * (unsigned)g.nby));
+    const int lane = (int)(threadIdx.x & 31u), warp = (int)(threadIdx.x >> 5);
+    for (int h = (int)threadIdx.x; h < 216; h += kStagedBlock) {
+        const int cx = 4 * bx - 1 + h % 6, cy = 4 * by - 1 + (h / 6) % 6, cz = 4 * bz - 1 + h / 36;
+        unsigned s = 0, e = 0, bs = 0, be = 0;
+        if (cx >= 0 && cx < g.dimx && cy >= 0 && cy < g.dimy && cz >= 0 && cz < g.dimz) {
+            const unsigned c = brick_morton(cx, cy, cz, g);
+            s = cell_start[c];
+            e = cell_start[c + 1];
+            if (P.nb > 0) {
+                bs = bcell_start[c];
+                be = bcell_start[c + 1];
+            }
+        }
+        s_gs[h] = s;
+        s_off[h] = e - s; /* the population until the scan below */
+        s_bs[h] = bs;
+        s_be[h] = be;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        /* exclusive scan of the 216 populations: 7 consecutive cells per lane */
+        unsigned v[7], t = 0;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            const int h = 7 * lane + k;
+            v[k] = h < 216 ? s_off[h] : 0u;
+            t += v[k];
+        }
+        unsigned incl = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        unsigned run = incl - t;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            const int h = 7 * lane + k;
+            if (h <= 216) s_off[h] = run;
+            run += v[k];
+        }
+    }
+    __syncthreads();
+    const bool staged = s_off[216] <= kHaloCap;
+    if (staged)
+        for (int h = warp; h < 216; h += kStagedBlock / 32) {
+            const unsigned s = s_gs[h], o = s_off[h], n = s_off[h + 1] - o;
+            for (unsigned k = (unsigned)lane; k < n; k += 32u) s_pos[o + k] = pos[s + k];
+        }
+    __syncthreads();
+    const size_t nf = (size_t)P.nf;
+    const float s2max = P.h2_exact;
+    for (unsigned i = ps + threadIdx.x; i < pe; i += kStagedBlock) {
+        const float4 xi = pos[i];
+        /* the particle's cell inside the brick (its sort cell) */
+        const int lx = cell_coord(xi.x, P.h, g.cminx, g.dimx) - 4 * bx;
+        const int ly = cell_coord(xi.y, P.h, g.cminy, g.dimy) - 4 * by;
+        const int lz = cell_coord(xi.z, P.h, g.cminz, g.dimz) - 4 * bz;
+        if ((unsigned)lx > 3u || (unsigned)ly > 3u || (unsigned)lz > 3u) {
+            /* moved out of its sort cell's brick since the sort: walk the
+               cells around its position in global memory */
+            build_lists_global(P, (int)i, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f, nbr_b, cnt_b, st);
+            continue;
+        }
+        unsigned nF = 0, nB = 0;
+        /* x outermost, z innermost (HashTable.cpp:59-65); cells outside the
+           grid have empty ranges */
+        for (int dx = 0; dx < 3; ++dx)
+            for (int dy = 0; dy < 3; ++dy)
+                for (int dz = 0; dz < 3; ++dz) {
+                    const int h = (lz + dz) * 36 + (ly + dy) * 6 + (lx + dx);
+                    const unsigned o = s_off[h], n = s_off[h + 1] - o, s = s_gs[h];
+                    for (unsigned k = 0; k < n; ++k) {
+                        const float4 xq = staged ? s_pos[o + k] : pos[s + k];
+                        if (dist2_exact(xi, xq) <= s2max) {
+                            if (nF < P.capF) __stcs(nbr_f + (size_t)nF * nf + i, s + k);
+                            ++nF;
+                        }
+                    }
+                    for (unsigned q = s_bs[h]; q < s_be[h]; ++q) {
+                        if (dist2_exact(xi, bpos[q]) <= s2max) {
+                            if (nB < P.capB) __stcs(nbr_b + (size_t)nB * nf + i, q);
+                            ++nB;
+                        }
+                    }
+                }
+        cnt_f[i] = min(nF, P.capF);
+        cnt_b[i] = min(nB, P.capB);
+        if (nF > P.capF || nB > P.capB) {
+            atomicAdd(&st->overflow, 1u);
+            atomicOr(&st->err, ERRBIT_OVERFLOW);
+        }
     }
 }
 
@@ -290,9 +441,16 @@ void launch_sort(const SimParams& P, const SceneRef& S, int n, const float4* pos
 void launch_build_lists(const SimParams& P, const SceneRef& S, const float4* pos, const unsigned* cell_start,
                         const float4* bpos,
                         const unsigned* bcell_start, unsigned* nbr_f, unsigned* cnt_f, unsigned* nbr_b,
-                        unsigned* cnt_b, DevState* st, cudaStream_t s)
+                        unsigned* cnt_b, DevState* st, cudaStream_t s, bool staged)
 {
     if (P.nf <= 0) return;
+    if (staged && !S.scenes && P.cell_order == 0 && P.nf >= (1 << 16)) {
+        /* one block per brick; bricks without fluid leave at once */
+        const int nbricks = P.nbx * P.nby * (P.dimz / 4);
+        k_ns_build_lists_staged<<<nbricks, kStagedBlock, 0, s>>>(P, pos, cell_start, bpos, bcell_start, nbr_f, cnt_f,
+                                                                  nbr_b, cnt_b, st);
+        return;
+    }
     /* A warp per particle below 2^16 particles, where one lane's serial walk
        over ~216 candidates is the critical path (32k: 32 vs 56 us per build);
        one lane per particle above, where the particles fill the GPU and the

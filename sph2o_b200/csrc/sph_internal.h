@@ -74,7 +74,7 @@ void launch_sort(const SimParams& P, const SceneRef& S, int n, const float4* pos
 void launch_build_lists(const SimParams& P, const SceneRef& S, const float4* pos, const unsigned* cell_start,
                         const float4* bpos,
                         const unsigned* bcell_start, unsigned* nbr_f, unsigned* cnt_f, unsigned* nbr_b,
-                        unsigned* cnt_b, DevState* st, cudaStream_t s);
+                        unsigned* cnt_b, DevState* st, cudaStream_t s, bool staged = false);
 void launch_boundary_volume(const SimParams& P, const SceneRef& S, float4* bpos, const unsigned* bcell_start,
                             float* bvol, cudaStream_t s);
 void launch_unsort_v4(int n, const unsigned* orig, const float4* in, float* out3, cudaStream_t s);

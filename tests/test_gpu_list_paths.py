@@ -62,3 +62,26 @@ def test_list_build_matches_exact_search(n):
         assert np.all((dk > 0) | ((dk == 0) & (dj > 0))), f"candidate order of particle {i}"
         got_b = bi[bo[i]:bo[i + 1]].astype(np.int64)
         assert np.array_equal(np.sort(got_b), want_b[i]), f"boundary set of particle {i}"
+
+
+@pytest.mark.parametrize("make,steps", [
+    (lambda: S.small(method=S.WCSPH, n=(42, 42, 40), seed=9), 60),   # 70,560: full cells, tank walls
+    (lambda: S.dam_break_dfsph_125k(), 25),                          # surface tension, splashing cells
+    (lambda: S.double_dam_break_1m(), 2),                            # 1M, sphere obstacle
+])
+def test_staged_build_equals_one_lane_build(make, steps):
+    """OPT_LIST_STAGED = 1 builds the lists of large single scenes one brick
+    per block from the brick's 6x6x6 cells staged in shared memory; it must
+    write the one-lane build's lists entry for entry, and so give the same
+    trajectory bit for bit: at the start and after `steps` steps."""
+    from sph2o_b200.api import OPT_LIST_STAGED
+    d = make()
+    out = {}
+    for staged in (1, 0):
+        sim = Simulation.from_scene(Scene.from_dict(d), options={OPT_LIST_STAGED: staged})
+        first = sim.neighbors()
+        sim.step(steps)
+        out[staged] = first + sim.neighbors() + sim.state()
+        sim.close()
+    for k, (a, b) in enumerate(zip(out[1], out[0])):
+        assert a.dtype == b.dtype and np.array_equal(a, b), f"array {k} differs"
