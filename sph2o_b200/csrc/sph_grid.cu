@@ -35,16 +35,22 @@ __global__ void __launch_bounds__(256) k_ns_count(SimParams P, SceneRef S, int n
     ns_count_at(P, S, i, pos, cell_count, cell_of, slot);
 }
 
-/* Exclusive scan, phase 1: each 1024-thread block scans 4096 populations,
-   writes block-local exclusive offsets and zeroes the populations. */
-__global__ void __launch_bounds__(1024) k_scan_local(unsigned* __restrict__ count, unsigned* __restrict__ start,
-                                                     unsigned* __restrict__ block_sums)
+/* Exclusive scan, phase 1: each 256-thread block scans 4096 populations (16
+   per thread, four 16-byte loads in flight), writes block-local exclusive
+   offsets and zeroes the populations. */
+__global__ void __launch_bounds__(256) k_scan_local(unsigned* __restrict__ count, unsigned* __restrict__ start,
+                                                    unsigned* __restrict__ block_sums)
 {
-    __shared__ unsigned warp_tot[32];
-    const size_t base = (size_t)blockIdx.x * 4096 + (size_t)threadIdx.x * 4;
-    uint4 c = *reinterpret_cast<const uint4*>(count + base);
-    *reinterpret_cast<uint4*>(count + base) = make_uint4(0, 0, 0, 0);
-    const unsigned t = c.x + c.y + c.z + c.w;
+    __shared__ unsigned warp_tot[8];
+    const size_t base = (size_t)blockIdx.x * 4096 + (size_t)threadIdx.x * 16;
+    uint4 c[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c[k] = *reinterpret_cast<const uint4*>(count + base + 4 * k);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) *reinterpret_cast<uint4*>(count + base + 4 * k) = make_uint4(0, 0, 0, 0);
+    unsigned t = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) t += (c[k].x + c[k].y) + (c[k].z + c[k].w);
     unsigned incl = t;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int o = 1; o < 32; o <<= 1) {
@@ -54,18 +60,26 @@ __global__ void __launch_bounds__(1024) k_scan_local(unsigned* __restrict__ coun
     if (lane == 31) warp_tot[wid] = incl;
     __syncthreads();
     if (wid == 0) {
-        unsigned w = warp_tot[lane];
+        const unsigned w = lane < 8 ? warp_tot[lane] : 0u;
         unsigned wi = w;
-        for (int o = 1; o < 32; o <<= 1) {
+        for (int o = 1; o < 8; o <<= 1) {
             const unsigned v = __shfl_up_sync(0xffffffffu, wi, o);
             if (lane >= o) wi += v;
         }
-        warp_tot[lane] = wi - w;
-        if (lane == 31) block_sums[blockIdx.x] = wi;
+        if (lane < 8) warp_tot[lane] = wi - w;
+        if (lane == 7) block_sums[blockIdx.x] = wi;
     }
     __syncthreads();
-    const unsigned ex = warp_tot[wid] + incl - t;
-    *reinterpret_cast<uint4*>(start + base) = make_uint4(ex, ex + c.x, ex + c.x + c.y, ex + c.x + c.y + c.z);
+    unsigned run = warp_tot[wid] + incl - t;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        uint4 o;
+        o.x = run; run += c[k].x;
+        o.y = run; run += c[k].y;
+        o.z = run; run += c[k].z;
+        o.w = run; run += c[k].w;
+        *reinterpret_cast<uint4*>(start + base + 4 * k) = o;
+    }
 }
 
 /* Phase 2: one block scans the block totals (any count, 1024 at a time). */
@@ -431,7 +445,7 @@ void launch_sort(const SimParams& P, const SceneRef& S, int n, const float4* pos
     }
     k_ns_count<<<blocks_for(n, 256), 256, 0, s>>>(P, S, n, g.n_dev, pos_for_keys, cell_count, cell_of, slot);
     const int nblk = (int)(P.ncells / 4096);
-    k_scan_local<<<nblk, 1024, 0, s>>>(cell_count, cell_start, block_sums);
+    k_scan_local<<<nblk, 256, 0, s>>>(cell_count, cell_start, block_sums);
     k_scan_blocks<<<1, 1024, 0, s>>>(block_sums, nblk, cell_start + P.ncells);
     k_scan_add<<<nblk, 1024, 0, s>>>(cell_start, block_sums);
     k_ns_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, g.n_dev, cell_of, slot, cell_start, orig_in, tmp_key, tmp_src);
