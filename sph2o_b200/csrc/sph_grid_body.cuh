@@ -54,6 +54,10 @@ __device__ __forceinline__ void ns_rank_gather_at(int p, const unsigned* __restr
                                                   const unsigned* __restrict__ tmp_src, const GatherSet& g)
 {
     const unsigned src = tmp_src[p];
+    /* the carried position and velocity are loaded before the cell lookup
+       and the rank loop, so their latency overlaps that chain */
+    const float4 v0 = g.v4_in[0] ? g.v4_in[0][src] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float4 v1 = g.v4_in[1] ? g.v4_in[1][src] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const unsigned c = cell_of[src];
     const unsigned key = tmp_key[p];
     const unsigned s = cell_start[c], e = cell_start[c + 1];
@@ -62,8 +66,8 @@ __device__ __forceinline__ void ns_rank_gather_at(int p, const unsigned* __restr
     const unsigned dst = s + rank;
     g.orig_out[dst] = key;
     if (g.cell_out) g.cell_out[dst] = c;
-    if (g.v4_in[0]) g.v4_out[0][dst] = g.v4_in[0][src];
-    if (g.v4_in[1]) g.v4_out[1][dst] = g.v4_in[1][src];
+    if (g.v4_in[0]) g.v4_out[0][dst] = v0;
+    if (g.v4_in[1]) g.v4_out[1][dst] = v1;
     if (g.v4_in[2]) g.v4_out[2][dst] = g.v4_in[2][src];
     if (g.v4_in[3]) g.v4_out[3][dst] = g.v4_in[3][src];
     if (g.f_in[0]) g.f_out[0][dst] = g.f_in[0][src];
