@@ -15,7 +15,9 @@
  *   5. ns_build_lists  for each particle, the 27 cells in the reference's
  *                      offset order (x outermost, HashTable.cpp:59-65), keep
  *                      candidates with |xi - xj| <= h (exact IEEE test), in
- *                      column-major neighbour lists
+ *                      column-major neighbour lists (optionally one block
+ *                      per cell brick with the brick's halo staged in
+ *                      shared memory: k_ns_build_lists_staged, same lists)
  * The static boundary is sorted once at init with steps 1-4 into its own
  * cellStart table, and AkinciBoundaryObject::computeVolume
  * (src/SPH2O/BoundaryObject/AkinciBoundaryObject.cpp:10-34) runs on it.
