@@ -450,7 +450,7 @@ int neighbor_search(sph_ctx* c)
         if (c->P.pcib) { g.v4_in[2] = c->normal; g.v4_out[2] = c->normal2; }
     }
     {
-        Phase ph(c, SPH_PROF_SORT, 6);
+        Phase ph(c, SPH_PROF_SORT, 5);
         launch_sort(c->P, SceneRef{c->d_scenes, c->d_scene_of}, (int)c->nf, c->pos, c->cell_count, c->cell_start, c->block_sums, c->cell_of, c->slot,
                     c->tmp_key, c->tmp_src, c->orig, g, c->stream);
     }

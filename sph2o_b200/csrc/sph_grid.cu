@@ -6,7 +6,7 @@
  * Per step:
  *   1. ns_count        cell key floor(x / h) -> brick-Morton cell index,
  *                      per-cell population by atomicAdd (slot = old count)
- *   2. scan_*          exclusive scan of the populations -> cellStart[ncells+1]
+ *   2. scan_local/add  exclusive scan of the populations -> cellStart[ncells+1]
  *                      (the scan zeroes the populations for the next step)
  *   3. ns_scatter      (orig id, source index) into its cell segment
  *   4. ns_rank_gather  rank inside the cell by orig id (deterministic, equal
@@ -84,49 +84,29 @@ __global__ void __launch_bounds__(256) k_scan_local(unsigned* __restrict__ count
     }
 }
 
-/* Phase 2: one block scans the block totals (any count, 1024 at a time). */
-__global__ void __launch_bounds__(1024) k_scan_blocks(unsigned* __restrict__ block_sums, int nblocks,
-                                                      unsigned* __restrict__ total_out)
+/* Phase 2: each block adds to its chunk the totals of all chunks before it
+   (summed by the block itself, so the chunk totals need no scan of their
+   own), and the last block writes the grand total. */
+__global__ void __launch_bounds__(1024) k_scan_add(unsigned* __restrict__ start,
+                                                   const unsigned* __restrict__ block_sums, int nblocks,
+                                                   unsigned* __restrict__ total_out)
 {
     __shared__ unsigned warp_tot[32];
-    __shared__ unsigned carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int base = 0; base < nblocks; base += 1024) {
-        const int i = base + threadIdx.x;
-        const unsigned v0 = i < nblocks ? block_sums[i] : 0u;
-        unsigned incl = v0;
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        if (lane == 31) warp_tot[wid] = incl;
-        __syncthreads();
-        if (wid == 0) {
-            const unsigned w = warp_tot[lane];
-            unsigned wi = w;
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned v = __shfl_up_sync(0xffffffffu, wi, o);
-                if (lane >= o) wi += v;
-            }
-            warp_tot[lane] = wi - w;
-        }
-        __syncthreads();
-        const unsigned ex = carry + warp_tot[wid] + incl - v0;
-        if (i < nblocks) block_sums[i] = ex;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry = ex + v0;
-        __syncthreads();
+    unsigned v = 0;
+    for (int k = threadIdx.x; k < (int)blockIdx.x; k += 1024) v += block_sums[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) warp_tot[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned w = warp_tot[lane];
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+        if (lane == 0) warp_tot[0] = w;
     }
-    if (threadIdx.x == 0) *total_out = carry;
-}
-
-/* Phase 3: add the block offsets. */
-__global__ void __launch_bounds__(1024) k_scan_add(unsigned* __restrict__ start, const unsigned* __restrict__ block_sums)
-{
+    __syncthreads();
+    const unsigned off = warp_tot[0];
+    if ((int)blockIdx.x == nblocks - 1 && threadIdx.x == 0) *total_out = off + block_sums[blockIdx.x];
     const size_t base = (size_t)blockIdx.x * 4096 + (size_t)threadIdx.x * 4;
-    const unsigned off = block_sums[blockIdx.x];
     uint4 s = *reinterpret_cast<uint4*>(start + base);
     s.x += off; s.y += off; s.z += off; s.w += off;
     *reinterpret_cast<uint4*>(start + base) = s;
@@ -448,8 +428,7 @@ void launch_sort(const SimParams& P, const SceneRef& S, int n, const float4* pos
     k_ns_count<<<blocks_for(n, 256), 256, 0, s>>>(P, S, n, g.n_dev, pos_for_keys, cell_count, cell_of, slot);
     const int nblk = (int)(P.ncells / 4096);
     k_scan_local<<<nblk, 256, 0, s>>>(cell_count, cell_start, block_sums);
-    k_scan_blocks<<<1, 1024, 0, s>>>(block_sums, nblk, cell_start + P.ncells);
-    k_scan_add<<<nblk, 1024, 0, s>>>(cell_start, block_sums);
+    k_scan_add<<<nblk, 1024, 0, s>>>(cell_start, block_sums, nblk, cell_start + P.ncells);
     k_ns_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, g.n_dev, cell_of, slot, cell_start, orig_in, tmp_key, tmp_src);
     k_ns_rank_gather<<<blocks_for(n, 256), 256, 0, s>>>(n, cell_of, cell_start, tmp_key, tmp_src, g);
 }
